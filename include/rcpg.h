@@ -1,0 +1,234 @@
+/* rcpgenerator_b200 -- C ABI of the B200 packing engine.
+ *
+ * Drop-in replacement for the relaxation path of RCPGenerator
+ * (KD-physics/RCPGenerator, paths relative to its python_code/python/):
+ *   rcpgenerator::run_packing / run_packing_observed
+ *       include/rcpgenerator/rcp_generator.hpp:269-280, bound to Python by
+ *       src/bindings/module.cpp:236-296 as _rcpgenerator.run_packing(_observed)
+ *   its exported per-step kernels
+ *       get_pairs_nd_3 (rcp_generator.hpp:200-216), get_forces_nd_3 (:218-243),
+ *       adam_update (:245-267), compute_mean_force (:150-155),
+ *       scale_diameters_nd (:180-185)
+ *   and the initializer
+ *       rcpgenerator::initialize_particles (include/rcpgenerator/initialize_particles.hpp:90),
+ *       bound as _rcpgenerator.initialize_particles (src/bindings/module.cpp:228-234).
+ *
+ * Conventions
+ *   - Plain pointers and sizes only. Arrays of per-particle vectors are flat and
+ *     particle-major: x[i*ndim + d] (the reference flattens its nested vectors
+ *     the same way, rcp_generator.cpp:4357-4363).
+ *   - "_dev" pointers are CUDA device pointers on the current device; `stream`
+ *     is a cudaStream_t (NULL = legacy default stream).
+ *   - Every function returns RCPG_OK (0) or a negative error code and, when
+ *     `err` is non-NULL, writes a NUL-terminated message into err[errlen].
+ *     RCPG_ERUNTIME carries the reference's std::runtime_error text (neighbour
+ *     capacity overflow, box/walls length), RCPG_EINVAL an argument error
+ *     (the reference's std::invalid_argument / ValueError cases).
+ *   - No CPU fallback: without a usable CUDA device every compute entry point
+ *     fails with RCPG_ECUDA.
+ */
+#ifndef RCPG_H
+#define RCPG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RCPG_ABI_VERSION 1
+
+#define RCPG_OK 0
+#define RCPG_ERUNTIME (-1)
+#define RCPG_ECUDA (-2)
+#define RCPG_EINVAL (-22)
+#define RCPG_ENOSPC (-28)
+
+/* PackingInput + PackingConfig (rcp_generator.hpp:18-33). box/walls may be
+ * NULL with length 0 (the reference's defaults: unit box, all periodic). */
+typedef struct rcpg_packing_input {
+    uint64_t N;
+    int32_t ndim;
+    const double* positions; /* [N*ndim] */
+    const double* diameters; /* [N] */
+    const double* box;       /* [box_len] */
+    int32_t box_len;
+    const int8_t* walls;     /* [walls_len]; walls[0] = -t: t-ball container */
+    int32_t walls_len;
+    uint32_t neighbor_max;   /* 0 = the reference's default per Ndim */
+    uint32_t seed;           /* accepted and unused, as in the reference */
+    int32_t fix_height;
+} rcpg_packing_input;
+
+/* PackingRunOptions (rcp_generator.hpp:102-123) plus engine selection. */
+typedef struct rcpg_run_options {
+    uint64_t max_steps;          /* 0 = schedule-derived cap */
+    int32_t has_mu_override;
+    double mu_override;
+    int32_t fix_diameter;
+    int32_t has_target_phi;
+    double target_phi;
+    uint64_t reorder_interval;   /* default 2000; 0 disables the spatial reorder */
+    int32_t has_initial_phi_target;
+    double initial_phi_target;
+    int32_t exact;               /* 1: host-controlled steps + one-thread reduction order */
+    int32_t device;              /* CUDA device ordinal */
+    int32_t graph_steps;         /* steps per CUDA graph replay (graph mode), 0 = default */
+} rcpg_run_options;
+
+/* PackingObservation (rcp_generator.hpp:92-98). */
+typedef struct rcpg_observation {
+    uint64_t step;
+    double phi;
+    double force_magnitude;
+    double energy;
+    double max_min_dist;
+} rcpg_observation;
+
+/* Observer (PackingObserver, rcp_generator.hpp:125-127): positions is
+ * [N*ndim] when the call captures this sample's positions, else NULL. */
+typedef void (*rcpg_observer_fn)(const rcpg_observation* obs, const double* positions, void* user);
+
+/* PackingResult (rcp_generator.hpp:35-90) + PackingTrace (:100-108).
+ * Library-owned; release with rcpg_result_free. */
+typedef struct rcpg_result {
+    uint64_t N;
+    int32_t ndim;
+    uint64_t steps;
+    double phi;                /* box-relative, as the reference's result.phi */
+    double max_min_dist;
+    double force_magnitude;
+    double* positions;         /* [N*ndim] (after the spatial reorders) */
+    double* diameters;         /* [N] */
+    double* box;               /* [ndim] */
+    int8_t* walls;             /* [ndim] (normalised) */
+    double* phi_history;       /* [steps] each */
+    double* force_history;
+    double* energy_history;
+    double* max_overlap_history;
+    double* mu_history;
+    double* alpha_history;
+    int8_t* mu_flag_history;
+    uint64_t* particle_origin; /* [N] */
+    uint64_t trace_len;
+    uint64_t* trace_steps;     /* [trace_len] */
+    double* trace_positions;   /* [trace_len*N*ndim] (NULL unless captured) */
+    double* trace_diameters;   /* [trace_len*N] (NULL unless captured) */
+    double* trace_phi;
+    double* trace_force;
+    double* trace_energy;
+    double* trace_max_min_dist;
+    uint64_t pair_builds;      /* neighbour-list builds performed */
+    uint32_t row_capacity;     /* neighbour row capacity in use at the end */
+    uint64_t kernel_launches;  /* kernels launched by this run */
+} rcpg_result;
+
+const char* rcpg_version(void);
+int32_t rcpg_abi_version(void);
+/* Number of visible CUDA devices (0 when none / no driver). */
+int32_t rcpg_device_count(void);
+
+void rcpg_default_options(rcpg_run_options* opt);
+
+/* run_packing_observed (rcp_generator.hpp:272-280; module.cpp:247-296).
+ * progress_interval / trajectory_interval 0 = off. */
+int32_t rcpg_run_packing(const rcpg_packing_input* in, const rcpg_run_options* opt,
+                         uint64_t progress_interval, int32_t capture_positions,
+                         uint64_t trajectory_interval, rcpg_observer_fn observer, void* user,
+                         rcpg_result** out, char* err, size_t errlen);
+void rcpg_result_free(rcpg_result* r);
+
+/* Step-wise control of one packing (the loop of run_packing_observed,
+ * rcp_generator.cpp:5511-6662, advanced in slices). */
+typedef struct rcpg_engine rcpg_engine;
+int32_t rcpg_engine_create(const rcpg_packing_input* in, const rcpg_run_options* opt,
+                           void* stream, rcpg_engine** out, char* err, size_t errlen);
+/* Advance by at most max_new_steps (0 = to completion); *finished = 1 once
+ * the run has converged or reached its step cap. */
+int32_t rcpg_engine_advance(rcpg_engine* e, uint64_t max_new_steps, int32_t* finished,
+                            char* err, size_t errlen);
+uint64_t rcpg_engine_steps(const rcpg_engine* e);
+uint64_t rcpg_engine_kernel_launches(const rcpg_engine* e);
+int32_t rcpg_engine_result(rcpg_engine* e, rcpg_result** out, char* err, size_t errlen);
+void rcpg_engine_destroy(rcpg_engine* e);
+
+/* ---- per-step kernels on device buffers ---------------------------------- */
+
+/* Pair shell of a full refresh: min(max(median*1.02, Dmin*2.25), Dmax)*0.5
+ * (rcp_generator.cpp:2846, :1210). Host arrays. */
+double rcpg_t_shell(const double* D, uint64_t N);
+
+/* Full-refresh neighbour rows (get_pairs_kdtree for ndim <= 3, get_pairs_nd_3
+ * otherwise, with every particle refreshed): row i holds every j != i with
+ * MIC |x_j - x_i|^2 < r_c^2 (the reference's predicate), ascending, stored
+ * column-major: nbr_dev[k*N + i], k < cnt_dev[i] <= row_capacity.
+ * *row_need_out = longest row; when it exceeds row_capacity the rows are
+ * truncated and RCPG_ENOSPC is returned. box/walls are host arrays [ndim]. */
+int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const double* D_dev,
+                        const double* box, const int8_t* walls, double t_shell,
+                        uint32_t row_capacity, uint32_t* nbr_dev, uint32_t* cnt_dev,
+                        uint32_t* row_need_out, void* stream, char* err, size_t errlen);
+
+/* get_forces_nd_3 (rcp_generator.hpp:218-243) on rows from rcpg_pairs_full
+ * (any superset of the overlapping pairs gives the same result), followed by
+ * compute_mean_force (:150-155). Writes F_dev [N*ndim] and
+ * scalars[7] = {U, max_min_dist, Lc, Fmean, dkappa, mean_force, count}.
+ * exact_order = 1 reduces the scalars in the reference's one-thread order. */
+int32_t rcpg_forces(uint64_t N, int32_t ndim, const double* x_dev, const double* D_dev,
+                    const double* box, const int8_t* walls, const uint32_t* nbr_dev,
+                    const uint32_t* cnt_dev, uint32_t row_capacity, double mu,
+                    int32_t exact_order, double* F_dev, double* scalars, void* stream,
+                    char* err, size_t errlen);
+
+/* compute_mean_force (rcp_generator.hpp:150-155) of F_dev [N*ndim]. */
+int32_t rcpg_mean_force(uint64_t N, int32_t ndim, const double* F_dev, double* mean_out,
+                        void* stream, char* err, size_t errlen);
+
+/* adam_update (rcp_generator.hpp:245-267) for the particles followed by the
+ * position step and the single-box wrap, i.e. the fused pass of
+ * rcp_generator.cpp:6410-6521, at bias-correction step t >= 1. */
+int32_t rcpg_adam_step(uint64_t N, int32_t ndim, const double* F_dev, double* m_dev,
+                       double* v_dev, double* x_dev, const double* box, double alpha,
+                       uint64_t t, void* stream, char* err, size_t errlen);
+
+/* Growth-aware displacement refresh trigger (rcp_generator.cpp:6104-6145):
+ * updates D_last (running min), theta_anchor and, for refreshed particles,
+ * x_last; refresh_dev[i] in {0,1}; *count_out = refreshed particles. */
+int32_t rcpg_refresh_check(uint64_t N, int32_t ndim, const double* x_dev, double* x_last_dev,
+                           const double* D_dev, double* D_last_dev, double* theta_dev,
+                           double theta_new, uint8_t* refresh_dev, uint64_t* count_out,
+                           void* stream, char* err, size_t errlen);
+
+/* scale_diameters_nd (rcp_generator.hpp:180-185), host arrays; returns the factor. */
+double rcpg_scale_diameters_nd(const double* D, uint64_t N, double phi_target, const double* box,
+                               int32_t ndim, int32_t fix_height, double* D_out);
+
+/* ---- initializer ---------------------------------------------------------- */
+
+/* Distribution (initialize_particles.hpp:18-31); type is a NUL-terminated
+ * name: mono, gaussian, bigaussian, bidisperse, lognormal, flat, powerlaw,
+ * exponential, weibull, custom. */
+typedef struct rcpg_distribution {
+    const char* type;
+    double d, mu, sigma, mu1, sigma1, mu2, sigma2, p, d1, d2, d_min, d_max, exponent, scale,
+        shape;
+    const double* custom; /* [custom_len] */
+    uint64_t custom_len;
+} rcpg_distribution;
+
+/* initialize_particles (initialize_particles.hpp:33-53, :90). Host arrays:
+ * positions_out [N*ndim], diameters_out [N], box_out [ndim], walls_out [ndim];
+ * box/walls inputs may be NULL with length 0. */
+int32_t rcpg_initialize_particles(double phi, uint64_t N, int32_t ndim, const double* box,
+                                  int32_t box_len, const int8_t* walls, int32_t walls_len,
+                                  int32_t fix_height, const rcpg_distribution* dist,
+                                  uint64_t seed, double* positions_out, double* diameters_out,
+                                  double* box_out, int8_t* walls_out, double* scale_factor_out,
+                                  double* phi_modifier_out, char* err, size_t errlen);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RCPG_H */

@@ -1,0 +1,27 @@
+"""rcpgenerator_b200: RCPGenerator's packing engine on one NVIDIA B200.
+
+Drop-in for the relaxation path of RCPGenerator (``Packing(...).pack()``):
+the same ``Packing`` class and the same module functions as the reference
+package ``rcpgenerator`` / its binding ``_rcpgenerator``, computed by
+hand-written sm_100a CUDA kernels behind a C ABI (include/rcpg.h).
+"""
+
+from ._api import (
+    PackingEngine,
+    get_num_threads,
+    initialize_particles,
+    run_packing,
+    run_packing_observed,
+    set_num_threads,
+)
+from ._wrapper import Packing
+
+__all__ = [
+    "Packing",
+    "PackingEngine",
+    "get_num_threads",
+    "initialize_particles",
+    "run_packing",
+    "run_packing_observed",
+    "set_num_threads",
+]

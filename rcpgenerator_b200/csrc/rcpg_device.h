@@ -1,0 +1,133 @@
+// Device-resident state of one packing and the launchers of its kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rcpg_core.h"
+#include "rcpg_schedule.h"
+
+namespace rcpg {
+
+// Scalars the particle kernels read, plus status words they write. Lives in
+// device memory; in exact (host-controlled) mode the host rewrites it every
+// step, in graph mode the controller kernel does.
+struct DevCtl {
+    Controller c;        // schedule state (graph mode: owned by the controller kernel)
+    Geometry g;          // box / walls of the current step
+    ForceSums sums;      // reduced sums of the last force evaluation
+    StepScalars scal;    // finalised scalars of the last force evaluation
+    // ADAM pass parameters (of the step being finished)
+    double adam_box[kMaxDim];
+    double adam_alpha, adam_inv_b1, adam_inv_b2;
+    double fix_height_scale;
+    // pair-list build parameters
+    double build_kappa;  // D = D0 * build_kappa during the build
+    double build_t_shell;
+    double build_Dmax;
+    // refresh anchor (shared by all particles: every rebuild re-anchors all)
+    double refresh_kappa;  // D = D0 * refresh_kappa in the trigger
+    double kappa_min;      // running minimum of kappa since the anchor
+    double theta;          // budget
+    double force_kappa;    // D = D0 * force_kappa in the forces
+    double force_mu;       // mu fed to the forces
+    // cell grid of the current build
+    int ncell[kMaxDim];
+    double cell_scale[kMaxDim];
+    std::uint32_t ncells;
+    // control words
+    std::uint32_t rebuild_flag;   // rebuild the pair list before the forces
+    std::uint32_t adam_go;        // ADAM pass of the finished step is pending
+    std::uint32_t stopped;        // graph steps after this point do nothing
+    std::uint32_t halted;         // stopped because of an error / capacity overflow
+    std::uint32_t row_need;       // largest full row seen by a build
+    std::uint32_t cap_error;      // a half row exceeded the reference capacity
+    std::uint32_t cap_error_particle;
+    std::uint32_t cap_error_cap;
+    std::uint32_t nbuilds;        // pair-list builds performed
+    std::uint32_t pad0;
+    std::uint64_t graph_steps;    // steps completed by the controller kernel
+};
+
+struct DevArrays {
+    std::uint64_t N;
+    int ndim;
+    int P;                  // pos stride
+    double* pos;            // [N*P] x_0..x_{d-1}, D0
+    double* pos_tmp;        // [N*P] reorder gather target
+    double* F;              // [N*ndim]
+    double* m;              // [N*ndim]
+    double* v;              // [N*ndim]
+    double* vec_tmp;        // [N*ndim] reorder gather target
+    double* x_last;         // [N*ndim] refresh anchor positions
+    std::uint32_t* nbr;     // [S*N] column-major full rows, ascending
+    std::uint32_t* nbr_cnt; // [N]
+    std::uint32_t S;        // row capacity
+    std::uint32_t* caps;    // [N] half-row capacity of the reference layout
+    std::uint64_t* origin;  // [N] particle_origin
+    std::uint64_t* u64_tmp; // [N]
+    std::uint32_t* cell_of;    // [N]
+    std::uint32_t* cell_rank;  // [N]
+    std::uint32_t* cell_count; // [C_alloc + 1]
+    std::uint32_t* cell_start; // [C_alloc + 1]
+    std::uint32_t* cell_list;  // [N]
+    std::uint32_t C_alloc;
+    std::uint32_t* scan_tmp;   // block sums of the scan
+    ForceSums* block_sums;     // [nblocks of the force kernel]
+    PairTerms* pterm;          // [S*N] exact-order pair terms (exact mode only)
+    std::uint32_t* pterm_cnt;  // [N]
+    // radix sort
+    std::uint64_t* sort_keys[2];
+    std::uint32_t* sort_vals[2];
+    std::uint32_t* sort_hist;  // [256 * nblocks]
+    DevCtl* ctl;
+    Histories hist;            // device histories (graph mode)
+};
+
+constexpr int kForceBlock = 256;
+constexpr int kSearchBlock = 128;
+constexpr int kSearchSmemRow = 64;
+
+RCPG_HD unsigned force_blocks(std::uint64_t N) {
+    return static_cast<unsigned>((N + kForceBlock - 1) / kForceBlock);
+}
+
+// ---- launchers (rcpg_kernels.cu) ------------------------------------------
+// All take the device arrays by value and enqueue on `st`.
+void launch_adam_refresh(const DevArrays& a, int do_adam, int do_refresh, cudaStream_t st);
+void launch_rebuild(const DevArrays& a, cudaStream_t st);
+void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st);
+void launch_reduce_exact(const DevArrays& a, cudaStream_t st);
+void launch_reduce_fast(const DevArrays& a, cudaStream_t st);
+void launch_controller(const DevArrays& a, int open_only, cudaStream_t st);
+void launch_reorder(const DevArrays& a, cudaStream_t st);
+void launch_fix_height(const DevArrays& a, cudaStream_t st);
+// Half-row counts of the current full rows (j > i entries) into out[N].
+void launch_half_counts(const DevArrays& a, std::uint32_t* out, cudaStream_t st);
+
+void launch_pack(std::uint64_t N, int ndim, const double* x, const double* D, double* pos,
+                 cudaStream_t st);
+void launch_unpack(std::uint64_t N, int ndim, const double* pos, double* x, cudaStream_t st);
+void launch_refresh_arrays(std::uint64_t N, int ndim, const double* x, double* x_last,
+                           const double* D, double* D_last, double* theta, double theta_new,
+                           std::uint8_t* refresh, unsigned long long* count, cudaStream_t st);
+void launch_mean_force_blocks(const DevArrays& a, cudaStream_t st);
+
+// Host-side finalisation shared with the controller kernel (ENG:4259-4268, :769-803).
+RCPG_HD StepScalars finalize_sums(const ForceSums& s, double mu_eff, int ndim) {
+    StepScalars r;
+    const double count = static_cast<double>(1ull + s.pair_count + s.wall_count);
+    const double U_tot = xadd(s.pair_U, s.wall_U);
+    r.U = pow(xdiv(U_tot, count), 2.0);
+    r.max_overlap = s.pair_maxov;
+    r.Lc = xdiv(s.pair_Lc, count);
+    r.dkappa = xadd(xadd(s.pair_dk, s.wall_dk), xmul(mu_eff, s.sum_D));
+    r.Fmean = xdiv(-xadd(s.pair_Fm, s.wall_Fm), count);
+    const double mean_mag = xdiv(s.sum_mag, static_cast<double>(static_cast<std::uint32_t>(s.mag_count)));
+    r.mean_force = xdiv(mean_mag, xsqrt(static_cast<double>(ndim)));
+    r.count = count;
+    return r;
+}
+
+}  // namespace rcpg

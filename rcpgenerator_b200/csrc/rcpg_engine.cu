@@ -1,0 +1,835 @@
+// Host driver of one packing: the setup of run_packing_observed
+// (python_code/python/src/core/rcp_generator.cpp, "ENG", :4353-5013), then the
+// step loop in one of two modes:
+//   graph mode  -- the controller runs on the GPU (k_controller) and whole
+//                  steps are replayed from a captured CUDA graph; the host
+//                  only intervenes every few dozen steps, at reorders and at
+//                  the end.
+//   exact mode  -- the controller runs on the host with the host libm and
+//                  every force evaluation is reduced in the reference's
+//                  one-thread order, so a run reproduces the reference engine
+//                  at one OpenMP thread step for step.
+#include "rcpg_engine.h"
+#include "rcpg_setup.h"
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace rcpg {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+}  // namespace
+
+void Engine::check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        throw EngineError(-2, std::string("rcpgenerator_b200: CUDA error in ") + what + ": " +
+                                  cudaGetErrorString(e));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// setup (ENG:4353-4990), shared with the host emulation (rcpg_setup.cpp)
+// ---------------------------------------------------------------------------
+void Engine::setup_host(const EngineInput& in) {
+    // the target-phi lock rescales every diameter on the host, so runs that
+    // can lock are host-controlled
+    exact_ = in.exact || in.has_target_phi;
+    graph_steps_ = in.graph_steps > 0 ? in.graph_steps : 32;
+    device_ = in.device;
+    RunSetup s = prepare_run(in);
+    N_ = s.N;
+    ndim_ = s.ndim;
+    host_c_ = s.c;
+    x0_ = std::move(s.x);
+    D0_ = std::move(s.D0);
+    caps_ = std::move(s.caps);
+    walls_ = std::move(s.walls);
+    neighbor_max_ = s.neighbor_max;
+    hist_size_ = host_c_.step_cap + 1;
+}
+
+void Engine::alloc_device() {
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    const std::uint64_t N = N_;
+    const int nd = ndim_;
+    P_ = pos_stride(nd);
+    auto dalloc = [&](std::size_t bytes) -> void* {
+        void* p = nullptr;
+        check(cudaMalloc(&p, bytes < 16 ? 16 : bytes), "cudaMalloc");
+        allocs_.push_back(p);
+        return p;
+    };
+    a_.N = N;
+    a_.ndim = nd;
+    a_.P = P_;
+    a_.pos = static_cast<double*>(dalloc(N * P_ * sizeof(double)));
+    a_.pos_tmp = static_cast<double*>(dalloc(N * P_ * sizeof(double)));
+    a_.F = static_cast<double*>(dalloc(N * nd * sizeof(double)));
+    a_.m = static_cast<double*>(dalloc(N * nd * sizeof(double)));
+    a_.v = static_cast<double*>(dalloc(N * nd * sizeof(double)));
+    a_.vec_tmp = static_cast<double*>(dalloc(N * nd * sizeof(double)));
+    a_.x_last = static_cast<double*>(dalloc(N * nd * sizeof(double)));
+    a_.nbr_cnt = static_cast<std::uint32_t*>(dalloc(N * 4));
+    a_.caps = static_cast<std::uint32_t*>(dalloc(N * 4));
+    a_.origin = static_cast<std::uint64_t*>(dalloc(N * 8));
+    a_.u64_tmp = static_cast<std::uint64_t*>(dalloc(N * 8));
+    a_.cell_of = static_cast<std::uint32_t*>(dalloc(N * 4));
+    a_.cell_rank = static_cast<std::uint32_t*>(dalloc(N * 4));
+    a_.cell_list = static_cast<std::uint32_t*>(dalloc(N * 4));
+    // cell grid capacity: the grid at the initial (smallest) cutoff
+    {
+        const double cutoff = (host_c_.Dmax_cur + host_c_.t_shell) * (1.0 + 1e-6);
+        double cells = 1.0;
+        for (int d = 0; d < nd; ++d) cells *= std::max(1.0, std::floor(host_c_.box[d] / cutoff));
+        double cap = std::min(cells * 1.5 + 64.0, 8.0 * static_cast<double>(N) + 1024.0);
+        cap = std::min(cap, 2.0e9);
+        a_.C_alloc = static_cast<std::uint32_t>(cap);
+    }
+    a_.cell_count = static_cast<std::uint32_t*>(dalloc((a_.C_alloc + 1ull) * 4));
+    a_.cell_start = static_cast<std::uint32_t*>(dalloc((a_.C_alloc + 1ull) * 4));
+    a_.scan_tmp = static_cast<std::uint32_t*>(dalloc(2 * 4096 * 4 + 64));
+    a_.block_sums = static_cast<ForceSums*>(dalloc(force_blocks(N) * sizeof(ForceSums)));
+    a_.pterm_cnt = static_cast<std::uint32_t*>(dalloc(N * 4));
+    for (int b = 0; b < 2; ++b) {
+        a_.sort_keys[b] = static_cast<std::uint64_t*>(dalloc(N * 8));
+        a_.sort_vals[b] = static_cast<std::uint32_t*>(dalloc(N * 4));
+    }
+    const std::uint64_t tiles = (N + 4095) / 4096;
+    a_.sort_hist = static_cast<std::uint32_t*>(dalloc(256 * tiles * 4 + 64));
+    a_.ctl = static_cast<DevCtl*>(dalloc(sizeof(DevCtl)));
+    // row capacity: grown on demand when a build reports a longer row
+    a_.S = 0;
+    a_.nbr = nullptr;
+    a_.pterm = nullptr;
+    ensure_row_capacity(nd == 2 ? 24u : (nd == 3 ? 48u : 96u));
+    histories_on_device_ = !exact_;
+    if (histories_on_device_) {
+        const std::size_t hs = hist_size_;
+        a_.hist.phi = static_cast<double*>(dalloc(hs * 8));
+        a_.hist.force = static_cast<double*>(dalloc(hs * 8));
+        a_.hist.energy = static_cast<double*>(dalloc(hs * 8));
+        a_.hist.max_overlap = static_cast<double*>(dalloc(hs * 8));
+        a_.hist.mu = static_cast<double*>(dalloc(hs * 8));
+        a_.hist.alpha = static_cast<double*>(dalloc(hs * 8));
+        a_.hist.mu_flag = static_cast<std::int8_t*>(dalloc(hs));
+        check(cudaMemsetAsync(a_.hist.phi, 0, hs * 8, st_), "memset");
+        check(cudaMemsetAsync(a_.hist.force, 0, hs * 8, st_), "memset");
+        check(cudaMemsetAsync(a_.hist.energy, 0, hs * 8, st_), "memset");
+        check(cudaMemsetAsync(a_.hist.max_overlap, 0, hs * 8, st_), "memset");
+        check(cudaMemsetAsync(a_.hist.mu, 0, hs * 8, st_), "memset");
+        check(cudaMemsetAsync(a_.hist.alpha, 0, hs * 8, st_), "memset");
+        check(cudaMemsetAsync(a_.hist.mu_flag, 0, hs, st_), "memset");
+    } else {
+        h_phi_.assign(hist_size_, 0.0);
+        h_force_.assign(hist_size_, 0.0);
+        h_energy_.assign(hist_size_, 0.0);
+        h_maxov_.assign(hist_size_, 0.0);
+        h_mu_.assign(hist_size_, 0.0);
+        h_alpha_.assign(hist_size_, 0.0);
+        h_muflag_.assign(hist_size_, 0);
+        hh_ = Histories{h_phi_.data(), h_force_.data(), h_energy_.data(), h_maxov_.data(),
+                        h_mu_.data(), h_alpha_.data(), h_muflag_.data()};
+    }
+    check(cudaMallocHost(&hctl_pinned_, sizeof(DevCtl)), "cudaMallocHost");
+}
+
+void Engine::ensure_row_capacity(std::uint32_t need) {
+    if (need <= a_.S && a_.nbr) return;
+    std::uint32_t S = std::max<std::uint32_t>(a_.S, 8u);
+    while (S < need) S = S + S / 2 + 8;
+    if (static_cast<std::uint64_t>(S) > N_) S = static_cast<std::uint32_t>(std::max<std::uint64_t>(N_, 1));
+    if (S < need) S = need;
+    auto drop = [&](void* p) {
+        if (!p) return;
+        cudaFree(p);
+        allocs_.erase(std::remove(allocs_.begin(), allocs_.end(), p), allocs_.end());
+    };
+    drop(a_.nbr);
+    drop(a_.pterm);
+    a_.nbr = nullptr;
+    a_.pterm = nullptr;
+    void* p = nullptr;
+    check(cudaMalloc(&p, static_cast<std::size_t>(S) * N_ * 4), "cudaMalloc(nbr)");
+    allocs_.push_back(p);
+    a_.nbr = static_cast<std::uint32_t*>(p);
+    if (exact_) {
+        check(cudaMalloc(&p, static_cast<std::size_t>(S) * N_ * sizeof(PairTerms)), "cudaMalloc(pterm)");
+        allocs_.push_back(p);
+        a_.pterm = static_cast<PairTerms*>(p);
+    }
+    a_.S = S;
+    destroy_graph();
+}
+
+void Engine::free_device() {
+    destroy_graph();
+    for (void* p : allocs_) cudaFree(p);
+    allocs_.clear();
+    if (hctl_pinned_) cudaFreeHost(hctl_pinned_);
+    hctl_pinned_ = nullptr;
+}
+
+void Engine::push_ctl() {
+    *hctl_pinned_ = hctl_;
+    check(cudaMemcpyAsync(a_.ctl, hctl_pinned_, sizeof(DevCtl), cudaMemcpyHostToDevice, st_), "push ctl");
+    check(cudaStreamSynchronize(st_), "sync");
+}
+
+void Engine::pull_ctl() {
+    check(cudaMemcpyAsync(hctl_pinned_, a_.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, st_), "pull ctl");
+    check(cudaStreamSynchronize(st_), "sync");
+    hctl_ = *hctl_pinned_;
+}
+
+// Parameters of the kernels of the step that begin_step() just opened
+// (the host twin of the tail of k_controller).
+void Engine::publish_step_params() {
+    const Controller& c = host_c_;
+    hctl_.c = c;
+    for (int d = 0; d < ndim_; ++d) {
+        hctl_.g.box[d] = c.box[d];
+        hctl_.g.inv_box[d] = 1.0 / c.box[d];
+    }
+    hctl_.refresh_kappa = c.kappa_D;
+    hctl_.force_kappa = c.kappa_D;
+    hctl_.force_mu = c.mu_eff;
+    hctl_.build_kappa = c.kappa_D;
+    hctl_.build_t_shell = c.t_shell;
+    hctl_.build_Dmax = c.Dmax_cur;
+    hctl_.theta = c.theta;
+    if (c.rebuild_mode == REBUILD_FULL) {
+        hctl_.rebuild_flag = 1u;
+    } else {
+        hctl_.rebuild_flag = 0u;
+        hctl_.kappa_min = std::fmin(hctl_.kappa_min, c.kappa_D);
+    }
+}
+
+void Engine::upload_initial() {
+    const std::uint64_t N = N_;
+    const int nd = ndim_;
+    std::vector<double> pos(N * P_, 0.0);
+    for (std::uint64_t i = 0; i < N; ++i) {
+        for (int d = 0; d < nd; ++d) pos[i * P_ + d] = x0_[i * nd + d];
+        pos[i * P_ + nd] = D0_[i];
+    }
+    std::vector<std::uint64_t> origin(N);
+    std::iota(origin.begin(), origin.end(), 0ull);
+    check(cudaMemcpyAsync(a_.pos, pos.data(), pos.size() * 8, cudaMemcpyHostToDevice, st_), "H2D pos");
+    check(cudaMemcpyAsync(a_.origin, origin.data(), N * 8, cudaMemcpyHostToDevice, st_), "H2D origin");
+    check(cudaMemcpyAsync(a_.caps, caps_.data(), N * 4, cudaMemcpyHostToDevice, st_), "H2D caps");
+    check(cudaMemsetAsync(a_.m, 0, N * nd * 8, st_), "memset m");
+    check(cudaMemsetAsync(a_.v, 0, N * nd * 8, st_), "memset v");
+    check(cudaMemsetAsync(a_.F, 0, N * nd * 8, st_), "memset F");
+    check(cudaStreamSynchronize(st_), "sync");
+
+    std::memset(&hctl_, 0, sizeof(hctl_));
+    Geometry& g = hctl_.g;
+    g.ndim = nd;
+    g.circle_k = walls_[0] < 0 ? -walls_[0] : 0;
+    g.any_flat_wall = 0;
+    for (int d = 0; d < nd; ++d) {
+        g.walls[d] = walls_[d];
+        if (walls_[d] == 1) g.any_flat_wall = 1;
+        g.box[d] = host_c_.box[d];
+        g.inv_box[d] = 1.0 / host_c_.box[d];
+    }
+    hctl_.c = host_c_;
+    hctl_.fix_height_scale = 1.0;
+    hctl_.build_kappa = 1.0;
+    hctl_.build_t_shell = host_c_.t_shell;
+    hctl_.build_Dmax = host_c_.Dmax_cur;
+    hctl_.refresh_kappa = 1.0;
+    hctl_.kappa_min = 1.0;
+    hctl_.theta = host_c_.theta;
+    hctl_.force_kappa = 1.0;
+    hctl_.force_mu = host_c_.mu;
+    hctl_.rebuild_flag = 1u;
+    push_ctl();
+
+    // initial spatial reorder + full build (ENG:4992-5009), initial forces (ENG:5011-5013)
+    if (host_c_.reorder_interval > 0) {
+        launch_reorder(a_, st_);
+        launches_ += 3 + 8 * 4 + 3;
+    }
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        launch_rebuild(a_, st_);
+        launches_ += 7;
+        forces_and_reduce(exact_);
+        pull_ctl();
+        if (hctl_.cap_error) break;
+        if (hctl_.row_need <= a_.S) break;
+        ensure_row_capacity(hctl_.row_need);
+        hctl_.rebuild_flag = 1u;
+        push_ctl();
+    }
+    if (hctl_.cap_error) {
+        throw EngineError(-ENOSPC, std::string("rcpgenerator: particle ") +
+                                       std::to_string(hctl_.cap_error_particle) +
+                                       " exceeded its neighbor capacity (" +
+                                       std::to_string(hctl_.cap_error_cap) +
+                                       " slots) during pair-list construction (kdtree own-write). "
+                                       "This usually means the per-particle neighbor allocation is too small for the size ratio in this packing. "
+                                       "Recommendation: pass a larger neighbor_max (the per-particle base; e.g. neighbor_max=1500 -- capacity scales as 50*(D_i/D_min)^omega + neighbor_max), or reduce the size ratio.");
+    }
+    const StepScalars s0 = finalize_sums(hctl_.sums, host_c_.mu, ndim_);
+    initial_U_ = s0.U;
+    initial_maxov_ = s0.max_overlap;
+    host_c_.U = s0.U;
+    host_c_.max_min_dist = s0.max_overlap;
+    hctl_.rebuild_flag = 0u;
+    hctl_.c = host_c_;
+    push_ctl();
+}
+
+Engine::Engine(const EngineInput& in, cudaStream_t stream) {
+    setup_host(in);
+    check(cudaSetDevice(in.device), "cudaSetDevice");
+    if (stream) {
+        st_ = stream;
+    } else {
+        check(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
+        own_stream_ = true;
+    }
+    try {
+        alloc_device();
+        upload_initial();
+    } catch (...) {
+        free_device();
+        if (own_stream_) cudaStreamDestroy(st_);
+        throw;
+    }
+}
+
+Engine::~Engine() {
+    cudaSetDevice(device_);
+    free_device();
+    if (own_stream_ && st_) cudaStreamDestroy(st_);
+}
+
+std::uint64_t Engine::builds() {
+    pull_ctl();
+    return hctl_.nbuilds;
+}
+
+void Engine::forces_and_reduce(bool exact_reduce) {
+    launch_forces(a_, exact_reduce ? 1 : 0, st_);
+    if (exact_reduce) launch_reduce_exact(a_, st_);
+    else launch_reduce_fast(a_, st_);
+    launches_ += 2;
+}
+
+// Reorder of the step that begin_step() opened: permutes with the positions
+// after the previous step and rebuilds with the previous diameters (ENG:4850-4948).
+void Engine::do_reorder_and_rebuild() {
+    const Controller& c = host_c_;
+    const double kp = c.runtime_fix_diameter ? 1.0 : c.kappa_D_prev;
+    hctl_.build_kappa = kp;
+    hctl_.build_t_shell = shell_of(xmul(c.D0_min, kp), xmul(c.D0_med, kp), xmul(c.D0_max, kp));
+    hctl_.build_Dmax = xmul(c.D0_max, kp);
+    hctl_.rebuild_flag = 1u;
+    hctl_.stopped = 0u;
+    push_ctl();
+    launch_reorder(a_, st_);
+    launches_ += 3 + 8 * 4 + 3;
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        launch_rebuild(a_, st_);
+        launches_ += 7;
+        pull_ctl();
+        if (hctl_.cap_error || hctl_.row_need <= a_.S) break;
+        ensure_row_capacity(hctl_.row_need);
+        hctl_.rebuild_flag = 1u;
+        push_ctl();
+    }
+}
+
+// Target-phi lock (ENG:5783-5832): D0 := D rescaled to the target, kappa := 1.
+void Engine::do_target_lock(std::uint64_t step) {
+    Controller& c = host_c_;
+    const std::uint64_t N = N_;
+    const int nd = ndim_;
+    std::vector<double> pos(N * P_);
+    check(cudaMemcpyAsync(pos.data(), a_.pos, pos.size() * 8, cudaMemcpyDeviceToHost, st_), "D2H pos");
+    check(cudaStreamSynchronize(st_), "sync");
+    std::vector<double> D(N);
+    for (std::uint64_t i = 0; i < N; ++i) D[i] = pos[i * P_ + nd] * c.kappa;
+    std::vector<double> boxv(c.box, c.box + nd);
+    double factor = 1.0;
+    std::vector<double> Dn = scale_diameters_nd(D, c.target_phi * c.phi_modifier, boxv, nd, c.fix_height != 0, &factor);
+    double D0min = Dn[0], D0max = 0.0, S = 0.0;
+    for (std::uint64_t i = 0; i < N; ++i) {
+        if (Dn[i] < D0min) D0min = Dn[i];
+        if (Dn[i] > D0max) D0max = Dn[i];
+        double r = Dn[i] * 0.5, rN = 1.0;
+        for (int k = 0; k < nd; ++k) rN *= r;
+        S += rN;
+        pos[i * P_ + nd] = Dn[i];
+    }
+    std::vector<double> Dm = Dn;
+    std::nth_element(Dm.begin(), Dm.begin() + N / 2, Dm.end());
+    const double D0med = Dm[N / 2];
+    check(cudaMemcpyAsync(a_.pos, pos.data(), pos.size() * 8, cudaMemcpyHostToDevice, st_), "H2D pos");
+    // caps of the new diameters (ENG:5815-5819 recomputes the pair layout)
+    {
+        const double scaling = static_cast<double>(nd) / 3.0;
+        const double omega = 1.0 + static_cast<double>(nd) / 6.0;
+        const double dmin = D0min > 0.0 ? D0min : 1.0;
+        for (std::uint64_t i = 0; i < N; ++i) {
+            const double cap_d = scaling * (50.0 * std::pow(Dn[i] / dmin, omega) + static_cast<double>(neighbor_max_));
+            std::uint32_t cap = static_cast<std::uint32_t>(std::ceil(cap_d));
+            if (static_cast<std::uint64_t>(cap) > N) cap = static_cast<std::uint32_t>(N);
+            caps_[i] = cap;
+        }
+        check(cudaMemcpyAsync(a_.caps, caps_.data(), N * 4, cudaMemcpyHostToDevice, st_), "H2D caps");
+    }
+    finish_lock(c, hh_, step, D0min, D0max, D0med, S);
+    // full rebuild with the new diameters, re-anchor everything
+    hctl_.build_kappa = 1.0;
+    hctl_.build_t_shell = shell_of(D0min, D0med, D0max);
+    hctl_.build_Dmax = D0max;
+    hctl_.rebuild_flag = 1u;
+    push_ctl();
+    launch_rebuild(a_, st_);
+    launches_ += 7;
+}
+
+}  // namespace rcpg
+
+namespace rcpg {
+
+// ---------------------------------------------------------------------------
+// exact mode: one step with the controller on the host
+// ---------------------------------------------------------------------------
+// Returns false when the run has ended (convergence at the top of the step or
+// step cap reached before it).
+bool Engine::step_host() {
+    Controller& c = host_c_;
+    const std::uint64_t step = c.hist_filled + 1;
+    if (step > c.step_cap) return false;
+    begin_step(c, hh_, step);
+    // 1. pending ADAM pass of the previous step (positions after step-1)
+    if (adam_pending_) {
+        hctl_.adam_go = 1u;
+        hctl_.fix_height_scale = 1.0;
+        hctl_.stopped = 0u;
+        hctl_.halted = 0u;
+        push_ctl();
+        launch_adam_refresh(a_, 1, 0, st_);
+        ++launches_;
+        adam_pending_ = false;
+        hctl_.adam_go = 0u;
+    }
+    if (c.done) return false;
+    // 2. reorder at the top of the step, with the previous diameters
+    if (c.reorder) {
+        do_reorder_and_rebuild();
+        if (hctl_.cap_error) pull_ctl();
+    }
+    // 3. fix_height stretch of the last axis (ENG:5758-5764)
+    if (c.fix_height && !c.runtime_fix_diameter) {
+        hctl_.fix_height_scale = c.fix_height_scale;
+        push_ctl();
+        launch_fix_height(a_, st_);
+        ++launches_;
+    }
+    // 4. target-phi lock (rescale + full rebuild), else the refresh decision
+    if (c.lock_now) {
+        do_target_lock(step);
+    }
+    publish_step_params();
+    hctl_.adam_go = 0u;
+    hctl_.stopped = 0u;
+    hctl_.halted = 0u;
+    push_ctl();
+    if (c.rebuild_mode == REBUILD_CHECK) {
+        launch_adam_refresh(a_, 0, 1, st_);
+        ++launches_;
+    }
+    // 5. rebuild (if flagged) + forces + one-thread-order reduction
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        launch_rebuild(a_, st_);
+        launches_ += 7;
+        forces_and_reduce(true);
+        pull_ctl();
+        if (hctl_.cap_error || hctl_.row_need <= a_.S) break;
+        ensure_row_capacity(hctl_.row_need);
+        hctl_.rebuild_flag = 1u;
+        push_ctl();
+    }
+    if (hctl_.cap_error) {
+        throw EngineError(-ENOSPC, std::string("rcpgenerator: particle ") +
+                                       std::to_string(hctl_.cap_error_particle) +
+                                       " exceeded its neighbor capacity (" +
+                                       std::to_string(hctl_.cap_error_cap) +
+                                       " slots) during pair-list construction (kdtree own-write). "
+                                       "This usually means the per-particle neighbor allocation is too small for the size ratio in this packing. "
+                                       "Recommendation: pass a larger neighbor_max (the per-particle base; e.g. neighbor_max=1500 -- capacity scales as 50*(D_i/D_min)^omega + neighbor_max), or reduce the size ratio.");
+    }
+    hctl_.rebuild_flag = 0u;
+    // 6. end of step on the host
+    const StepScalars sc = finalize_sums(hctl_.sums, c.mu_eff, ndim_);
+    hctl_.scal = sc;
+    end_step(c, hh_, sc);
+    for (int d = 0; d < ndim_; ++d) hctl_.adam_box[d] = c.box[d];
+    hctl_.adam_alpha = c.adam_alpha;
+    hctl_.adam_inv_b1 = c.inv_b1;
+    hctl_.adam_inv_b2 = c.inv_b2;
+    adam_pending_ = true;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// graph mode
+// ---------------------------------------------------------------------------
+void Engine::destroy_graph() {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graph_exec_ = nullptr;
+    graph_ = nullptr;
+}
+
+void Engine::capture_graph() {
+    destroy_graph();
+    check(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    for (int k = 0; k < graph_steps_; ++k) {
+        launch_rebuild(a_, st_);
+        launch_forces(a_, 0, st_);
+        launch_controller(a_, 0, st_);
+        launch_adam_refresh(a_, 1, 1, st_);
+    }
+    check(cudaStreamEndCapture(st_, &graph_), "end capture");
+    check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
+    std::size_t nodes = 0;
+    check(cudaGraphGetNodes(graph_, nullptr, &nodes), "graph nodes");
+    graph_nodes_per_step_ = nodes / static_cast<std::uint64_t>(graph_steps_);
+}
+
+// Opening of step 1 (or of the step after a host intervention): the host
+// already ran begin_step(); publish it and run the refresh trigger.
+void Engine::after_stop() {
+    Controller& c = host_c_;
+    const std::uint64_t step = c.steps;
+    if (c.reorder) do_reorder_and_rebuild();
+    if (hctl_.cap_error) return;
+    if (c.fix_height && !c.runtime_fix_diameter && c.fix_height_scale != 1.0 && c.reorder) {
+        // the stretch was deferred past the reorder
+        hctl_.fix_height_scale = c.fix_height_scale;
+        push_ctl();
+        launch_fix_height(a_, st_);
+        ++launches_;
+    }
+    (void)step;
+    publish_step_params();
+    hctl_.adam_go = 0u;
+    hctl_.stopped = 0u;
+    hctl_.halted = 0u;
+    push_ctl();
+    if (c.rebuild_mode == REBUILD_CHECK) {
+        launch_adam_refresh(a_, 0, 1, st_);
+        ++launches_;
+    }
+}
+
+bool Engine::advance_graph(std::uint64_t max_new_steps) {
+    Controller& c = host_c_;
+    const std::uint64_t start = c.hist_filled;
+    if (c.hist_filled == 0 && c.steps == 0) {
+        // step 1 opens on the device like every later step
+        hctl_.c = c;
+        hctl_.stopped = 0u;
+        hctl_.halted = 0u;
+        push_ctl();
+        launch_controller(a_, 1, st_);
+        ++launches_;
+        pull_ctl();
+        c = hctl_.c;
+        if (hctl_.stopped) {
+            if (c.done || c.steps + 1 > c.step_cap) {
+                finished_ = true;
+                return true;
+            }
+            after_stop();
+        } else if (c.rebuild_mode == REBUILD_CHECK) {
+            launch_adam_refresh(a_, 0, 1, st_);
+            ++launches_;
+        }
+    }
+    while (!finished_) {
+        const std::uint64_t done_steps = c.hist_filled - start;
+        if (max_new_steps && done_steps >= max_new_steps) break;
+        const std::uint64_t want = max_new_steps ? max_new_steps - done_steps : ~0ull;
+        if (!graph_exec_) capture_graph();
+        if (want >= static_cast<std::uint64_t>(graph_steps_)) {
+            check(cudaGraphLaunch(graph_exec_, st_), "graph launch");
+            launches_ += graph_nodes_per_step_ * graph_steps_;
+        } else {
+            for (std::uint64_t k = 0; k < want; ++k) {
+                launch_rebuild(a_, st_);
+                launch_forces(a_, 0, st_);
+                launch_controller(a_, 0, st_);
+                launch_adam_refresh(a_, 1, 1, st_);
+                launches_ += graph_nodes_per_step_;
+            }
+        }
+        pull_ctl();
+        c = hctl_.c;
+        if (hctl_.halted) {
+            if (hctl_.cap_error) {
+                throw EngineError(-ENOSPC, std::string("rcpgenerator: particle ") +
+                                               std::to_string(hctl_.cap_error_particle) +
+                                               " exceeded its neighbor capacity (" +
+                                               std::to_string(hctl_.cap_error_cap) +
+                                               " slots) during pair-list construction (kdtree own-write). "
+                                               "This usually means the per-particle neighbor allocation is too small for the size ratio in this packing. "
+                                               "Recommendation: pass a larger neighbor_max (the per-particle base; e.g. neighbor_max=1500 -- capacity scales as 50*(D_i/D_min)^omega + neighbor_max), or reduce the size ratio.");
+            }
+            handle_overflow_and_resume();
+            continue;
+        }
+        if (hctl_.stopped) {
+            if (c.done || c.steps + 1 > c.step_cap || c.hist_filled >= c.step_cap) {
+                if (!c.done && c.hist_filled < c.step_cap) {
+                    // stopped before opening the next step: nothing pending
+                }
+                finished_ = true;
+                break;
+            }
+            after_stop();
+            if (hctl_.cap_error) {
+                pull_ctl();
+                throw EngineError(-ENOSPC, "rcpgenerator: neighbor capacity exceeded during reorder rebuild");
+            }
+        }
+    }
+    return finished_;
+}
+
+// A build found a row longer than the allocated capacity: grow, rebuild and
+// redo the interrupted step from its forces.
+void Engine::handle_overflow_and_resume() {
+    ensure_row_capacity(hctl_.row_need);
+    hctl_.halted = 0u;
+    hctl_.stopped = 0u;
+    hctl_.rebuild_flag = 1u;
+    hctl_.row_need = 0u;
+    push_ctl();
+    launch_rebuild(a_, st_);
+    launch_forces(a_, 0, st_);
+    launch_controller(a_, 0, st_);
+    launch_adam_refresh(a_, 1, 1, st_);
+    launches_ += graph_nodes_per_step_;
+}
+
+bool Engine::advance(std::uint64_t max_new_steps) {
+    if (finished_) return true;
+    if (exact_) {
+        std::uint64_t n = 0;
+        while (!max_new_steps || n < max_new_steps) {
+            if (!step_host()) {
+                finished_ = true;
+                break;
+            }
+            ++n;
+        }
+        if (finished_ && adam_pending_) {
+            hctl_.adam_go = 1u;
+            hctl_.fix_height_scale = 1.0;
+            push_ctl();
+            launch_adam_refresh(a_, 1, 0, st_);
+            ++launches_;
+            adam_pending_ = false;
+            hctl_.adam_go = 0u;
+        }
+        return finished_;
+    }
+    return advance_graph(max_new_steps);
+}
+
+void Engine::download_histories() {
+    if (!histories_on_device_) return;
+    const std::size_t n = host_c_.hist_filled;
+    h_phi_.assign(n, 0.0);
+    h_force_.assign(n, 0.0);
+    h_energy_.assign(n, 0.0);
+    h_maxov_.assign(n, 0.0);
+    h_mu_.assign(n, 0.0);
+    h_alpha_.assign(n, 0.0);
+    h_muflag_.assign(n, 0);
+    if (n) {
+        check(cudaMemcpyAsync(h_phi_.data(), a_.hist.phi, n * 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaMemcpyAsync(h_force_.data(), a_.hist.force, n * 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaMemcpyAsync(h_energy_.data(), a_.hist.energy, n * 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaMemcpyAsync(h_maxov_.data(), a_.hist.max_overlap, n * 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaMemcpyAsync(h_mu_.data(), a_.hist.mu, n * 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaMemcpyAsync(h_alpha_.data(), a_.hist.alpha, n * 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaMemcpyAsync(h_muflag_.data(), a_.hist.mu_flag, n, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaStreamSynchronize(st_), "sync");
+    }
+}
+
+EngineResult Engine::result() {
+    if (exact_ && adam_pending_) {
+        hctl_.adam_go = 1u;
+        hctl_.fix_height_scale = 1.0;
+        push_ctl();
+        launch_adam_refresh(a_, 1, 0, st_);
+        ++launches_;
+        adam_pending_ = false;
+        hctl_.adam_go = 0u;
+    }
+    if (!exact_) {
+        pull_ctl();
+        host_c_ = hctl_.c;
+    }
+    const Controller& c = host_c_;
+    const std::uint64_t N = N_;
+    const int nd = ndim_;
+    EngineResult r;
+    std::vector<double> pos(N * P_);
+    r.particle_origin.resize(N);
+    check(cudaMemcpyAsync(pos.data(), a_.pos, pos.size() * 8, cudaMemcpyDeviceToHost, st_), "D2H pos");
+    check(cudaMemcpyAsync(r.particle_origin.data(), a_.origin, N * 8, cudaMemcpyDeviceToHost, st_), "D2H origin");
+    check(cudaStreamSynchronize(st_), "sync");
+    r.positions.resize(N * nd);
+    r.diameters.resize(N);
+    // diameters of the last diameter update: D = D0*kappa (ENG:5733)
+    const double kd = c.runtime_fix_diameter ? 1.0 : c.kappa_D;
+    for (std::uint64_t i = 0; i < N; ++i) {
+        for (int d = 0; d < nd; ++d) r.positions[i * nd + d] = pos[i * P_ + d];
+        r.diameters[i] = c.runtime_fix_diameter ? pos[i * P_ + nd] : pos[i * P_ + nd] * kd;
+    }
+    r.box.assign(c.box, c.box + nd);
+    r.walls = walls_;
+    download_histories();
+    const std::size_t n = c.hist_filled;
+    r.phi_history.assign(h_phi_.begin(), h_phi_.begin() + n);
+    r.force_history.assign(h_force_.begin(), h_force_.begin() + n);
+    r.energy_history.assign(h_energy_.begin(), h_energy_.begin() + n);
+    r.max_overlap_history.assign(h_maxov_.begin(), h_maxov_.begin() + n);
+    r.mu_history.assign(h_mu_.begin(), h_mu_.begin() + n);
+    r.alpha_history.assign(h_alpha_.begin(), h_alpha_.begin() + n);
+    r.mu_flag_history.assign(h_muflag_.begin(), h_muflag_.begin() + n);
+    r.steps = n;
+    r.phi = c.phi;
+    r.max_min_dist = c.max_min_dist;
+    r.force_magnitude = c.F_magnitude;
+    pull_ctl();
+    r.builds = hctl_.nbuilds;
+    r.row_capacity = a_.S;
+    return r;
+}
+
+void Engine::observe(std::uint64_t step, bool capture, const ObserverFn& observer,
+                     std::vector<TraceSample>* trace) {
+    double vals[4] = {0, 0, 0, 0};
+    if (step == 0) {
+        vals[0] = host_c_.phi;  // setup phi (already divided by phi_modifier, ENG:4505)
+        vals[1] = 0.0;
+        vals[2] = initial_U_;
+        vals[3] = initial_maxov_;
+    } else if (histories_on_device_) {
+        check(cudaMemcpyAsync(&vals[0], a_.hist.phi + step - 1, 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaMemcpyAsync(&vals[1], a_.hist.force + step - 1, 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaMemcpyAsync(&vals[2], a_.hist.energy + step - 1, 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaMemcpyAsync(&vals[3], a_.hist.max_overlap + step - 1, 8, cudaMemcpyDeviceToHost, st_), "D2H");
+        check(cudaStreamSynchronize(st_), "sync");
+    } else {
+        vals[0] = h_phi_[step - 1];
+        vals[1] = h_force_[step - 1];
+        vals[2] = h_energy_[step - 1];
+        vals[3] = h_maxov_[step - 1];
+    }
+    Observation ob{step, vals[0], vals[1], vals[2], vals[3]};
+    std::vector<double> xs;
+    if (capture) {
+        if (exact_ && adam_pending_) {
+            hctl_.adam_go = 1u;
+            hctl_.fix_height_scale = 1.0;
+            push_ctl();
+            launch_adam_refresh(a_, 1, 0, st_);
+            ++launches_;
+            adam_pending_ = false;
+            hctl_.adam_go = 0u;
+        }
+        std::vector<double> pos(N_ * P_);
+        check(cudaMemcpyAsync(pos.data(), a_.pos, pos.size() * 8, cudaMemcpyDeviceToHost, st_), "D2H pos");
+        check(cudaStreamSynchronize(st_), "sync");
+        xs.resize(N_ * ndim_);
+        TraceSample ts;
+        ts.step = step;
+        ts.diameters.resize(N_);
+        double kd = host_c_.kappa_D;
+        if (!exact_ && step > 0) {
+            pull_ctl();
+            kd = hctl_.c.kappa_D_prev;
+        }
+        if (host_c_.runtime_fix_diameter) kd = 1.0;
+        for (std::uint64_t i = 0; i < N_; ++i) {
+            for (int d = 0; d < ndim_; ++d) xs[i * ndim_ + d] = pos[i * P_ + d];
+            ts.diameters[i] = pos[i * P_ + ndim_] * kd;
+        }
+        ts.positions = xs;
+        ts.phi = ob.phi;
+        ts.force = ob.force_magnitude;
+        ts.energy = ob.energy;
+        ts.max_min_dist = ob.max_min_dist;
+        if (trace) trace->push_back(std::move(ts));
+    }
+    if (observer) observer(ob, capture ? &xs : nullptr);
+}
+
+void Engine::run(std::uint64_t progress_interval, bool capture_positions,
+                 std::uint64_t trajectory_interval, const ObserverFn& observer,
+                 std::vector<TraceSample>* trace) {
+    const bool want_obs = observer && progress_interval > 0;
+    const bool want_cap = capture_positions && trajectory_interval > 0;
+    if (want_obs || want_cap) observe(0, want_cap, observer, trace);
+    if (!want_obs && !want_cap) {
+        advance(0);
+    } else {
+        std::uint64_t every = 0;
+        if (want_obs) every = progress_interval;
+        if (want_cap) every = every ? std::gcd(every, trajectory_interval) : trajectory_interval;
+        while (!finished_) {
+            const std::uint64_t s0 = steps_done();
+            const std::uint64_t next = (s0 / every + 1) * every;
+            advance(next - s0);
+            const std::uint64_t s = steps_done();
+            if (s == next && s > 0) {
+                const bool rep = want_obs && (s % progress_interval == 0);
+                const bool cap = want_cap && (s % trajectory_interval == 0);
+                if (rep || cap) observe(s, cap, rep ? observer : ObserverFn(), trace);
+            }
+        }
+    }
+    // final sample when the last step was not already recorded (ENG:6736-6762)
+    const std::uint64_t last = host_c_.steps;
+    const bool final_cap = want_cap && last > 0 && (last % trajectory_interval == 0);
+    const bool final_rep = want_obs && last > 0 && (last % progress_interval == 0);
+    if ((capture_positions && !final_cap) || (observer && !final_rep)) {
+        EngineResult r = result();
+        if (trace && capture_positions) {
+            TraceSample ts;
+            ts.step = last;
+            ts.positions = r.positions;
+            ts.diameters = r.diameters;
+            ts.phi = r.phi;
+            ts.force = r.force_magnitude;
+            ts.energy = host_c_.U;
+            ts.max_min_dist = r.max_min_dist;
+            trace->push_back(std::move(ts));
+        }
+        if (observer) {
+            Observation ob{last, r.phi, r.force_magnitude, host_c_.U, r.max_min_dist};
+            observer(ob, capture_positions ? &r.positions : nullptr);
+        }
+    }
+}
+
+}  // namespace rcpg

@@ -1,0 +1,144 @@
+// Host driver of one packing on one GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "rcpg_device.h"
+#include "rcpg_setup.h"
+
+namespace rcpg {
+
+struct Observation {
+    std::uint64_t step;
+    double phi, force_magnitude, energy, max_min_dist;
+};
+
+// PackingResult (rcp_generator.hpp:35-90) minus the research-only fields.
+struct EngineResult {
+    std::vector<double> positions;  // [N*ndim]
+    std::vector<double> diameters;
+    std::vector<double> box;
+    std::vector<std::int8_t> walls;
+    std::vector<double> phi_history, force_history, energy_history, max_overlap_history,
+        mu_history, alpha_history;
+    std::vector<std::int8_t> mu_flag_history;
+    std::uint64_t steps = 0;
+    double phi = 0.0, max_min_dist = 0.0, force_magnitude = 0.0;
+    std::vector<std::uint64_t> particle_origin;
+    // engine statistics
+    std::uint64_t builds = 0;
+    std::uint32_t row_capacity = 0;
+};
+
+struct TraceSample {
+    std::uint64_t step;
+    std::vector<double> positions;  // [N*ndim]
+    std::vector<double> diameters;
+    double phi, force, energy, max_min_dist;
+};
+
+using ObserverFn = std::function<void(const Observation&, const std::vector<double>* positions)>;
+
+class EngineError : public std::runtime_error {
+   public:
+    EngineError(int code, const std::string& msg) : std::runtime_error(msg), code_(code) {}
+    int code() const { return code_; }
+
+   private:
+    int code_;
+};
+
+class Engine {
+   public:
+    explicit Engine(const EngineInput& in, cudaStream_t stream = nullptr);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // Advance by at most max_new_steps steps (0 = to completion). Returns
+    // true once the run is finished (converged or step cap).
+    bool advance(std::uint64_t max_new_steps);
+    // Run to completion with optional observation / trajectory capture.
+    void run(std::uint64_t progress_interval, bool capture_positions,
+             std::uint64_t trajectory_interval, const ObserverFn& observer,
+             std::vector<TraceSample>* trace);
+    EngineResult result();
+    std::uint64_t steps_done() const { return host_c_.hist_filled; }
+    bool finished() const { return finished_; }
+    cudaStream_t stream() const { return st_; }
+    std::uint64_t N() const { return N_; }
+    int ndim() const { return ndim_; }
+    // Kernel launches issued so far by this engine (the graph counts per node).
+    std::uint64_t launches() const { return launches_; }
+    std::uint64_t builds();
+
+   private:
+    void setup_host(const EngineInput& in);
+    void alloc_device();
+    void free_device();
+    void upload_initial();
+    void ensure_row_capacity(std::uint32_t need);
+    void push_ctl();
+    void pull_ctl();
+    void publish_step_params();
+    void do_reorder_and_rebuild();
+    void do_target_lock(std::uint64_t step);
+    void forces_and_reduce(bool exact_reduce);
+    void finish_step_host();
+    bool step_host();
+    bool advance_graph(std::uint64_t max_new_steps);
+    void capture_graph();
+    void destroy_graph();
+    void handle_overflow_and_resume();
+    void after_stop();
+    void observe(std::uint64_t step, bool capture, const ObserverFn& observer,
+                 std::vector<TraceSample>* trace);
+    void download_histories();
+    void check(cudaError_t e, const char* what);
+
+    // configuration
+    std::uint64_t N_ = 0;
+    int ndim_ = 0;
+    int P_ = 0;
+    bool exact_ = false;
+    int graph_steps_ = 32;
+    int device_ = 0;
+    cudaStream_t st_ = nullptr;
+    bool own_stream_ = false;
+    std::uint32_t neighbor_max_ = 0;
+
+    // host copies
+    std::vector<double> x0_;          // initial positions (after setup scaling)
+    std::vector<double> D0_;          // D0 after setup
+    std::vector<std::uint32_t> caps_;
+    std::vector<std::int8_t> walls_;
+    Controller host_c_{};
+    DevCtl hctl_{};
+    std::vector<double> h_phi_, h_force_, h_energy_, h_maxov_, h_mu_, h_alpha_;
+    std::vector<std::int8_t> h_muflag_;
+    Histories hh_{};
+    std::uint64_t hist_size_ = 0;
+    bool histories_on_device_ = false;
+    bool finished_ = false;
+    bool adam_pending_ = false;   // exact mode: ADAM pass of the last finished step not yet applied
+    std::uint64_t launches_ = 0;
+    double initial_U_ = 0.0, initial_maxov_ = 0.0;
+
+    // device
+    DevArrays a_{};
+    void* d_block_ = nullptr;
+    std::vector<void*> allocs_;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    cudaGraph_t graph_ = nullptr;
+    std::uint64_t graph_nodes_per_step_ = 0;
+    std::uint32_t* pinned_ = nullptr;
+    DevCtl* hctl_pinned_ = nullptr;
+};
+
+}  // namespace rcpg

@@ -1,0 +1,946 @@
+// CUDA kernels of the packing step (sm_100a).
+//
+// One thread per particle everywhere except the controller (one warp) and the
+// scans / radix sort. The pair list is a full list (both directions) stored
+// column-major, nbr[k*N + i], each row sorted by partner index, so a warp
+// reading entry k of 32 consecutive rows issues one coalesced 128-byte load,
+// and every particle sums its pair forces in ascending partner order -- the
+// order in which the reference's one-thread loop accumulates them -- without
+// atomics. Pair scalars (energy, dkappa, ...) are counted once per pair, by
+// the lower index.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rcpg_device.h"
+
+namespace rcpg {
+
+namespace {
+
+__device__ __forceinline__ bool ctl_idle(const DevCtl* ctl) {
+    return ctl->stopped != 0u || ctl->halted != 0u;
+}
+
+template <int ND>
+__device__ __forceinline__ void load_pos(const double* __restrict__ pos, std::uint64_t i,
+                                         double* x, double& D0) {
+    constexpr int P = pos_stride(ND);
+    const double2* p2 = reinterpret_cast<const double2*>(pos + i * P);
+#pragma unroll
+    for (int h = 0; h < P / 2; ++h) {
+        const double2 w = p2[h];
+        if (2 * h < ND) x[2 * h] = w.x;
+        else if (2 * h == ND) D0 = w.x;
+        if (2 * h + 1 < ND) x[2 * h + 1] = w.y;
+        else if (2 * h + 1 == ND) D0 = w.y;
+    }
+}
+
+template <int ND>
+__device__ __forceinline__ void store_pos(double* __restrict__ pos, std::uint64_t i,
+                                          const double* x, double D0) {
+    constexpr int P = pos_stride(ND);
+    double2* p2 = reinterpret_cast<double2*>(pos + i * P);
+#pragma unroll
+    for (int h = 0; h < P / 2; ++h) {
+        double2 w;
+        w.x = (2 * h < ND) ? x[2 * h] : ((2 * h == ND) ? D0 : 0.0);
+        w.y = (2 * h + 1 < ND) ? x[2 * h + 1] : ((2 * h + 1 == ND) ? D0 : 0.0);
+        p2[h] = w;
+    }
+}
+
+// Cell coordinate of one axis; the grid cell is at least as wide as the
+// largest pair cutoff, so partners sit in the 3^ndim neighbourhood.
+__device__ __forceinline__ int cell_coord(double x, double scale, int nc) {
+    double s = x * scale;
+    if (!(s > 0.0)) return 0;  // negative, zero or NaN
+    int c = static_cast<int>(s);
+    return c >= nc ? nc - 1 : c;
+}
+
+// ===========================================================================
+// A. ADAM step of the finished step + refresh trigger of the next step
+// ===========================================================================
+template <int ND>
+__global__ void __launch_bounds__(256) k_adam_refresh(DevArrays a, int do_adam, int do_refresh) {
+    const DevCtl* ctl = a.ctl;
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= a.N) return;
+    if (ctl->halted) return;
+    const bool adam = do_adam && ctl->adam_go;
+    const bool refresh = do_refresh && !ctl->stopped && ctl->c.rebuild_mode == REBUILD_CHECK;
+    if (!adam && !refresh) return;
+    double x[ND], D0;
+    load_pos<ND>(a.pos, i, x, D0);
+    if (adam) {
+        const double alpha = ctl->adam_alpha, ib1 = ctl->adam_inv_b1, ib2 = ctl->adam_inv_b2;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const std::uint64_t idx = i * ND + d;
+            double mm = a.m[idx], vv = a.v[idx];
+            x[d] = adam_coord(a.F[idx], mm, vv, x[d], alpha, ib1, ib2, ctl->adam_box[d]);
+            a.m[idx] = mm;
+            a.v[idx] = vv;
+        }
+        if (ctl->fix_height_scale != 1.0) x[ND - 1] = xmul(x[ND - 1], ctl->fix_height_scale);
+        store_pos<ND>(a.pos, i, x, D0);
+    }
+    if (refresh) {
+        double d2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const double dd = xsub(x[d], a.x_last[i * ND + d]);
+            d2 = xadd(d2, xmul(dd, dd));
+        }
+        const double D = xmul(D0, ctl->refresh_kappa);
+        const double D_last = xmul(D0, ctl->kappa_min);
+        if (refresh_trigger(d2, D, D_last, ctl->theta)) a.ctl->rebuild_flag = 1u;
+    }
+}
+
+// ===========================================================================
+// B. pair-list rebuild: grid -> bin -> scan -> scatter -> search
+// ===========================================================================
+__global__ void k_build_prepare(DevArrays a) {
+    DevCtl* ctl = a.ctl;
+    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    const std::uint32_t n = a.C_alloc + 1;
+    for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        a.cell_count[k] = 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int nd = a.ndim;
+        const double cutoff = (ctl->build_Dmax + ctl->build_t_shell) * (1.0 + 1e-6);
+        long long nc[kMaxDim];
+        double total = 1.0;
+        for (int d = 0; d < nd; ++d) {
+            double q = floor(ctl->g.box[d] / cutoff);
+            if (!(q >= 1.0)) q = 1.0;
+            if (q > 1048576.0) q = 1048576.0;
+            nc[d] = static_cast<long long>(q);
+            total *= q;
+        }
+        while (total > static_cast<double>(a.C_alloc)) {
+            int dm = 0;
+            for (int d = 1; d < nd; ++d)
+                if (nc[d] > nc[dm]) dm = d;
+            const long long nn = (nc[dm] * 3) / 4;
+            total = total / static_cast<double>(nc[dm]) * static_cast<double>(nn < 1 ? 1 : nn);
+            nc[dm] = nn < 1 ? 1 : nn;
+        }
+        std::uint32_t cells = 1;
+        for (int d = 0; d < nd; ++d) {
+            ctl->ncell[d] = static_cast<int>(nc[d]);
+            ctl->cell_scale[d] = static_cast<double>(nc[d]) / ctl->g.box[d];
+            cells *= static_cast<std::uint32_t>(nc[d]);
+        }
+        ctl->ncells = cells;
+        // every rebuild re-anchors every particle (x_last is written by k_bin)
+        ctl->kappa_min = ctl->build_kappa;
+        ctl->row_need = 0u;
+        ctl->nbuilds += 1u;
+    }
+}
+
+template <int ND>
+__global__ void __launch_bounds__(256) k_build_bin(DevArrays a) {
+    const DevCtl* ctl = a.ctl;
+    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= a.N) return;
+    double x[ND], D0;
+    load_pos<ND>(a.pos, i, x, D0);
+    std::uint32_t c = 0, mul = 1;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        const int cd = cell_coord(x[d], ctl->cell_scale[d], ctl->ncell[d]);
+        c += static_cast<std::uint32_t>(cd) * mul;
+        mul *= static_cast<std::uint32_t>(ctl->ncell[d]);
+        a.x_last[i * ND + d] = x[d];
+    }
+    a.cell_of[i] = c;
+    a.cell_rank[i] = atomicAdd(&a.cell_count[c], 1u);
+}
+
+// Exclusive scan of n uint32 in tiles of 4096 (1024 threads x 4).
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ std::uint32_t block_exclusive_scan(std::uint32_t v, std::uint32_t* smem,
+                                                              std::uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    std::uint32_t s = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const std::uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+    }
+    if (lane == 31) smem[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        std::uint32_t w = lane < nw ? smem[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const std::uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < nw) smem[lane] = w;
+    }
+    __syncthreads();
+    const std::uint32_t warp_off = warp ? smem[warp - 1] : 0u;
+    total = smem[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return warp_off + s - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_tiles(const std::uint32_t* in, std::uint32_t* out, std::uint32_t n,
+                 std::uint32_t* block_sums, const DevCtl* gate) {
+    if (gate && (ctl_idle(gate) || !gate->rebuild_flag)) return;
+    __shared__ std::uint32_t smem[32];
+    const std::uint64_t base = static_cast<std::uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
+    std::uint32_t v[kScanItems];
+    std::uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0u;
+        sum += v[k];
+    }
+    std::uint32_t total;
+    std::uint32_t off = block_exclusive_scan(sum, smem, total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = off;
+        off += v[k];
+    }
+    if (threadIdx.x == 0 && block_sums) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_add(std::uint32_t* out, std::uint32_t n, const std::uint32_t* block_offsets,
+               const DevCtl* gate) {
+    if (gate && (ctl_idle(gate) || !gate->rebuild_flag)) return;
+    const std::uint32_t add = block_offsets[blockIdx.x];
+    const std::uint64_t base = static_cast<std::uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < n) out[base + k] += add;
+}
+
+// Exclusive scan of n <= kScanTile^2 values, gated on a rebuild when gate != null.
+void scan_exclusive(const std::uint32_t* in, std::uint32_t* out, std::uint32_t n,
+                    std::uint32_t* tmp, const DevCtl* gate, cudaStream_t st) {
+    const std::uint32_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles <= 1) {
+        k_scan_tiles<<<1, kScanThreads, 0, st>>>(in, out, n, nullptr, gate);
+        return;
+    }
+    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(in, out, n, tmp, gate);
+    k_scan_tiles<<<1, kScanThreads, 0, st>>>(tmp, tmp + kScanTile, tiles, nullptr, gate);
+    k_scan_add<<<tiles, kScanThreads, 0, st>>>(out, n, tmp + kScanTile, gate);
+}
+
+__global__ void __launch_bounds__(256) k_build_scatter(DevArrays a) {
+    const DevCtl* ctl = a.ctl;
+    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= a.N) return;
+    a.cell_list[a.cell_start[a.cell_of[i]] + a.cell_rank[i]] = static_cast<std::uint32_t>(i);
+}
+
+// Neighbour rows: every j != i in the 3^ndim cell neighbourhood passing the
+// reference's shell test, sorted ascending. Rows are gathered in shared
+// memory (kSearchSmemRow per thread, bank = lane), longer rows continue in
+// the global row and are sorted there.
+template <int ND>
+__global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
+    DevCtl* ctl = a.ctl;
+    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    __shared__ std::uint32_t buf[kSearchSmemRow * kSearchBlock];
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= a.N) return;
+    const std::uint64_t N = a.N;
+    const std::uint32_t S = a.S;
+    const Geometry& g = ctl->g;
+    const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
+    double xi[ND], D0i;
+    load_pos<ND>(a.pos, i, xi, D0i);
+    const double Di = xmul(D0i, kap);
+    int cc[ND], nn[ND], nc[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        nc[d] = ctl->ncell[d];
+        cc[d] = cell_coord(xi[d], ctl->cell_scale[d], nc[d]);
+        nn[d] = nc[d] < 3 ? nc[d] : 3;  // distinct neighbour cells on this axis
+    }
+    int total_combo = 1;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) total_combo *= nn[d];
+    std::uint32_t n = 0, n_half = 0;
+    std::uint32_t* mine = buf + threadIdx.x;
+    for (int combo = 0; combo < total_combo; ++combo) {
+        int rem = combo;
+        std::uint32_t cell = 0, mul = 1;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const int k = rem % nn[d];
+            rem /= nn[d];
+            int c = (nc[d] >= 3) ? cc[d] - 1 + k : k;
+            if (c < 0) c += nc[d];
+            else if (c >= nc[d]) c -= nc[d];
+            cell += static_cast<std::uint32_t>(c) * mul;
+            mul *= static_cast<std::uint32_t>(nc[d]);
+        }
+        const std::uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
+        for (std::uint32_t q = q0; q < q1; ++q) {
+            const std::uint32_t j = a.cell_list[q];
+            if (j == i) continue;
+            double xj[ND], D0j;
+            load_pos<ND>(a.pos, j, xj, D0j);
+            const double Dj = xmul(D0j, kap);
+            const bool ok = (j > i) ? in_shell<ND>(xi, Di, xj, Dj, g, t_shell)
+                                    : in_shell<ND>(xj, Dj, xi, Di, g, t_shell);
+            if (!ok) continue;
+            if (n < kSearchSmemRow) mine[n * kSearchBlock] = j;
+            else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + i] = j;
+            ++n;
+            if (j > i) ++n_half;
+        }
+    }
+    const std::uint32_t cap = a.caps[i];
+    if (n_half > cap) {
+        if (atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
+            ctl->cap_error_particle = static_cast<std::uint32_t>(i);
+            ctl->cap_error_cap = cap;
+        }
+    }
+    if (n > S) {
+        atomicMax(&ctl->row_need, n);
+        a.nbr_cnt[i] = S;
+        return;
+    }
+    atomicMax(&ctl->row_need, n);
+    a.nbr_cnt[i] = n;
+    if (n <= static_cast<std::uint32_t>(kSearchSmemRow)) {
+        for (std::uint32_t k = 1; k < n; ++k) {
+            const std::uint32_t v = mine[k * kSearchBlock];
+            std::uint32_t p = k;
+            while (p > 0 && mine[(p - 1) * kSearchBlock] > v) {
+                mine[p * kSearchBlock] = mine[(p - 1) * kSearchBlock];
+                --p;
+            }
+            mine[p * kSearchBlock] = v;
+        }
+        for (std::uint32_t k = 0; k < n; ++k) a.nbr[static_cast<std::uint64_t>(k) * N + i] = mine[k * kSearchBlock];
+    } else {
+        for (std::uint32_t k = 0; k < static_cast<std::uint32_t>(kSearchSmemRow); ++k)
+            a.nbr[static_cast<std::uint64_t>(k) * N + i] = mine[k * kSearchBlock];
+        std::uint32_t* row = a.nbr + i;
+        for (std::uint32_t k = 1; k < n; ++k) {
+            const std::uint32_t v = row[static_cast<std::uint64_t>(k) * N];
+            std::uint32_t p = k;
+            while (p > 0 && row[static_cast<std::uint64_t>(p - 1) * N] > v) {
+                row[static_cast<std::uint64_t>(p) * N] = row[static_cast<std::uint64_t>(p - 1) * N];
+                --p;
+            }
+            row[static_cast<std::uint64_t>(p) * N] = v;
+        }
+    }
+}
+
+// ===========================================================================
+// C. forces + walls + per-block sums
+// ===========================================================================
+__device__ __forceinline__ double shfl_down_d(double v, int o) {
+    return __shfl_down_sync(0xffffffffu, v, o);
+}
+
+__device__ __forceinline__ void warp_reduce_sums(ForceSums& s) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s.pair_U = xadd(s.pair_U, shfl_down_d(s.pair_U, o));
+        s.pair_Lc = xadd(s.pair_Lc, shfl_down_d(s.pair_Lc, o));
+        s.pair_dk = xadd(s.pair_dk, shfl_down_d(s.pair_dk, o));
+        s.pair_Fm = xadd(s.pair_Fm, shfl_down_d(s.pair_Fm, o));
+        s.pair_maxov = fmax(s.pair_maxov, shfl_down_d(s.pair_maxov, o));
+        s.wall_U = xadd(s.wall_U, shfl_down_d(s.wall_U, o));
+        s.wall_dk = xadd(s.wall_dk, shfl_down_d(s.wall_dk, o));
+        s.wall_Fm = xadd(s.wall_Fm, shfl_down_d(s.wall_Fm, o));
+        s.sum_mag = xadd(s.sum_mag, shfl_down_d(s.sum_mag, o));
+        s.sum_D = xadd(s.sum_D, shfl_down_d(s.sum_D, o));
+        s.pair_count += __shfl_down_sync(0xffffffffu, s.pair_count, o);
+        s.wall_count += __shfl_down_sync(0xffffffffu, s.wall_count, o);
+        s.mag_count += __shfl_down_sync(0xffffffffu, s.mag_count, o);
+    }
+}
+
+__device__ __forceinline__ void sums_add(ForceSums& a, const ForceSums& b) {
+    a.pair_U = xadd(a.pair_U, b.pair_U);
+    a.pair_Lc = xadd(a.pair_Lc, b.pair_Lc);
+    a.pair_dk = xadd(a.pair_dk, b.pair_dk);
+    a.pair_Fm = xadd(a.pair_Fm, b.pair_Fm);
+    a.pair_maxov = fmax(a.pair_maxov, b.pair_maxov);
+    a.wall_U = xadd(a.wall_U, b.wall_U);
+    a.wall_dk = xadd(a.wall_dk, b.wall_dk);
+    a.wall_Fm = xadd(a.wall_Fm, b.wall_Fm);
+    a.sum_mag = xadd(a.sum_mag, b.sum_mag);
+    a.sum_D = xadd(a.sum_D, b.sum_D);
+    a.pair_count += b.pair_count;
+    a.wall_count += b.wall_count;
+    a.mag_count += b.mag_count;
+}
+
+// Deterministic block reduction (fixed shuffle tree, warps combined in order).
+template <int NT>
+__device__ __forceinline__ void block_reduce_sums(ForceSums& s, ForceSums* smem) {
+    warp_reduce_sums(s);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) smem[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ForceSums t = smem[0];
+#pragma unroll
+        for (int w = 1; w < NT / 32; ++w) sums_add(t, smem[w]);
+        s = t;
+    }
+}
+
+template <int ND>
+__global__ void __launch_bounds__(kForceBlock) k_forces(DevArrays a, int exact_terms) {
+    const DevCtl* ctl = a.ctl;
+    __shared__ ForceSums red[kForceBlock / 32];
+    if (ctl_idle(ctl)) return;
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    const std::uint64_t N = a.N;
+    ForceSums s;
+    sums_zero(s);
+    if (i < N) {
+        const Geometry& g = ctl->g;
+        const double kap = ctl->force_kappa;
+        double xi[ND], D0i;
+        load_pos<ND>(a.pos, i, xi, D0i);
+        const double Di = xmul(D0i, kap);
+        double fi[ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) fi[d] = 0.0;
+        const std::uint32_t n = a.nbr_cnt[i];
+        std::uint32_t nterm = 0;
+        for (std::uint32_t k = 0; k < n; ++k) {
+            const std::uint32_t j = a.nbr[static_cast<std::uint64_t>(k) * N + i];
+            double xj[ND], D0j;
+            load_pos<ND>(a.pos, j, xj, D0j);
+            const double Dj = xmul(D0j, kap);
+            PairTerms pt;
+            if (!pair_force<ND>(xi, Di, xj, Dj, g, fi, pt)) continue;
+            if (j > i) {
+                s.pair_U = xadd(s.pair_U, pt.U);
+                s.pair_Lc = xadd(s.pair_Lc, pt.Lc);
+                s.pair_dk = xadd(s.pair_dk, pt.dk);
+                s.pair_Fm = xadd(s.pair_Fm, pt.Fm);
+                s.pair_maxov = fmax(s.pair_maxov, pt.U);
+                s.pair_count += 1ull;
+                if (exact_terms) {
+                    a.pterm[static_cast<std::uint64_t>(nterm) * N + i] = pt;
+                    ++nterm;
+                }
+            }
+        }
+        if (exact_terms) a.pterm_cnt[i] = nterm;
+        wall_forces<ND>(xi, Di, g, fi, s.wall_U, s.wall_dk, s.wall_Fm, s.wall_count);
+        const double f2 = force_norm2<ND>(fi);
+        if (f2 > 1.0E-16) {
+            s.sum_mag = xsqrt(f2);
+            s.mag_count = 1ull;
+        }
+        s.sum_D = Di;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) a.F[i * ND + d] = fi[d];
+    }
+    block_reduce_sums<kForceBlock>(s, red);
+    if (threadIdx.x == 0) a.block_sums[blockIdx.x] = s;
+}
+
+// ===========================================================================
+// D. reductions and controller
+// ===========================================================================
+// Sums in the one-thread order of the reference: all pair terms row after
+// row, then the wall terms particle after particle (ENG:4086-4257), the
+// diameter sum and the force-magnitude sum in index order (ENG:4262, :785).
+template <int ND>
+__global__ void k_reduce_exact(DevArrays a) {
+    DevCtl* ctl = a.ctl;
+    if (ctl_idle(ctl)) return;
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const std::uint64_t N = a.N;
+    ForceSums s;
+    sums_zero(s);
+    for (std::uint64_t i = 0; i < N; ++i) {
+        const std::uint32_t n = a.pterm_cnt[i];
+        for (std::uint32_t k = 0; k < n; ++k) {
+            const PairTerms pt = a.pterm[static_cast<std::uint64_t>(k) * N + i];
+            s.pair_U = xadd(s.pair_U, pt.U);
+            s.pair_count += 1ull;
+            s.pair_Lc = xadd(s.pair_Lc, pt.Lc);
+            if (pt.U > s.pair_maxov) s.pair_maxov = pt.U;
+            s.pair_dk = xadd(s.pair_dk, pt.dk);
+            s.pair_Fm = xadd(s.pair_Fm, pt.Fm);
+        }
+    }
+    const Geometry& g = ctl->g;
+    const double kap = ctl->force_kappa;
+    for (std::uint64_t i = 0; i < N; ++i) {
+        double xi[ND], D0i, fdummy[ND];
+        load_pos<ND>(a.pos, i, xi, D0i);
+#pragma unroll
+        for (int d = 0; d < ND; ++d) fdummy[d] = 0.0;
+        // wall terms continue the pair chains, as in the reference
+        wall_forces<ND>(xi, xmul(D0i, kap), g, fdummy, s.pair_U, s.pair_dk, s.pair_Fm, s.wall_count);
+    }
+    for (std::uint64_t i = 0; i < N; ++i) {
+        double xi[ND], D0i;
+        load_pos<ND>(a.pos, i, xi, D0i);
+        s.sum_D = xadd(s.sum_D, xmul(D0i, kap));
+    }
+    std::uint32_t mc = 0;
+    for (std::uint64_t i = 0; i < N; ++i) {
+        const double f2 = force_norm2<ND>(a.F + i * ND);
+        if (f2 > 1.0E-16) {
+            s.sum_mag = xadd(s.sum_mag, xsqrt(f2));
+            ++mc;
+        }
+    }
+    s.mag_count = mc;
+    ctl->sums = s;
+}
+
+// Fixed-order reduction of the per-block partial sums by one block.
+__device__ void reduce_blocks(const DevArrays& a, ForceSums* smem, ForceSums& out) {
+    const unsigned nb = force_blocks(a.N);
+    ForceSums s;
+    sums_zero(s);
+    for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) sums_add(s, a.block_sums[b]);
+    block_reduce_sums<256>(s, smem);
+    if (threadIdx.x == 0) out = s;
+}
+
+__global__ void __launch_bounds__(256) k_reduce_fast(DevArrays a) {
+    __shared__ ForceSums red[256 / 32];
+    DevCtl* ctl = a.ctl;
+    if (ctl_idle(ctl)) return;
+    ForceSums s;
+    reduce_blocks(a, red, s);
+    if (threadIdx.x == 0) ctl->sums = s;
+}
+
+// Parameters of the kernels of the step that begin_step() just opened.
+__device__ void publish_step(DevCtl* ctl, const Controller& c, int ndim) {
+    for (int d = 0; d < ndim; ++d) {
+        ctl->g.box[d] = c.box[d];
+        ctl->g.inv_box[d] = 1.0 / c.box[d];
+    }
+    ctl->refresh_kappa = c.kappa_D;
+    ctl->force_kappa = c.kappa_D;
+    ctl->force_mu = c.mu_eff;
+    ctl->build_kappa = c.kappa_D;
+    ctl->build_t_shell = c.t_shell;
+    ctl->build_Dmax = c.Dmax_cur;
+    ctl->theta = c.theta;
+    if (c.rebuild_mode == REBUILD_FULL) {
+        ctl->rebuild_flag = 1u;
+    } else {
+        ctl->rebuild_flag = 0u;
+        ctl->kappa_min = fmin(ctl->kappa_min, c.kappa_D);
+    }
+}
+
+// Graph-mode controller: reduce, finish step s (end_step), open step s+1
+// (begin_step) and publish the parameters of the kernels that follow. With
+// open_only it just opens the next step (the first step of a run).
+__global__ void __launch_bounds__(256) k_controller(DevArrays a, int open_only) {
+    __shared__ ForceSums red[256 / 32];
+    DevCtl* ctl = a.ctl;
+    if (ctl_idle(ctl)) {
+        if (threadIdx.x == 0) ctl->adam_go = 0u;
+        return;
+    }
+    Controller& c = ctl->c;
+    if (!open_only) {
+        ForceSums s;
+        reduce_blocks(a, red, s);
+        if (threadIdx.x != 0) return;
+        ctl->sums = s;
+        // capacity problems of the last build stop the run before its results are used
+        if (ctl->row_need > a.S || ctl->cap_error) {
+            ctl->halted = 1u;
+            ctl->adam_go = 0u;
+            return;
+        }
+        const StepScalars sc = finalize_sums(s, ctl->force_mu, a.ndim);
+        ctl->scal = sc;
+        end_step(c, a.hist, sc);
+        ctl->graph_steps += 1ull;
+        for (int d = 0; d < a.ndim; ++d) ctl->adam_box[d] = c.box[d];
+        ctl->adam_alpha = c.adam_alpha;
+        ctl->adam_inv_b1 = c.inv_b1;
+        ctl->adam_inv_b2 = c.inv_b2;
+        ctl->adam_go = 1u;
+    } else {
+        if (threadIdx.x != 0) return;
+        ctl->adam_go = 0u;
+    }
+    ctl->fix_height_scale = 1.0;
+    if (c.steps + 1 > c.step_cap) {
+        ctl->stopped = 1u;
+        return;
+    }
+    begin_step(c, a.hist, c.steps + 1);
+    // the stretch of a reorder step waits until after the reorder (ENG:5661 < :5758)
+    ctl->fix_height_scale = c.reorder ? 1.0 : c.fix_height_scale;
+    if (c.done || c.reorder || c.lock_now) {
+        ctl->stopped = 1u;
+        return;
+    }
+    publish_step(ctl, c, a.ndim);
+}
+
+// fix_height stretch of the last coordinate without an ADAM step (used when
+// the stretch and the ADAM pass are not fused).
+template <int ND>
+__global__ void k_fix_height(DevArrays a) {
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= a.N) return;
+    const double s = a.ctl->fix_height_scale;
+    double* p = a.pos + i * pos_stride(ND) + (ND - 1);
+    *p = xmul(*p, s);
+}
+
+template <int ND>
+__global__ void k_half_counts(DevArrays a, std::uint32_t* out) {
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= a.N) return;
+    const std::uint32_t n = a.nbr_cnt[i];
+    std::uint32_t h = 0;
+    for (std::uint32_t k = 0; k < n; ++k) h += a.nbr[static_cast<std::uint64_t>(k) * a.N + i] > i;
+    out[i] = h;
+}
+
+// ===========================================================================
+// R. spatial reorder: key -> stable LSD radix sort -> gather
+// ===========================================================================
+template <int ND>
+__global__ void k_reorder_keys(DevArrays a) {
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= a.N) return;
+    double x[ND], D0;
+    load_pos<ND>(a.pos, i, x, D0);
+    std::uint64_t key;
+    if (ND == 3) {
+        const Geometry& g = a.ctl->g;
+        std::uint64_t code = 0;
+#pragma unroll
+        for (int d = 0; d < 3 && d < ND; ++d) {
+            const double scale = (static_cast<double>(1u << 21) - 1.0) / g.box[d];
+            code |= morton_spread21(morton_axis(x[d], g.box[d], scale)) << d;
+        }
+        key = code;
+    } else {
+        key = double_order_key(x[0]);
+    }
+    a.sort_keys[0][i] = key;
+    a.sort_vals[0][i] = static_cast<std::uint32_t>(i);
+}
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+
+// Per-tile digit histogram, digit-major: hist[digit * tiles + tile].
+__global__ void __launch_bounds__(kSortThreads)
+    k_sort_hist(const std::uint64_t* keys, std::uint32_t n, int shift, std::uint32_t* hist,
+                std::uint32_t tiles) {
+    __shared__ std::uint32_t h[256];
+    h[threadIdx.x] = 0u;
+    __syncthreads();
+    const std::uint64_t base = static_cast<std::uint64_t>(blockIdx.x) * kSortTile;
+    for (int k = threadIdx.x; k < kSortTile; k += kSortThreads) {
+        const std::uint64_t idx = base + k;
+        if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 0xFFu], 1u);
+    }
+    __syncthreads();
+    hist[static_cast<std::uint64_t>(threadIdx.x) * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter: elements of a tile are ranked in index order, chunk by
+// chunk of 256 (one per thread), with per-warp match masks.
+__global__ void __launch_bounds__(kSortThreads)
+    k_sort_scatter(const std::uint64_t* keys_in, const std::uint32_t* vals_in, std::uint64_t* keys_out,
+                   std::uint32_t* vals_out, std::uint32_t n, int shift, const std::uint32_t* offsets,
+                   std::uint32_t tiles) {
+    __shared__ std::uint32_t base_d[256];
+    __shared__ std::uint32_t wcnt[kSortThreads / 32][256];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    base_d[threadIdx.x] = offsets[static_cast<std::uint64_t>(threadIdx.x) * tiles + blockIdx.x];
+    const std::uint64_t tile0 = static_cast<std::uint64_t>(blockIdx.x) * kSortTile;
+    for (int chunk = 0; chunk < kSortItems; ++chunk) {
+#pragma unroll
+        for (int w = 0; w < kSortThreads / 32; ++w) wcnt[w][threadIdx.x] = 0u;
+        __syncthreads();
+        const std::uint64_t idx = tile0 + static_cast<std::uint64_t>(chunk) * kSortThreads + threadIdx.x;
+        const bool valid = idx < n;
+        std::uint64_t key = 0;
+        std::uint32_t val = 0, digit = 0xFFFFFFFFu;
+        if (valid) {
+            key = keys_in[idx];
+            val = vals_in[idx];
+            digit = static_cast<std::uint32_t>((key >> shift) & 0xFFu);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, digit);
+        const unsigned lt = (1u << lane) - 1u;
+        const std::uint32_t rank_w = __popc(peers & lt);
+        if (valid && rank_w == 0) wcnt[warp][digit] = __popc(peers);
+        __syncthreads();
+        std::uint32_t before = 0;
+        if (valid) {
+            for (int w = 0; w < warp; ++w) before += wcnt[w][digit];
+            const std::uint32_t pos = base_d[digit] + before + rank_w;
+            keys_out[pos] = key;
+            vals_out[pos] = val;
+        }
+        __syncthreads();
+        // advance the per-digit base by this chunk's count (thread d owns digit d)
+        std::uint32_t tot = 0;
+#pragma unroll
+        for (int w = 0; w < kSortThreads / 32; ++w) tot += wcnt[w][threadIdx.x];
+        base_d[threadIdx.x] += tot;
+        __syncthreads();
+    }
+}
+
+template <int ND>
+__global__ void k_reorder_gather(DevArrays a, const std::uint32_t* perm) {
+    const std::uint64_t k = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (k >= a.N) return;
+    const std::uint64_t src = perm[k];
+    constexpr int P = pos_stride(ND);
+#pragma unroll
+    for (int q = 0; q < P; ++q) a.pos_tmp[k * P + q] = a.pos[src * P + q];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) a.vec_tmp[k * ND + d] = a.m[src * ND + d];
+    a.u64_tmp[k] = a.origin[src];
+    a.cell_rank[k] = a.caps[src];  // cell_rank doubles as scratch here
+}
+
+template <int ND>
+__global__ void k_reorder_gather_v(DevArrays a, const std::uint32_t* perm) {
+    const std::uint64_t k = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (k >= a.N) return;
+    const std::uint64_t src = perm[k];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) a.x_last[k * ND + d] = a.v[src * ND + d];
+}
+
+template <int ND>
+__global__ void k_reorder_commit(DevArrays a) {
+    const std::uint64_t k = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (k >= a.N) return;
+    constexpr int P = pos_stride(ND);
+#pragma unroll
+    for (int q = 0; q < P; ++q) a.pos[k * P + q] = a.pos_tmp[k * P + q];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        a.m[k * ND + d] = a.vec_tmp[k * ND + d];
+        a.v[k * ND + d] = a.x_last[k * ND + d];
+    }
+    a.origin[k] = a.u64_tmp[k];
+    a.caps[k] = a.cell_rank[k];
+}
+
+// ===========================================================================
+// P. layout conversion and stand-alone kernels of the C ABI
+// ===========================================================================
+template <int ND>
+__global__ void k_pack(std::uint64_t N, const double* __restrict__ x, const double* __restrict__ D,
+                       double* __restrict__ pos) {
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= N) return;
+    double xi[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) xi[d] = x[i * ND + d];
+    store_pos<ND>(pos, i, xi, D ? D[i] : 0.0);
+}
+
+template <int ND>
+__global__ void k_unpack(std::uint64_t N, const double* __restrict__ pos, double* __restrict__ x) {
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= N) return;
+    double xi[ND], D0;
+    load_pos<ND>(pos, i, xi, D0);
+#pragma unroll
+    for (int d = 0; d < ND; ++d) x[i * ND + d] = xi[d];
+}
+
+// Per-particle anchors, as the reference keeps them (ENG:6104-6145).
+template <int ND>
+__global__ void k_refresh_arrays(std::uint64_t N, const double* __restrict__ x, double* x_last,
+                                 const double* __restrict__ D, double* D_last, double* theta,
+                                 double theta_new, std::uint8_t* refresh,
+                                 unsigned long long* count) {
+    const std::uint64_t k = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (k >= N) return;
+    double d2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        const double dd = xsub(x[k * ND + d], x_last[k * ND + d]);
+        d2 = xadd(d2, xmul(dd, dd));
+    }
+    double Dl = D_last[k];
+    if (D[k] < Dl) Dl = D[k];
+    double th = theta[k];
+    if (th > theta_new) th = theta_new;
+    std::uint8_t r = 0;
+    if (refresh_trigger(d2, D[k], Dl, th)) {
+        r = 1;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) x_last[k * ND + d] = x[k * ND + d];
+        Dl = D[k];
+        th = theta_new;
+        atomicAdd(count, 1ull);
+    }
+    D_last[k] = Dl;
+    theta[k] = th;
+    refresh[k] = r;
+}
+
+template <int ND>
+__global__ void __launch_bounds__(kForceBlock) k_mean_force_blocks(DevArrays a) {
+    __shared__ ForceSums red[kForceBlock / 32];
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    ForceSums s;
+    sums_zero(s);
+    if (i < a.N) {
+        const double f2 = force_norm2<ND>(a.F + i * ND);
+        if (f2 > 1.0E-16) {
+            s.sum_mag = xsqrt(f2);
+            s.mag_count = 1ull;
+        }
+    }
+    block_reduce_sums<kForceBlock>(s, red);
+    if (threadIdx.x == 0) a.block_sums[blockIdx.x] = s;
+}
+
+template <int ND>
+void reorder_impl(const DevArrays& a, cudaStream_t st) {
+    const unsigned nb = force_blocks(a.N);
+    const std::uint32_t n = static_cast<std::uint32_t>(a.N);
+    k_reorder_keys<ND><<<nb, kForceBlock, 0, st>>>(a);
+    const std::uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    int cur = 0;
+    for (int pass = 0; pass < 8; ++pass) {
+        const int shift = pass * 8;
+        k_sort_hist<<<tiles, kSortThreads, 0, st>>>(a.sort_keys[cur], n, shift, a.sort_hist, tiles);
+        scan_exclusive(a.sort_hist, a.sort_hist, 256u * tiles, a.scan_tmp, nullptr, st);
+        k_sort_scatter<<<tiles, kSortThreads, 0, st>>>(a.sort_keys[cur], a.sort_vals[cur],
+                                                       a.sort_keys[cur ^ 1], a.sort_vals[cur ^ 1], n,
+                                                       shift, a.sort_hist, tiles);
+        cur ^= 1;
+    }
+    const std::uint32_t* perm = a.sort_vals[cur];
+    k_reorder_gather<ND><<<nb, kForceBlock, 0, st>>>(a, perm);
+    k_reorder_gather_v<ND><<<nb, kForceBlock, 0, st>>>(a, perm);
+    k_reorder_commit<ND><<<nb, kForceBlock, 0, st>>>(a);
+}
+
+template <int ND>
+void rebuild_impl(const DevArrays& a, cudaStream_t st) {
+    const unsigned nb = force_blocks(a.N);
+    const unsigned cb = (a.C_alloc + 1 + 255) / 256;
+    k_build_prepare<<<cb < 1024 ? cb : 1024, 256, 0, st>>>(a);
+    k_build_bin<ND><<<nb, kForceBlock, 0, st>>>(a);
+    scan_exclusive(a.cell_count, a.cell_start, a.C_alloc + 1, a.scan_tmp, a.ctl, st);
+    k_build_scatter<<<nb, kForceBlock, 0, st>>>(a);
+    const unsigned sb = static_cast<unsigned>((a.N + kSearchBlock - 1) / kSearchBlock);
+    k_build_search<ND><<<sb, kSearchBlock, 0, st>>>(a);
+}
+
+}  // namespace
+
+#define RCPG_DISPATCH_ND(nd, CALL)                 \
+    switch (nd) {                                  \
+        case 2: { constexpr int ND = 2; CALL; } break; \
+        case 3: { constexpr int ND = 3; CALL; } break; \
+        case 4: { constexpr int ND = 4; CALL; } break; \
+        case 5: { constexpr int ND = 5; CALL; } break; \
+        case 6: { constexpr int ND = 6; CALL; } break; \
+        case 7: { constexpr int ND = 7; CALL; } break; \
+        case 8: { constexpr int ND = 8; CALL; } break; \
+        default: break;                            \
+    }
+
+void launch_adam_refresh(const DevArrays& a, int do_adam, int do_refresh, cudaStream_t st) {
+    const unsigned nb = force_blocks(a.N);
+    RCPG_DISPATCH_ND(a.ndim, (k_adam_refresh<ND><<<nb, kForceBlock, 0, st>>>(a, do_adam, do_refresh)));
+}
+
+void launch_rebuild(const DevArrays& a, cudaStream_t st) {
+    RCPG_DISPATCH_ND(a.ndim, (rebuild_impl<ND>(a, st)));
+}
+
+void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st) {
+    const unsigned nb = force_blocks(a.N);
+    RCPG_DISPATCH_ND(a.ndim, (k_forces<ND><<<nb, kForceBlock, 0, st>>>(a, exact_terms)));
+}
+
+void launch_reduce_exact(const DevArrays& a, cudaStream_t st) {
+    RCPG_DISPATCH_ND(a.ndim, (k_reduce_exact<ND><<<1, 1, 0, st>>>(a)));
+}
+
+void launch_reduce_fast(const DevArrays& a, cudaStream_t st) {
+    k_reduce_fast<<<1, 256, 0, st>>>(a);
+}
+
+void launch_controller(const DevArrays& a, int open_only, cudaStream_t st) {
+    k_controller<<<1, 256, 0, st>>>(a, open_only);
+}
+
+void launch_reorder(const DevArrays& a, cudaStream_t st) {
+    RCPG_DISPATCH_ND(a.ndim, (reorder_impl<ND>(a, st)));
+}
+
+void launch_fix_height(const DevArrays& a, cudaStream_t st) {
+    const unsigned nb = force_blocks(a.N);
+    RCPG_DISPATCH_ND(a.ndim, (k_fix_height<ND><<<nb, kForceBlock, 0, st>>>(a)));
+}
+
+void launch_half_counts(const DevArrays& a, std::uint32_t* out, cudaStream_t st) {
+    const unsigned nb = force_blocks(a.N);
+    RCPG_DISPATCH_ND(a.ndim, (k_half_counts<ND><<<nb, kForceBlock, 0, st>>>(a, out)));
+}
+
+void launch_pack(std::uint64_t N, int ndim, const double* x, const double* D, double* pos,
+                 cudaStream_t st) {
+    const unsigned nb = force_blocks(N);
+    RCPG_DISPATCH_ND(ndim, (k_pack<ND><<<nb, kForceBlock, 0, st>>>(N, x, D, pos)));
+}
+
+void launch_unpack(std::uint64_t N, int ndim, const double* pos, double* x, cudaStream_t st) {
+    const unsigned nb = force_blocks(N);
+    RCPG_DISPATCH_ND(ndim, (k_unpack<ND><<<nb, kForceBlock, 0, st>>>(N, pos, x)));
+}
+
+void launch_refresh_arrays(std::uint64_t N, int ndim, const double* x, double* x_last,
+                           const double* D, double* D_last, double* theta, double theta_new,
+                           std::uint8_t* refresh, unsigned long long* count, cudaStream_t st) {
+    const unsigned nb = force_blocks(N);
+    RCPG_DISPATCH_ND(ndim, (k_refresh_arrays<ND><<<nb, kForceBlock, 0, st>>>(
+                               N, x, x_last, D, D_last, theta, theta_new, refresh, count)));
+}
+
+void launch_mean_force_blocks(const DevArrays& a, cudaStream_t st) {
+    const unsigned nb = force_blocks(a.N);
+    RCPG_DISPATCH_ND(a.ndim, (k_mean_force_blocks<ND><<<nb, kForceBlock, 0, st>>>(a)));
+}
+
+}  // namespace rcpg
