@@ -1,0 +1,285 @@
+"""Throughput of the packing engine on BASELINE config 2.
+
+Workload (one replica per GPU, independent packings, no collective):
+2-D bidisperse disks, N = 1,000,000, diameters 1.0 : 1.4 at 50:50 number
+fraction, periodic unit square, initial phi 0.30, seed 123 (+ rank), placed by
+the engine's initializer (a bit-exact restatement of the reference's
+initialize_particles). One step = one ADAM step of Packing.pack()'s loop:
+refresh trigger, neighbour rebuild when triggered, forces + reductions,
+controller, ADAM + position update. Steps are timed from the start of the
+run (the heavy-overlap early phase the reference is timed on).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "packings/hour and ADAM steps/sec vs plain GPU engine at equal phi_J error"
+UNIT = "ADAM steps/s"
+WORKLOAD = dict(phi=0.30, N=1_000_000, Ndim=2, box=[1.0, 1.0], walls=[0, 0],
+                dist={"type": "bidisperse", "d1": 1.0, "d2": 1.4, "p": 0.5}, seed=123)
+PEAKS = REPO / "MEASURED_PEAKS.json"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def hbm_peak():
+    try:
+        p = json.loads(PEAKS.read_text())
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.flush()
+        rows = [r.split(",") for r in Path(self.out.name).read_text().strip().splitlines() if r.strip()]
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [c.strip() for c in r]
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_input(rank: int):
+    import rcpgenerator_b200 as rb
+    cfg = dict(WORKLOAD)
+    cfg["seed"] = WORKLOAD["seed"] + rank
+    init = rb.initialize_particles(cfg)
+    pos = np.ascontiguousarray(init["positions"], dtype=np.float64)
+    dia = np.ascontiguousarray(init["diameters"], dtype=np.float64)
+    return pos, dia, init
+
+
+def reference_sample(pos, dia, box, walls, steps: int, threads: int):
+    """The reference engine (oracle/_ref, compiled from the reference sources)
+    on the same input, timed per step through its own observer callback."""
+    ref_dir = REPO / "oracle" / "_ref"
+    if not any(ref_dir.glob("_rcpgenerator*.so")):
+        return None, "reference build oracle/_ref missing"
+    sys.path.insert(0, str(ref_dir))
+    for k in list(os.environ):
+        if k.startswith("RCP_"):
+            del os.environ[k]
+    import _rcpgenerator as ref
+    ref.set_num_threads(threads)
+    stamps = []
+
+    def cb(update):
+        stamps.append((int(update["step"]), time.perf_counter()))
+
+    t0 = time.perf_counter()
+    ref.run_packing_observed({"positions": pos.tolist(), "diameters": dia.tolist()},
+                             {"box": box, "walls": walls, "neighbor_max": 0, "seed": 0},
+                             1, False, 0, cb, {"max_steps": steps + 1})
+    t1 = time.perf_counter()
+    st = [t for s, t in stamps if 1 <= s <= steps + 1]
+    if len(st) < 2:
+        return None, "reference produced no step timings"
+    per = (st[-1] - st[0]) / (len(st) - 1)
+    return {"steps_per_s": 1.0 / per, "timed_steps": len(st) - 1, "setup_s": stamps[0][1] - t0
+            if stamps else None, "wall_s": t1 - t0}, None
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    pos, dia, init = make_input(0)
+    threads = os.cpu_count() or 1
+    s, why = reference_sample(pos, dia, init["box"], init["walls"], args.warmup + args.steps, threads)
+    if s is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return 0
+    v = s["steps_per_s"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "bidisperse2d_N1e6_phi0.30_seed123", "N": WORKLOAD["N"], "Ndim": 2,
+                   "engine": "reference C++/OpenMP run_packing_observed, portable build",
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"first {s['timed_steps']} steps after step 1 of config 2 "
+                                   f"(observer timestamps), setup excluded"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=12)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    import rcpgenerator_b200 as rb
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    pos, dia, init = make_input(rank)
+    stream = torch.cuda.Stream()
+    eng = rb.PackingEngine({"positions": pos, "diameters": dia},
+                           {"box": init["box"], "walls": init["walls"], "device": local}, {},
+                           stream=stream.cuda_stream)
+    eng.advance(args.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = eng.kernel_launches
+    s0 = eng.steps
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    eng.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    done_steps = eng.steps - s0
+    launches = eng.kernel_launches - l0
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        if dist.is_initialized():
+            dist.barrier()
+    prof = eng.profile_pair_kernel(reps=max(10, min(args.steps, 100)))
+    res = eng.result(as_arrays=True)
+    eng.close()
+
+    # end to end through the public API: host buffers in, results out
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r2 = rb.run_packing_observed({"positions": pos, "diameters": dia},
+                                 {"box": init["box"], "walls": init["walls"], "device": local},
+                                 0, False, 0, None, {"max_steps": args.steps}, as_arrays=True)["result"]
+    t_e2e = time.perf_counter() - t0
+    e2e_steps = int(r2["steps"])
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+    value = world * done_steps / (ms / 1e3)
+    peak, peak_kind = hbm_peak()
+    achieved = prof["alg_bytes"] / (prof["avg_ms"] / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        s, why = reference_sample(pos, dia, init["box"], init["walls"], args.cpu_sample_steps,
+                                  os.cpu_count() or 1)
+        if s is not None:
+            cpu = {"value": s["steps_per_s"], "unit": UNIT, "cores": os.cpu_count(),
+                   "kind": "reference",
+                   "sample": f"{s['timed_steps']} steps (2..{s['timed_steps'] + 1}) of the same "
+                             f"packing on the reference engine, all host threads"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": why}
+    n, nd = pos.shape
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done_steps,
+        "warmup": args.warmup, "ms_per_step": ms / max(done_steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "bidisperse2d_N1e6_phi0.30_seed123", "N": n, "Ndim": nd,
+                   "engine": "graph", "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (~150 MB touched per step)",
+                   "pair_builds": int(res["engine_stats"]["pair_builds"]),
+                   "row_capacity": int(res["engine_stats"]["row_capacity"])},
+        "roofline": {"bound": "hbm", "kernel": "k_forces (pair energy/gradient, full rows)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None,
+                     "alg_bytes_per_launch": prof["alg_bytes"], "avg_launch_ms": prof["avg_ms"],
+                     "mean_row": prof["mean_row"]},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_steps / t_e2e, "unit": UNIT,
+                "h2d_bytes_per_step": int((n * (nd + 1) * 8) / max(e2e_steps, 1)),
+                "d2h_bytes_per_step": int((n * (nd + 2) * 8 + e2e_steps * 6 * 8) / max(e2e_steps, 1)),
+                "note": "run_packing_observed(max_steps=K) from host NumPy arrays: setup, K steps, results"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

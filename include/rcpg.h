@@ -152,6 +152,13 @@ uint64_t rcpg_engine_steps(const rcpg_engine* e);
 uint64_t rcpg_engine_kernel_launches(const rcpg_engine* e);
 int32_t rcpg_engine_result(rcpg_engine* e, rcpg_result** out, char* err, size_t errlen);
 void rcpg_engine_destroy(rcpg_engine* e);
+/* Engine diagnostics (no reference counterpart): times `reps` launches of the
+ * pair-force kernel on the engine's current state with CUDA events on its
+ * stream; *avg_ms = mean launch time, *alg_bytes = algorithmic bytes of one
+ * launch, *mean_row = mean neighbour-row length. The run state is unchanged. */
+int32_t rcpg_engine_profile_pair_kernel(rcpg_engine* e, uint32_t reps, double* avg_ms,
+                                        double* alg_bytes, double* mean_row, char* err,
+                                        size_t errlen);
 
 /* ---- per-step kernels on device buffers ---------------------------------- */
 

@@ -325,6 +325,16 @@ class PackingEngine:
         finally:
             N.lib.rcpg_result_free(res)
 
+    def profile_pair_kernel(self, reps: int = 20) -> dict:
+        """Mean launch time of the pair-force kernel on the current state and
+        its algorithmic bytes per launch (CUDA events on the engine stream)."""
+        ms, b, row = C.c_double(), C.c_double(), C.c_double()
+        err = N.errbuf()
+        rc = N.lib.rcpg_engine_profile_pair_kernel(self._h, int(reps), C.byref(ms), C.byref(b),
+                                                   C.byref(row), err, len(err))
+        N.raise_for(rc, err)
+        return {"avg_ms": ms.value, "alg_bytes": b.value, "mean_row": row.value}
+
     def close(self) -> None:
         if self._h:
             N.lib.rcpg_engine_destroy(self._h)

@@ -290,6 +290,19 @@ int32_t rcpg_engine_result(rcpg_engine* e, rcpg_result** out, char* err, size_t 
     }
 }
 
+int32_t rcpg_engine_profile_pair_kernel(rcpg_engine* e, uint32_t reps, double* avg_ms,
+                                        double* alg_bytes, double* mean_row, char* err,
+                                        size_t errlen) {
+    if (!e || !avg_ms || !alg_bytes || !mean_row)
+        return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: null argument");
+    try {
+        e->eng->profile_pair_kernel(reps, avg_ms, alg_bytes, mean_row);
+        return RCPG_OK;
+    } catch (const std::exception& ex) {
+        return fail(err, errlen, classify(ex), ex.what());
+    }
+}
+
 void rcpg_engine_destroy(rcpg_engine* e) {
     if (!e) return;
     delete e->eng;

@@ -318,6 +318,40 @@ std::uint64_t Engine::builds() {
     return hctl_.nbuilds;
 }
 
+void Engine::profile_pair_kernel(std::uint32_t reps, double* avg_ms, double* alg_bytes,
+                                 double* mean_row) {
+    pull_ctl();
+    const DevCtl saved = hctl_;
+    hctl_.stopped = 0u;
+    hctl_.halted = 0u;
+    push_ctl();
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    launch_forces(a_, 0, st_);  // warm
+    check(cudaEventRecord(e0, st_), "record");
+    for (std::uint32_t k = 0; k < reps; ++k) launch_forces(a_, 0, st_);
+    check(cudaEventRecord(e1, st_), "record");
+    check(cudaEventSynchronize(e1), "sync");
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    launches_ += reps + 1;
+    std::vector<std::uint32_t> cnt(N_);
+    check(cudaMemcpyAsync(cnt.data(), a_.nbr_cnt, N_ * 4, cudaMemcpyDeviceToHost, st_), "D2H cnt");
+    check(cudaStreamSynchronize(st_), "sync");
+    double total = 0.0;
+    for (std::uint32_t c : cnt) total += c;
+    // per particle: read x_i (8*ndim) + D0_i (8) + row length (4) + row ids (4*k), write F_i (8*ndim)
+    const double bytes = static_cast<double>(N_) * (16.0 * ndim_ + 12.0) + 4.0 * total;
+    *avg_ms = reps ? ms / reps : 0.0;
+    *alg_bytes = bytes;
+    *mean_row = total / static_cast<double>(N_);
+    hctl_ = saved;
+    push_ctl();
+}
+
 void Engine::forces_and_reduce(bool exact_reduce) {
     launch_forces(a_, exact_reduce ? 1 : 0, st_);
     if (exact_reduce) launch_reduce_exact(a_, st_);

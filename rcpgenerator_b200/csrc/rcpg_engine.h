@@ -77,6 +77,11 @@ class Engine {
     // Kernel launches issued so far by this engine (the graph counts per node).
     std::uint64_t launches() const { return launches_; }
     std::uint64_t builds();
+    // Times `reps` back-to-back launches of the pair-force kernel on the
+    // current state (CUDA events on the engine stream); returns the average
+    // duration and the kernel's algorithmic bytes per launch.
+    void profile_pair_kernel(std::uint32_t reps, double* avg_ms, double* alg_bytes,
+                             double* mean_row);
 
    private:
     void setup_host(const EngineInput& in);

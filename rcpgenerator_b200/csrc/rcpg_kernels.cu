@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <stdexcept>
 
 #include "rcpg_device.h"
 
@@ -234,6 +235,7 @@ __global__ void __launch_bounds__(kScanThreads)
 void scan_exclusive(const std::uint32_t* in, std::uint32_t* out, std::uint32_t n,
                     std::uint32_t* tmp, const DevCtl* gate, cudaStream_t st) {
     const std::uint32_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles > static_cast<std::uint32_t>(kScanTile)) throw std::length_error("rcpg scan: more than 4096^2 elements");
     if (tiles <= 1) {
         k_scan_tiles<<<1, kScanThreads, 0, st>>>(in, out, n, nullptr, gate);
         return;

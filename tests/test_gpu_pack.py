@@ -1,0 +1,76 @@
+"""Whole packings on the GPU.
+
+* exact engine: bit-for-bit equal to the reference engine (one OpenMP thread)
+  on the golden packings, including BASELINE config 1 (N=2000 3D, seed 123);
+* graph engine: converges under the reference's own gate, and its first
+  steps agree with the exact engine to 1e-12 relative.
+"""
+
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HIST = ("phi_history", "force_history", "energy_history", "max_overlap_history", "mu_history",
+        "alpha_history")
+CASES = ["n4_2d", "n16_2d", "n64_3d_bi", "n64_2d_walls_500", "n128_3d_sphere_3000",
+         "n200_2d_disk_2500", "n300_4d_1500", "cfg1_n2000_3d"]
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def run(g, case, engine, extra=None):
+    import rcpgenerator_b200 as rb
+    inp = {"positions": g[f"{case}/input_positions"], "diameters": g[f"{case}/input_diameters"]}
+    cfg = {"box": g[f"{case}/box_in"].tolist(), "walls": g[f"{case}/walls_in"].tolist(),
+           "neighbor_max": 0, "engine": engine}
+    opts = {}
+    ms = int(g[f"{case}/max_steps"])
+    if ms:
+        opts["max_steps"] = ms
+    opts.update(extra or {})
+    return rb.run_packing_observed(inp, cfg, 0, False, 0, None, opts, as_arrays=True)["result"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_exact_engine_reproduces_reference(cuda_device, golden, case):
+    g = golden("packs.npz")
+    r = run(g, case, "exact")
+    sc = g[f"{case}/scalars"]
+    assert r["steps"] == int(sc[0])
+    assert r["phi"] == sc[1]
+    assert r["max_min_dist"] == sc[2]
+    assert np.array_equal(r["positions"], g[f"{case}/positions"])
+    assert np.array_equal(r["diameters"], g[f"{case}/diameters"])
+    assert np.array_equal(r["particle_origin"], g[f"{case}/particle_origin"])
+    for h in HIST:
+        assert digest(r[h]) == str(g[f"{case}/{h}_sha256"]), h
+
+
+@pytest.mark.parametrize("case", ["n16_2d", "n64_3d_bi", "cfg1_n2000_3d"])
+def test_graph_engine_converges(cuda_device, golden, case):
+    g = golden("packs.npz")
+    r = run(g, case, "graph")
+    ref_steps, ref_phi = int(g[f"{case}/scalars"][0]), g[f"{case}/scalars"][1]
+    assert np.isfinite(r["positions"]).all()
+    assert r["steps"] > 0.8 * ref_steps and r["steps"] < 1.2 * ref_steps
+    assert r["max_min_dist"] < 5e-4  # the reference's DONE gate
+    assert abs(r["phi"] - ref_phi) < 0.02
+    assert len(r["phi_history"]) == r["steps"]
+
+
+def test_graph_engine_tracks_exact_engine(cuda_device, golden):
+    g = golden("packs.npz")
+    case = "cfg1_n2000_3d"
+    a = run(g, case, "exact", {"max_steps": 60})
+    b = run(g, case, "graph", {"max_steps": 60})
+    assert a["steps"] == b["steps"] == 60
+    rel = np.abs(a["positions"] - b["positions"]).max()
+    assert rel < 1e-12
+    assert np.abs(a["phi_history"] - b["phi_history"]).max() <= 1e-12 * a["phi_history"].max()
