@@ -340,14 +340,18 @@ int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const dou
         a.ndim = ndim;
         a.P = P;
         a.pos = static_cast<double*>(sc.get(N * P * 8));
+        a.spos = static_cast<double*>(sc.get(N * P * 8));
         a.x_last = static_cast<double*>(sc.get(N * ndim * 8));
-        a.nbr = nbr_dev;
-        a.nbr_cnt = cnt_dev;
+        // the build writes rows in cell order into scratch, then they are
+        // transposed into the caller's particle-ordered buffers
+        a.nbr = static_cast<std::uint32_t*>(sc.get(static_cast<std::size_t>(row_capacity) * N * 4));
+        a.nbr_cnt = static_cast<std::uint32_t*>(sc.get(N * 4));
         a.S = row_capacity;
         a.caps = static_cast<std::uint32_t*>(sc.get(N * 4));
         a.cell_of = static_cast<std::uint32_t*>(sc.get(N * 4));
         a.cell_rank = static_cast<std::uint32_t*>(sc.get(N * 4));
         a.cell_list = static_cast<std::uint32_t*>(sc.get(N * 4));
+        a.work = a.cell_list;
         {
             const double cutoff = (Dmax + t_shell) * (1.0 + 1e-6);
             double cells = 1.0;
@@ -370,6 +374,7 @@ int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const dou
         cuda_ok(cudaMemsetAsync(a.caps, 0xFF, N * 4, st), "memset caps");
         rcpg::launch_pack(N, ndim, x_dev, D_dev, a.pos, st);
         rcpg::launch_rebuild(a, st);
+        rcpg::launch_rows_to_particle_order(N, a.cell_list, a.nbr, a.nbr_cnt, nbr_dev, cnt_dev, st);
         cuda_ok(cudaMemcpyAsync(&h, a.ctl, sizeof(h), cudaMemcpyDeviceToHost, st), "D2H ctl");
         cuda_ok(cudaStreamSynchronize(st), "sync");
         cuda_ok(cudaGetLastError(), "kernel launch");

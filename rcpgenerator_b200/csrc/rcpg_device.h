@@ -56,13 +56,19 @@ struct DevArrays {
     int P;                  // pos stride
     double* pos;            // [N*P] x_0..x_{d-1}, D0
     double* pos_tmp;        // [N*P] reorder gather target
+    double* spos;           // [N*P] positions in cell order (build scratch; may alias pos_tmp)
     double* F;              // [N*ndim]
     double* m;              // [N*ndim]
     double* v;              // [N*ndim]
     double* vec_tmp;        // [N*ndim] reorder gather target
     double* x_last;         // [N*ndim] refresh anchor positions
-    std::uint32_t* nbr;     // [S*N] column-major full rows, ascending
+    std::uint32_t* nbr;     // [S*N] column-major full rows, ascending partner index
     std::uint32_t* nbr_cnt; // [N]
+    // Row slot -> particle map. Row t (nbr[k*N + t], nbr_cnt[t]) belongs to
+    // particle work[t]; the engine keeps rows in cell order (work = cell_list)
+    // so a warp's particles, and their partners, are spatial neighbours.
+    // nullptr = identity (rows in particle order).
+    const std::uint32_t* work;
     std::uint32_t S;        // row capacity
     std::uint32_t* caps;    // [N] half-row capacity of the reference layout
     std::uint64_t* origin;  // [N] particle_origin
@@ -113,6 +119,9 @@ void launch_refresh_arrays(std::uint64_t N, int ndim, const double* x, double* x
                            const double* D, double* D_last, double* theta, double theta_new,
                            std::uint8_t* refresh, unsigned long long* count, cudaStream_t st);
 void launch_mean_force_blocks(const DevArrays& a, cudaStream_t st);
+void launch_rows_to_particle_order(std::uint64_t N, const std::uint32_t* work, const std::uint32_t* src,
+                                   const std::uint32_t* src_cnt, std::uint32_t* dst,
+                                   std::uint32_t* dst_cnt, cudaStream_t st);
 
 // Host-side finalisation shared with the controller kernel (ENG:4259-4268, :769-803).
 RCPG_HD StepScalars finalize_sums(const ForceSums& s, double mu_eff, int ndim) {

@@ -70,6 +70,7 @@ void Engine::alloc_device() {
     a_.P = P_;
     a_.pos = static_cast<double*>(dalloc(N * P_ * sizeof(double)));
     a_.pos_tmp = static_cast<double*>(dalloc(N * P_ * sizeof(double)));
+    a_.spos = a_.pos_tmp;  // the build's sorted copy; the reorder uses it only before a build
     a_.F = static_cast<double*>(dalloc(N * nd * sizeof(double)));
     a_.m = static_cast<double*>(dalloc(N * nd * sizeof(double)));
     a_.v = static_cast<double*>(dalloc(N * nd * sizeof(double)));
@@ -82,6 +83,7 @@ void Engine::alloc_device() {
     a_.cell_of = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.cell_rank = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.cell_list = static_cast<std::uint32_t*>(dalloc(N * 4));
+    a_.work = a_.cell_list;  // rows are kept in the cell order of their build
     // cell grid capacity: the grid at the initial (smallest) cutoff
     {
         const double cutoff = (host_c_.Dmax_cur + host_c_.t_shell) * (1.0 + 1e-6);

@@ -66,39 +66,43 @@ __device__ __forceinline__ int cell_coord(double x, double scale, int nc) {
 // ===========================================================================
 template <int ND>
 __global__ void __launch_bounds__(256) k_adam_refresh(DevArrays a, int do_adam, int do_refresh) {
-    const DevCtl* ctl = a.ctl;
-    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
-    if (i >= a.N) return;
+    DevCtl* ctl = a.ctl;
     if (ctl->halted) return;
     const bool adam = do_adam && ctl->adam_go;
     const bool refresh = do_refresh && !ctl->stopped && ctl->c.rebuild_mode == REBUILD_CHECK;
     if (!adam && !refresh) return;
-    double x[ND], D0;
-    load_pos<ND>(a.pos, i, x, D0);
-    if (adam) {
-        const double alpha = ctl->adam_alpha, ib1 = ctl->adam_inv_b1, ib2 = ctl->adam_inv_b2;
-#pragma unroll
-        for (int d = 0; d < ND; ++d) {
-            const std::uint64_t idx = i * ND + d;
-            double mm = a.m[idx], vv = a.v[idx];
-            x[d] = adam_coord(a.F[idx], mm, vv, x[d], alpha, ib1, ib2, ctl->adam_box[d]);
-            a.m[idx] = mm;
-            a.v[idx] = vv;
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    bool trig = false;
+    if (i < a.N) {
+        double x[ND], D0;
+        load_pos<ND>(a.pos, i, x, D0);
+        if (adam) {
+            const double alpha = ctl->adam_alpha, ib1 = ctl->adam_inv_b1, ib2 = ctl->adam_inv_b2;
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) {
+                const std::uint64_t idx = i * ND + d;
+                double mm = a.m[idx], vv = a.v[idx];
+                x[d] = adam_coord(a.F[idx], mm, vv, x[d], alpha, ib1, ib2, ctl->adam_box[d]);
+                a.m[idx] = mm;
+                a.v[idx] = vv;
+            }
+            if (ctl->fix_height_scale != 1.0) x[ND - 1] = xmul(x[ND - 1], ctl->fix_height_scale);
+            store_pos<ND>(a.pos, i, x, D0);
         }
-        if (ctl->fix_height_scale != 1.0) x[ND - 1] = xmul(x[ND - 1], ctl->fix_height_scale);
-        store_pos<ND>(a.pos, i, x, D0);
-    }
-    if (refresh) {
-        double d2 = 0.0;
-#pragma unroll
-        for (int d = 0; d < ND; ++d) {
-            const double dd = xsub(x[d], a.x_last[i * ND + d]);
-            d2 = xadd(d2, xmul(dd, dd));
+        if (refresh) {
+            double d2 = 0.0;
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) {
+                const double dd = xsub(x[d], a.x_last[i * ND + d]);
+                d2 = xadd(d2, xmul(dd, dd));
+            }
+            const double D = xmul(D0, ctl->refresh_kappa);
+            const double D_last = xmul(D0, ctl->kappa_min);
+            trig = refresh_trigger(d2, D, D_last, ctl->theta);
         }
-        const double D = xmul(D0, ctl->refresh_kappa);
-        const double D_last = xmul(D0, ctl->kappa_min);
-        if (refresh_trigger(d2, D, D_last, ctl->theta)) a.ctl->rebuild_flag = 1u;
     }
+    // one flag write per block (a million same-address stores would serialise in L2)
+    if (__syncthreads_or(trig) && threadIdx.x == 0) ctl->rebuild_flag = 1u;
 }
 
 // ===========================================================================
@@ -253,79 +257,118 @@ __global__ void __launch_bounds__(256) k_build_scatter(DevArrays a) {
     a.cell_list[a.cell_start[a.cell_of[i]] + a.cell_rank[i]] = static_cast<std::uint32_t>(i);
 }
 
+// Members of each cell in ascending particle order (the atomic ranks of
+// k_build_bin are arrival order; row slots and per-block force sums must not
+// depend on it), and a copy of their positions in that order (spos), so the
+// search reads each cell's candidates from contiguous memory.
+template <int ND>
+__global__ void __launch_bounds__(256) k_build_cell_sort(DevArrays a) {
+    const DevCtl* ctl = a.ctl;
+    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    const std::uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ctl->ncells) return;
+    const std::uint32_t q0 = a.cell_start[c], q1 = a.cell_start[c + 1];
+    for (std::uint32_t k = q0 + 1; k < q1; ++k) {
+        const std::uint32_t v = a.cell_list[k];
+        std::uint32_t p = k;
+        while (p > q0 && a.cell_list[p - 1] > v) {
+            a.cell_list[p] = a.cell_list[p - 1];
+            --p;
+        }
+        a.cell_list[p] = v;
+    }
+    constexpr int P = pos_stride(ND);
+    for (std::uint32_t q = q0; q < q1; ++q) {
+        const double2* src = reinterpret_cast<const double2*>(a.pos + static_cast<std::uint64_t>(a.cell_list[q]) * P);
+        double2* dst = reinterpret_cast<double2*>(a.spos + static_cast<std::uint64_t>(q) * P);
+        RCPG_UNROLL
+        for (int h = 0; h < P / 2; ++h) dst[h] = src[h];
+    }
+}
+
 // Neighbour rows: every j != i in the 3^ndim cell neighbourhood passing the
-// reference's shell test, sorted ascending. Rows are gathered in shared
-// memory (kSearchSmemRow per thread, bank = lane), longer rows continue in
-// the global row and are sorted there.
+// reference's shell test, sorted ascending. Thread t builds row slot t, the
+// row of particle cell_list[t]: the threads of a warp hold neighbouring cells
+// and read the same candidate cells. Rows are gathered in shared memory
+// (kSearchSmemRow per thread, bank = lane); longer rows continue in the
+// global row and are sorted there.
 template <int ND>
 __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
     DevCtl* ctl = a.ctl;
     if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
     __shared__ std::uint32_t buf[kSearchSmemRow * kSearchBlock];
-    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
-    if (i >= a.N) return;
+    __shared__ std::uint32_t block_need;
+    if (threadIdx.x == 0) block_need = 0u;
+    __syncthreads();
+    const std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
     const std::uint64_t N = a.N;
     const std::uint32_t S = a.S;
-    const Geometry& g = ctl->g;
-    const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
-    double xi[ND], D0i;
-    load_pos<ND>(a.pos, i, xi, D0i);
-    const double Di = xmul(D0i, kap);
-    int cc[ND], nn[ND], nc[ND];
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-        nc[d] = ctl->ncell[d];
-        cc[d] = cell_coord(xi[d], ctl->cell_scale[d], nc[d]);
-        nn[d] = nc[d] < 3 ? nc[d] : 3;  // distinct neighbour cells on this axis
-    }
-    int total_combo = 1;
-#pragma unroll
-    for (int d = 0; d < ND; ++d) total_combo *= nn[d];
     std::uint32_t n = 0, n_half = 0;
+    std::uint64_t i = 0;
     std::uint32_t* mine = buf + threadIdx.x;
-    for (int combo = 0; combo < total_combo; ++combo) {
-        int rem = combo;
-        std::uint32_t cell = 0, mul = 1;
-#pragma unroll
+    if (t < N) {
+        i = a.cell_list[t];
+        const Geometry& g = ctl->g;
+        const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
+        double xi[ND], D0i;
+        load_pos<ND>(a.spos, t, xi, D0i);
+        const double Di = xmul(D0i, kap);
+        int cc[ND], nn[ND], nc[ND];
+        RCPG_UNROLL
         for (int d = 0; d < ND; ++d) {
-            const int k = rem % nn[d];
-            rem /= nn[d];
-            int c = (nc[d] >= 3) ? cc[d] - 1 + k : k;
-            if (c < 0) c += nc[d];
-            else if (c >= nc[d]) c -= nc[d];
-            cell += static_cast<std::uint32_t>(c) * mul;
-            mul *= static_cast<std::uint32_t>(nc[d]);
+            nc[d] = ctl->ncell[d];
+            cc[d] = cell_coord(xi[d], ctl->cell_scale[d], nc[d]);
+            nn[d] = nc[d] < 3 ? nc[d] : 3;  // distinct neighbour cells on this axis
         }
-        const std::uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
-        for (std::uint32_t q = q0; q < q1; ++q) {
-            const std::uint32_t j = a.cell_list[q];
-            if (j == i) continue;
-            double xj[ND], D0j;
-            load_pos<ND>(a.pos, j, xj, D0j);
-            const double Dj = xmul(D0j, kap);
-            const bool ok = (j > i) ? in_shell<ND>(xi, Di, xj, Dj, g, t_shell)
-                                    : in_shell<ND>(xj, Dj, xi, Di, g, t_shell);
-            if (!ok) continue;
-            if (n < kSearchSmemRow) mine[n * kSearchBlock] = j;
-            else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + i] = j;
-            ++n;
-            if (j > i) ++n_half;
+        int total_combo = 1;
+        RCPG_UNROLL
+        for (int d = 0; d < ND; ++d) total_combo *= nn[d];
+        for (int combo = 0; combo < total_combo; ++combo) {
+            int rem = combo;
+            std::uint32_t cell = 0, mul = 1;
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) {
+                const int k = rem % nn[d];
+                rem /= nn[d];
+                int c = (nc[d] >= 3) ? cc[d] - 1 + k : k;
+                if (c < 0) c += nc[d];
+                else if (c >= nc[d]) c -= nc[d];
+                cell += static_cast<std::uint32_t>(c) * mul;
+                mul *= static_cast<std::uint32_t>(nc[d]);
+            }
+            const std::uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
+            for (std::uint32_t q = q0; q < q1; ++q) {
+                const std::uint32_t j = a.cell_list[q];
+                if (j == i) continue;
+                double xj[ND], D0j;
+                load_pos<ND>(a.spos, q, xj, D0j);
+                const double Dj = xmul(D0j, kap);
+                const bool ok = (j > i) ? in_shell<ND>(xi, Di, xj, Dj, g, t_shell)
+                                        : in_shell<ND>(xj, Dj, xi, Di, g, t_shell);
+                if (!ok) continue;
+                if (n < kSearchSmemRow) mine[n * kSearchBlock] = j;
+                else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + t] = j;
+                ++n;
+                if (j > i) ++n_half;
+            }
         }
+        const std::uint32_t cap = a.caps[i];
+        if (n_half > cap) {
+            if (atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
+                ctl->cap_error_particle = static_cast<std::uint32_t>(i);
+                ctl->cap_error_cap = cap;
+            }
+        }
+        atomicMax(&block_need, n);  // shared-memory atomic
     }
-    const std::uint32_t cap = a.caps[i];
-    if (n_half > cap) {
-        if (atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-            ctl->cap_error_particle = static_cast<std::uint32_t>(i);
-            ctl->cap_error_cap = cap;
-        }
-    }
+    __syncthreads();
+    if (threadIdx.x == 0 && block_need) atomicMax(&ctl->row_need, block_need);
+    if (t >= N) return;
     if (n > S) {
-        atomicMax(&ctl->row_need, n);
-        a.nbr_cnt[i] = S;
+        a.nbr_cnt[t] = S;
         return;
     }
-    atomicMax(&ctl->row_need, n);
-    a.nbr_cnt[i] = n;
+    a.nbr_cnt[t] = n;
     if (n <= static_cast<std::uint32_t>(kSearchSmemRow)) {
         for (std::uint32_t k = 1; k < n; ++k) {
             const std::uint32_t v = mine[k * kSearchBlock];
@@ -336,11 +379,11 @@ __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
             }
             mine[p * kSearchBlock] = v;
         }
-        for (std::uint32_t k = 0; k < n; ++k) a.nbr[static_cast<std::uint64_t>(k) * N + i] = mine[k * kSearchBlock];
+        for (std::uint32_t k = 0; k < n; ++k) a.nbr[static_cast<std::uint64_t>(k) * N + t] = mine[k * kSearchBlock];
     } else {
         for (std::uint32_t k = 0; k < static_cast<std::uint32_t>(kSearchSmemRow); ++k)
-            a.nbr[static_cast<std::uint64_t>(k) * N + i] = mine[k * kSearchBlock];
-        std::uint32_t* row = a.nbr + i;
+            a.nbr[static_cast<std::uint64_t>(k) * N + t] = mine[k * kSearchBlock];
+        std::uint32_t* row = a.nbr + t;
         for (std::uint32_t k = 1; k < n; ++k) {
             const std::uint32_t v = row[static_cast<std::uint64_t>(k) * N];
             std::uint32_t p = k;
@@ -420,6 +463,8 @@ __global__ void __launch_bounds__(kForceBlock) k_forces(DevArrays a, int exact_t
     ForceSums s;
     sums_zero(s);
     if (i < N) {
+        const std::uint64_t t = i;  // row slot
+        const std::uint64_t i = a.work ? a.work[t] : t;
         const Geometry& g = ctl->g;
         const double kap = ctl->force_kappa;
         double xi[ND], D0i;
@@ -428,25 +473,39 @@ __global__ void __launch_bounds__(kForceBlock) k_forces(DevArrays a, int exact_t
         double fi[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) fi[d] = 0.0;
-        const std::uint32_t n = a.nbr_cnt[i];
+        const std::uint32_t n = a.nbr_cnt[t];
         std::uint32_t nterm = 0;
-        for (std::uint32_t k = 0; k < n; ++k) {
-            const std::uint32_t j = a.nbr[static_cast<std::uint64_t>(k) * N + i];
-            double xj[ND], D0j;
-            load_pos<ND>(a.pos, j, xj, D0j);
-            const double Dj = xmul(D0j, kap);
-            PairTerms pt;
-            if (!pair_force<ND>(xi, Di, xj, Dj, g, fi, pt)) continue;
-            if (j > i) {
-                s.pair_U = xadd(s.pair_U, pt.U);
-                s.pair_Lc = xadd(s.pair_Lc, pt.Lc);
-                s.pair_dk = xadd(s.pair_dk, pt.dk);
-                s.pair_Fm = xadd(s.pair_Fm, pt.Fm);
-                s.pair_maxov = fmax(s.pair_maxov, pt.U);
-                s.pair_count += 1ull;
-                if (exact_terms) {
-                    a.pterm[static_cast<std::uint64_t>(nterm) * N + i] = pt;
-                    ++nterm;
+        // Partners in chunks of kChunk: the row ids and then the partner
+        // positions of a chunk are loaded before any of its arithmetic, so a
+        // thread keeps kChunk gathers in flight; the pairs are still summed in
+        // row (ascending partner) order.
+        constexpr std::uint32_t kChunk = 4;
+        for (std::uint32_t k0 = 0; k0 < n; k0 += kChunk) {
+            std::uint32_t jj[kChunk];
+            double xj[kChunk][ND], D0j[kChunk];
+            RCPG_UNROLL
+            for (std::uint32_t u = 0; u < kChunk; ++u)
+                jj[u] = (k0 + u < n) ? __ldg(a.nbr + static_cast<std::uint64_t>(k0 + u) * N + t) : 0u;
+            RCPG_UNROLL
+            for (std::uint32_t u = 0; u < kChunk; ++u)
+                if (k0 + u < n) load_pos<ND>(a.pos, jj[u], xj[u], D0j[u]);
+            RCPG_UNROLL
+            for (std::uint32_t u = 0; u < kChunk; ++u) {
+                if (k0 + u >= n) break;
+                const std::uint32_t j = jj[u];
+                PairTerms pt;
+                if (!pair_force<ND>(xi, Di, xj[u], xmul(D0j[u], kap), g, fi, pt)) continue;
+                if (j > i) {
+                    s.pair_U = xadd(s.pair_U, pt.U);
+                    s.pair_Lc = xadd(s.pair_Lc, pt.Lc);
+                    s.pair_dk = xadd(s.pair_dk, pt.dk);
+                    s.pair_Fm = xadd(s.pair_Fm, pt.Fm);
+                    s.pair_maxov = fmax(s.pair_maxov, pt.U);
+                    s.pair_count += 1ull;
+                    if (exact_terms) {
+                        a.pterm[static_cast<std::uint64_t>(nterm) * N + i] = pt;
+                        ++nterm;
+                    }
                 }
             }
         }
@@ -519,17 +578,19 @@ __global__ void k_reduce_exact(DevArrays a) {
 }
 
 // Fixed-order reduction of the per-block partial sums by one block.
+constexpr int kCtlThreads = 1024;
+
 __device__ void reduce_blocks(const DevArrays& a, ForceSums* smem, ForceSums& out) {
     const unsigned nb = force_blocks(a.N);
     ForceSums s;
     sums_zero(s);
     for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) sums_add(s, a.block_sums[b]);
-    block_reduce_sums<256>(s, smem);
+    block_reduce_sums<kCtlThreads>(s, smem);
     if (threadIdx.x == 0) out = s;
 }
 
-__global__ void __launch_bounds__(256) k_reduce_fast(DevArrays a) {
-    __shared__ ForceSums red[256 / 32];
+__global__ void __launch_bounds__(kCtlThreads) k_reduce_fast(DevArrays a) {
+    __shared__ ForceSums red[kCtlThreads / 32];
     DevCtl* ctl = a.ctl;
     if (ctl_idle(ctl)) return;
     ForceSums s;
@@ -561,8 +622,8 @@ __device__ void publish_step(DevCtl* ctl, const Controller& c, int ndim) {
 // Graph-mode controller: reduce, finish step s (end_step), open step s+1
 // (begin_step) and publish the parameters of the kernels that follow. With
 // open_only it just opens the next step (the first step of a run).
-__global__ void __launch_bounds__(256) k_controller(DevArrays a, int open_only) {
-    __shared__ ForceSums red[256 / 32];
+__global__ void __launch_bounds__(kCtlThreads) k_controller(DevArrays a, int open_only) {
+    __shared__ ForceSums red[kCtlThreads / 32];
     DevCtl* ctl = a.ctl;
     if (ctl_idle(ctl)) {
         if (threadIdx.x == 0) ctl->adam_go = 0u;
@@ -621,12 +682,25 @@ __global__ void k_fix_height(DevArrays a) {
 
 template <int ND>
 __global__ void k_half_counts(DevArrays a, std::uint32_t* out) {
-    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
-    if (i >= a.N) return;
-    const std::uint32_t n = a.nbr_cnt[i];
+    const std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (t >= a.N) return;
+    const std::uint64_t i = a.work ? a.work[t] : t;
+    const std::uint32_t n = a.nbr_cnt[t];
     std::uint32_t h = 0;
-    for (std::uint32_t k = 0; k < n; ++k) h += a.nbr[static_cast<std::uint64_t>(k) * a.N + i] > i;
+    for (std::uint32_t k = 0; k < n; ++k) h += a.nbr[static_cast<std::uint64_t>(k) * a.N + t] > i;
     out[i] = h;
+}
+
+// Rows in cell order -> rows in particle order (dst[k*N + work[t]] = src[k*N + t]).
+__global__ void k_rows_to_particle_order(std::uint64_t N, const std::uint32_t* work,
+                                         const std::uint32_t* src, const std::uint32_t* src_cnt,
+                                         std::uint32_t* dst, std::uint32_t* dst_cnt) {
+    const std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (t >= N) return;
+    const std::uint64_t i = work[t];
+    const std::uint32_t n = src_cnt[t];
+    dst_cnt[i] = n;
+    for (std::uint32_t k = 0; k < n; ++k) dst[static_cast<std::uint64_t>(k) * N + i] = src[static_cast<std::uint64_t>(k) * N + t];
 }
 
 // ===========================================================================
@@ -863,6 +937,7 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     k_build_bin<ND><<<nb, kForceBlock, 0, st>>>(a);
     scan_exclusive(a.cell_count, a.cell_start, a.C_alloc + 1, a.scan_tmp, a.ctl, st);
     k_build_scatter<<<nb, kForceBlock, 0, st>>>(a);
+    k_build_cell_sort<ND><<<(a.C_alloc + 255) / 256, 256, 0, st>>>(a);
     const unsigned sb = static_cast<unsigned>((a.N + kSearchBlock - 1) / kSearchBlock);
     k_build_search<ND><<<sb, kSearchBlock, 0, st>>>(a);
 }
@@ -900,11 +975,11 @@ void launch_reduce_exact(const DevArrays& a, cudaStream_t st) {
 }
 
 void launch_reduce_fast(const DevArrays& a, cudaStream_t st) {
-    k_reduce_fast<<<1, 256, 0, st>>>(a);
+    k_reduce_fast<<<1, kCtlThreads, 0, st>>>(a);
 }
 
 void launch_controller(const DevArrays& a, int open_only, cudaStream_t st) {
-    k_controller<<<1, 256, 0, st>>>(a, open_only);
+    k_controller<<<1, kCtlThreads, 0, st>>>(a, open_only);
 }
 
 void launch_reorder(const DevArrays& a, cudaStream_t st) {
@@ -938,6 +1013,12 @@ void launch_refresh_arrays(std::uint64_t N, int ndim, const double* x, double* x
     const unsigned nb = force_blocks(N);
     RCPG_DISPATCH_ND(ndim, (k_refresh_arrays<ND><<<nb, kForceBlock, 0, st>>>(
                                N, x, x_last, D, D_last, theta, theta_new, refresh, count)));
+}
+
+void launch_rows_to_particle_order(std::uint64_t N, const std::uint32_t* work, const std::uint32_t* src,
+                                   const std::uint32_t* src_cnt, std::uint32_t* dst,
+                                   std::uint32_t* dst_cnt, cudaStream_t st) {
+    k_rows_to_particle_order<<<force_blocks(N), kForceBlock, 0, st>>>(N, work, src, src_cnt, dst, dst_cnt);
 }
 
 void launch_mean_force_blocks(const DevArrays& a, cudaStream_t st) {
