@@ -293,9 +293,12 @@ __global__ void __launch_bounds__(256) k_build_cell_sort(DevArrays a) {
 // (kSearchSmemRow per thread, bank = lane); longer rows continue in the
 // global row and are sorted there.
 template <int ND>
+__device__ __forceinline__ bool tiled_build_ok(const DevCtl* ctl);
+
+template <int ND>
 __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
     DevCtl* ctl = a.ctl;
-    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    if (ctl_idle(ctl) || !ctl->rebuild_flag || tiled_build_ok<ND>(ctl)) return;
     __shared__ std::uint32_t buf[kSearchSmemRow * kSearchBlock];
     __shared__ std::uint32_t block_need;
     if (threadIdx.x == 0) block_need = 0u;
@@ -394,6 +397,288 @@ __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
             row[static_cast<std::uint64_t>(p) * N] = v;
         }
     }
+}
+
+// ---- tiled search (ndim 2, 3) ---------------------------------------------
+// One block per tile of cells (persistent over tiles). The particles of the
+// tile and of its one-cell halo are staged in shared memory (positions, ids,
+// row slots, local cell), then every particle of the tile tests its 3^ndim
+// neighbour cells from shared memory only. Used when every axis has at least
+// tile + 2 cells (no cell of the halo is loaded twice); otherwise, and for
+// ndim > 3, k_build_search handles the build.
+template <int ND> struct TileShape;
+template <> struct TileShape<2> {
+    __host__ __device__ static constexpr int t(int d) { return d == 0 ? 16 : 8; }
+    static constexpr int halo_cells = 18 * 10;
+    static constexpr int stage = 1024;
+};
+template <> struct TileShape<3> {
+    __host__ __device__ static constexpr int t(int) { return 4; }
+    static constexpr int halo_cells = 6 * 6 * 6;
+    static constexpr int stage = 1280;
+};
+constexpr int kTileThreads = 256;
+constexpr int kTileRow = 24;
+
+// dynamic shared memory of k_build_search_tiled<ND>
+template <int ND>
+constexpr std::size_t tile_smem_bytes() {
+    using TS = TileShape<ND <= 3 ? ND : 3>;
+    return static_cast<std::size_t>(TS::stage) * pos_stride(ND) * 8 + 2ull * TS::stage * 4 +
+           static_cast<std::size_t>(kTileRow) * kTileThreads * 4 + (TS::halo_cells + 2) * 4 +
+           static_cast<std::size_t>(TS::stage) * 2;
+}
+
+template <int ND>
+__device__ __forceinline__ bool tiled_build_ok(const DevCtl* ctl) {
+    if (ND > 3) return false;
+    for (int d = 0; d < ND; ++d)
+        if (ctl->ncell[d] < TileShape<(ND <= 3 ? ND : 3)>::t(d) + 2) return false;
+    return true;
+}
+
+// Sorts a row gathered partly in shared memory (column `mine`, stride kTileThreads)
+// and partly in the global row, and writes it to row slot q.
+__device__ __forceinline__ void finish_row(std::uint32_t* mine, int stride, int smem_cap,
+                                           std::uint32_t n, std::uint32_t S, std::uint32_t* nbr,
+                                           std::uint32_t* nbr_cnt, std::uint64_t N, std::uint64_t q) {
+    if (n > S) {
+        nbr_cnt[q] = S;
+        return;
+    }
+    nbr_cnt[q] = n;
+    if (n <= static_cast<std::uint32_t>(smem_cap)) {
+        for (std::uint32_t k = 1; k < n; ++k) {
+            const std::uint32_t v = mine[k * stride];
+            std::uint32_t p = k;
+            while (p > 0 && mine[(p - 1) * stride] > v) {
+                mine[p * stride] = mine[(p - 1) * stride];
+                --p;
+            }
+            mine[p * stride] = v;
+        }
+        for (std::uint32_t k = 0; k < n; ++k) nbr[static_cast<std::uint64_t>(k) * N + q] = mine[k * stride];
+    } else {
+        for (std::uint32_t k = 0; k < static_cast<std::uint32_t>(smem_cap); ++k)
+            nbr[static_cast<std::uint64_t>(k) * N + q] = mine[k * stride];
+        std::uint32_t* row = nbr + q;
+        for (std::uint32_t k = 1; k < n; ++k) {
+            const std::uint32_t v = row[static_cast<std::uint64_t>(k) * N];
+            std::uint32_t p = k;
+            while (p > 0 && row[static_cast<std::uint64_t>(p - 1) * N] > v) {
+                row[static_cast<std::uint64_t>(p) * N] = row[static_cast<std::uint64_t>(p - 1) * N];
+                --p;
+            }
+            row[static_cast<std::uint64_t>(p) * N] = v;
+        }
+    }
+}
+
+template <int ND>
+__global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a) {
+    constexpr int NDT = ND <= 3 ? ND : 3;
+    using TS = TileShape<NDT>;
+    constexpr int P = pos_stride(ND);
+    constexpr int STAGE = TS::stage;
+    constexpr int HC = TS::halo_cells;
+    DevCtl* ctl = a.ctl;
+    if (ND > 3) return;
+    if (ctl_idle(ctl) || !ctl->rebuild_flag || !tiled_build_ok<ND>(ctl)) return;
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    double* s_pos = reinterpret_cast<double*>(tile_smem);
+    std::uint32_t* s_id = reinterpret_cast<std::uint32_t*>(s_pos + STAGE * P);
+    std::uint32_t* s_slot = s_id + STAGE;
+    std::uint32_t* s_rows = s_slot + STAGE;
+    std::uint32_t* s_cstart = s_rows + kTileRow * kTileThreads;
+    std::uint16_t* s_cell = reinterpret_cast<std::uint16_t*>(s_cstart + HC + 2);
+    __shared__ std::uint32_t s_warp[kTileThreads / 32];
+    __shared__ std::uint32_t s_total, s_need;
+    const std::uint64_t N = a.N;
+    const std::uint32_t S = a.S;
+    const Geometry& g = ctl->g;
+    const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
+    int nc[ND], nt[ND];
+    std::uint32_t tiles = 1;
+    RCPG_UNROLL
+    for (int d = 0; d < ND; ++d) {
+        nc[d] = ctl->ncell[d];
+        nt[d] = (nc[d] + TS::t(d) - 1) / TS::t(d);
+        tiles *= static_cast<std::uint32_t>(nt[d]);
+    }
+    if (threadIdx.x == 0) s_need = 0u;
+    std::uint32_t* mine = s_rows + threadIdx.x;
+    for (std::uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        int t0[ND], hw[ND];
+        std::uint32_t rem = tile;
+        int H = 1;
+        RCPG_UNROLL
+        for (int d = 0; d < ND; ++d) {
+            const int tc = static_cast<int>(rem % static_cast<std::uint32_t>(nt[d]));
+            rem /= static_cast<std::uint32_t>(nt[d]);
+            t0[d] = tc * TS::t(d);
+            const int tw = min(TS::t(d), nc[d] - t0[d]);
+            hw[d] = tw + 2;
+            H *= hw[d];
+        }
+        __syncthreads();  // the previous tile is done with shared memory
+        // 1. particle count of every halo cell, 2. block scan -> staging offsets
+        std::uint32_t cs = 0, cnt = 0;
+        if (static_cast<int>(threadIdx.x) < H) {
+            int r = threadIdx.x;
+            std::uint32_t c = 0, mul = 1;
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) {
+                const int l = r % hw[d];
+                r /= hw[d];
+                int gc = t0[d] - 1 + l;
+                if (gc < 0) gc += nc[d];
+                else if (gc >= nc[d]) gc -= nc[d];
+                c += static_cast<std::uint32_t>(gc) * mul;
+                mul *= static_cast<std::uint32_t>(nc[d]);
+            }
+            cs = a.cell_start[c];
+            cnt = a.cell_start[c + 1] - cs;
+        }
+        std::uint32_t total;
+        const std::uint32_t off = block_exclusive_scan(cnt, s_warp, total);
+        if (static_cast<int>(threadIdx.x) < H) s_cstart[threadIdx.x] = off;
+        if (threadIdx.x == 0) {
+            s_cstart[H] = total;
+            s_total = total;
+        }
+        const bool fits = total <= static_cast<std::uint32_t>(STAGE);
+        // 3. stage the halo particles (one thread per halo cell)
+        if (fits && static_cast<int>(threadIdx.x) < H) {
+            for (std::uint32_t k = 0; k < cnt; ++k) {
+                const std::uint32_t q = cs + k, dst = off + k;
+                const double2* src = reinterpret_cast<const double2*>(a.spos + static_cast<std::uint64_t>(q) * P);
+                double2* sp = reinterpret_cast<double2*>(s_pos + dst * P);
+                RCPG_UNROLL
+                for (int h = 0; h < P / 2; ++h) sp[h] = src[h];
+                s_id[dst] = a.cell_list[q];
+                s_slot[dst] = q;
+                s_cell[dst] = static_cast<std::uint16_t>(threadIdx.x);
+            }
+        }
+        __syncthreads();
+        if (fits) {
+            // 4. rows of the tile's own particles, candidates from shared memory
+            for (std::uint32_t k = threadIdx.x; k < total; k += blockDim.x) {
+                int hl[ND];
+                int r = s_cell[k];
+                bool inner = true;
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    hl[d] = r % hw[d];
+                    r /= hw[d];
+                    inner = inner && hl[d] >= 1 && hl[d] <= hw[d] - 2;
+                }
+                if (!inner) continue;
+                const std::uint32_t i = s_id[k];
+                const std::uint64_t q = s_slot[k];
+                double xi[ND], D0i;
+                load_pos<ND>(s_pos, k, xi, D0i);
+                const double Di = xmul(D0i, kap);
+                std::uint32_t n = 0, n_half = 0;
+                constexpr int NCOMBO = (ND == 2) ? 9 : 27;
+                for (int combo = 0; combo < NCOMBO; ++combo) {
+                    int cr = combo, hc = 0, mul = 1;
+                    RCPG_UNROLL
+                    for (int d = 0; d < ND; ++d) {
+                        hc += (hl[d] - 1 + cr % 3) * mul;
+                        cr /= 3;
+                        mul *= hw[d];
+                    }
+                    const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 1];
+                    for (std::uint32_t pp = p0; pp < p1; ++pp) {
+                        if (pp == k) continue;
+                        const std::uint32_t j = s_id[pp];
+                        double xj[ND], D0j;
+                        load_pos<ND>(s_pos, pp, xj, D0j);
+                        const double Dj = xmul(D0j, kap);
+                        const bool ok = (j > i) ? in_shell<ND>(xi, Di, xj, Dj, g, t_shell)
+                                                : in_shell<ND>(xj, Dj, xi, Di, g, t_shell);
+                        if (!ok) continue;
+                        if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = j;
+                        else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
+                        ++n;
+                        if (j > i) ++n_half;
+                    }
+                }
+                const std::uint32_t cap = a.caps[i];
+                if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
+                    ctl->cap_error_particle = i;
+                    ctl->cap_error_cap = cap;
+                }
+                atomicMax(&s_need, n);
+                finish_row(mine, kTileThreads, kTileRow, n, S, a.nbr, a.nbr_cnt, N, q);
+            }
+        } else {
+            // more halo particles than the staging area: rows of this tile from global memory
+            for (int h = threadIdx.x; h < H; h += blockDim.x) {
+                int hl[ND];
+                int r = h;
+                bool inner = true;
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    hl[d] = r % hw[d];
+                    r /= hw[d];
+                    inner = inner && hl[d] >= 1 && hl[d] <= hw[d] - 2;
+                }
+                if (!inner) continue;
+                std::uint32_t c = 0, mul = 1;
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    c += static_cast<std::uint32_t>(t0[d] - 1 + hl[d]) * mul;
+                    mul *= static_cast<std::uint32_t>(nc[d]);
+                }
+                for (std::uint32_t q = a.cell_start[c]; q < a.cell_start[c + 1]; ++q) {
+                    const std::uint32_t i = a.cell_list[q];
+                    double xi[ND], D0i;
+                    load_pos<ND>(a.spos, q, xi, D0i);
+                    const double Di = xmul(D0i, kap);
+                    std::uint32_t n = 0, n_half = 0;
+                    constexpr int NCOMBO = (ND == 2) ? 9 : 27;
+                    for (int combo = 0; combo < NCOMBO; ++combo) {
+                        int cr = combo;
+                        std::uint32_t cn = 0, mm = 1;
+                        RCPG_UNROLL
+                        for (int d = 0; d < ND; ++d) {
+                            int gc = t0[d] - 1 + hl[d] - 1 + cr % 3;
+                            cr /= 3;
+                            if (gc < 0) gc += nc[d];
+                            else if (gc >= nc[d]) gc -= nc[d];
+                            cn += static_cast<std::uint32_t>(gc) * mm;
+                            mm *= static_cast<std::uint32_t>(nc[d]);
+                        }
+                        for (std::uint32_t pp = a.cell_start[cn]; pp < a.cell_start[cn + 1]; ++pp) {
+                            const std::uint32_t j = a.cell_list[pp];
+                            if (j == i) continue;
+                            double xj[ND], D0j;
+                            load_pos<ND>(a.spos, pp, xj, D0j);
+                            const double Dj = xmul(D0j, kap);
+                            const bool ok = (j > i) ? in_shell<ND>(xi, Di, xj, Dj, g, t_shell)
+                                                    : in_shell<ND>(xj, Dj, xi, Di, g, t_shell);
+                            if (!ok) continue;
+                            if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = j;
+                            else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
+                            ++n;
+                            if (j > i) ++n_half;
+                        }
+                    }
+                    const std::uint32_t cap = a.caps[i];
+                    if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
+                        ctl->cap_error_particle = i;
+                        ctl->cap_error_cap = cap;
+                    }
+                    atomicMax(&s_need, n);
+                    finish_row(mine, kTileThreads, kTileRow, n, S, a.nbr, a.nbr_cnt, N, q);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
 }
 
 // ===========================================================================
@@ -624,49 +909,70 @@ __device__ void publish_step(DevCtl* ctl, const Controller& c, int ndim) {
 // open_only it just opens the next step (the first step of a run).
 __global__ void __launch_bounds__(kCtlThreads) k_controller(DevArrays a, int open_only) {
     __shared__ ForceSums red[kCtlThreads / 32];
+    // the controller state is worked on in shared memory: one coalesced copy
+    // in and out instead of a chain of dependent global loads in one thread
+    __shared__ Controller cs;
+    __shared__ int s_publish;
     DevCtl* ctl = a.ctl;
     if (ctl_idle(ctl)) {
         if (threadIdx.x == 0) ctl->adam_go = 0u;
         return;
     }
-    Controller& c = ctl->c;
-    if (!open_only) {
-        ForceSums s;
-        reduce_blocks(a, red, s);
-        if (threadIdx.x != 0) return;
-        ctl->sums = s;
-        // capacity problems of the last build stop the run before its results are used
-        if (ctl->row_need > a.S || ctl->cap_error) {
-            ctl->halted = 1u;
+    static_assert(sizeof(Controller) % 8 == 0, "controller copy by 8-byte words");
+    constexpr int kWords = sizeof(Controller) / 8;
+    {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&ctl->c);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&cs);
+        for (int w = threadIdx.x; w < kWords; w += blockDim.x) dst[w] = src[w];
+    }
+    __syncthreads();
+    ForceSums s;
+    if (!open_only) reduce_blocks(a, red, s);
+    if (threadIdx.x == 0) {
+        Controller& c = cs;
+        s_publish = 0;
+        bool go = true;
+        if (!open_only) {
+            ctl->sums = s;
+            // capacity problems of the last build stop the run before its results are used
+            if (ctl->row_need > a.S || ctl->cap_error) {
+                ctl->halted = 1u;
+                ctl->adam_go = 0u;
+                go = false;
+            } else {
+                const StepScalars sc = finalize_sums(s, ctl->force_mu, a.ndim);
+                ctl->scal = sc;
+                end_step(c, a.hist, sc);
+                ctl->graph_steps += 1ull;
+                for (int d = 0; d < a.ndim; ++d) ctl->adam_box[d] = c.box[d];
+                ctl->adam_alpha = c.adam_alpha;
+                ctl->adam_inv_b1 = c.inv_b1;
+                ctl->adam_inv_b2 = c.inv_b2;
+                ctl->adam_go = 1u;
+            }
+        } else {
             ctl->adam_go = 0u;
-            return;
         }
-        const StepScalars sc = finalize_sums(s, ctl->force_mu, a.ndim);
-        ctl->scal = sc;
-        end_step(c, a.hist, sc);
-        ctl->graph_steps += 1ull;
-        for (int d = 0; d < a.ndim; ++d) ctl->adam_box[d] = c.box[d];
-        ctl->adam_alpha = c.adam_alpha;
-        ctl->adam_inv_b1 = c.inv_b1;
-        ctl->adam_inv_b2 = c.inv_b2;
-        ctl->adam_go = 1u;
-    } else {
-        if (threadIdx.x != 0) return;
-        ctl->adam_go = 0u;
+        if (go) {
+            ctl->fix_height_scale = 1.0;
+            if (c.steps + 1 > c.step_cap) {
+                ctl->stopped = 1u;
+            } else {
+                begin_step(c, a.hist, c.steps + 1);
+                // the stretch of a reorder step waits until after the reorder (ENG:5661 < :5758)
+                ctl->fix_height_scale = c.reorder ? 1.0 : c.fix_height_scale;
+                if (c.done || c.reorder || c.lock_now) ctl->stopped = 1u;
+                else s_publish = 1;
+            }
+        }
     }
-    ctl->fix_height_scale = 1.0;
-    if (c.steps + 1 > c.step_cap) {
-        ctl->stopped = 1u;
-        return;
+    __syncthreads();
+    {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&cs);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&ctl->c);
+        for (int w = threadIdx.x; w < kWords; w += blockDim.x) dst[w] = src[w];
     }
-    begin_step(c, a.hist, c.steps + 1);
-    // the stretch of a reorder step waits until after the reorder (ENG:5661 < :5758)
-    ctl->fix_height_scale = c.reorder ? 1.0 : c.fix_height_scale;
-    if (c.done || c.reorder || c.lock_now) {
-        ctl->stopped = 1u;
-        return;
-    }
-    publish_step(ctl, c, a.ndim);
+    if (threadIdx.x == 0 && s_publish) publish_step(ctl, cs, a.ndim);
 }
 
 // fix_height stretch of the last coordinate without an ADAM step (used when
@@ -939,6 +1245,19 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     k_build_scatter<<<nb, kForceBlock, 0, st>>>(a);
     k_build_cell_sort<ND><<<(a.C_alloc + 255) / 256, 256, 0, st>>>(a);
     const unsigned sb = static_cast<unsigned>((a.N + kSearchBlock - 1) / kSearchBlock);
+    if (ND <= 3) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        constexpr std::size_t smem = tile_smem_bytes<ND>();
+        static bool attr_set[64][2] = {};
+        if (dev >= 0 && dev < 64 && !attr_set[dev][ND - 2]) {
+            cudaFuncSetAttribute(k_build_search_tiled<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+            attr_set[dev][ND - 2] = true;
+        }
+        k_build_search_tiled<ND><<<static_cast<unsigned>(sms) * 3u, kTileThreads, smem, st>>>(a);
+    }
     k_build_search<ND><<<sb, kSearchBlock, 0, st>>>(a);
 }
 
