@@ -90,16 +90,19 @@ struct Geometry {
 };
 
 // ---- pair shell test (neighbour-list membership) --------------------------
-// Full-refresh membership of pair {lo < hi}: MIC d2 < r_c^2 with
+// Full-refresh membership of the pair of particles at xi, xj: MIC d2 < r_c^2,
 //   r_c = (D_lo + D_hi)*0.5 + t                       for ndim <= 3 (kd-tree, ENG:3296)
 //   r_c = D_lo*0.5 + t + (double)(float)(D_hi*0.5)     for ndim > 3  (sort+walk, ENG:1357)
+// with D_lo / D_hi the diameters of the lower / higher particle index. d2 is
+// symmetric bit for bit (the minimum image of -a is exactly -(image of a)),
+// and so is r_c for ndim <= 3; only the ndim > 3 cutoff depends on the order.
 template <int ND>
-RCPG_HD bool in_shell(const double* x_lo, double D_lo, const double* x_hi, double D_hi,
-                      const Geometry& g, double t_shell) {
+RCPG_HD bool in_shell(const double* xi, const double* xj, double D_lo, double D_hi,
+                      const double* box, const double* inv_box, double t_shell) {
     double d2 = 0.0;
-RCPG_UNROLL
+    RCPG_UNROLL
     for (int d = 0; d < ND; ++d) {
-        const double dd = mic(xsub(x_hi[d], x_lo[d]), g.inv_box[d], g.box[d]);
+        const double dd = mic(xsub(xj[d], xi[d]), inv_box[d], box[d]);
         d2 = xadd(d2, xmul(dd, dd));
     }
     double r_c;

@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
     std::uint32_t* mine = buf + threadIdx.x;
     if (t < N) {
         i = a.cell_list[t];
-        const Geometry& g = ctl->g;
+        const Geometry g = ctl->g;  // register copy: the loops below store through other pointers
         const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
         double xi[ND], D0i;
         load_pos<ND>(a.spos, t, xi, D0i);
@@ -326,18 +326,24 @@ __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
         int total_combo = 1;
         RCPG_UNROLL
         for (int d = 0; d < ND; ++d) total_combo *= nn[d];
+        int odo[ND];
+        RCPG_UNROLL
+        for (int d = 0; d < ND; ++d) odo[d] = 0;
         for (int combo = 0; combo < total_combo; ++combo) {
-            int rem = combo;
             std::uint32_t cell = 0, mul = 1;
             RCPG_UNROLL
             for (int d = 0; d < ND; ++d) {
-                const int k = rem % nn[d];
-                rem /= nn[d];
+                const int k = odo[d];
                 int c = (nc[d] >= 3) ? cc[d] - 1 + k : k;
                 if (c < 0) c += nc[d];
                 else if (c >= nc[d]) c -= nc[d];
                 cell += static_cast<std::uint32_t>(c) * mul;
                 mul *= static_cast<std::uint32_t>(nc[d]);
+            }
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) {
+                if (++odo[d] < nn[d]) break;
+                odo[d] = 0;
             }
             const std::uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
             for (std::uint32_t q = q0; q < q1; ++q) {
@@ -346,8 +352,9 @@ __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
                 double xj[ND], D0j;
                 load_pos<ND>(a.spos, q, xj, D0j);
                 const double Dj = xmul(D0j, kap);
-                const bool ok = (j > i) ? in_shell<ND>(xi, Di, xj, Dj, g, t_shell)
-                                        : in_shell<ND>(xj, Dj, xi, Di, g, t_shell);
+                const bool ok = (ND <= 3 || j > i)
+                                    ? in_shell<ND>(xi, xj, Di, Dj, g.box, g.inv_box, t_shell)
+                                    : in_shell<ND>(xi, xj, Dj, Di, g.box, g.inv_box, t_shell);
                 if (!ok) continue;
                 if (n < kSearchSmemRow) mine[n * kSearchBlock] = j;
                 else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + t] = j;
@@ -495,7 +502,7 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
     __shared__ std::uint32_t s_total, s_need;
     const std::uint64_t N = a.N;
     const std::uint32_t S = a.S;
-    const Geometry& g = ctl->g;
+    const Geometry g = ctl->g;  // register copy: the loops below store through other pointers
     const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
     int nc[ND], nt[ND];
     std::uint32_t tiles = 1;
@@ -581,13 +588,20 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
                 const double Di = xmul(D0i, kap);
                 std::uint32_t n = 0, n_half = 0;
                 constexpr int NCOMBO = (ND == 2) ? 9 : 27;
+                int odo[ND];
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) odo[d] = 0;
                 for (int combo = 0; combo < NCOMBO; ++combo) {
-                    int cr = combo, hc = 0, mul = 1;
+                    int hc = 0, mul = 1;
                     RCPG_UNROLL
                     for (int d = 0; d < ND; ++d) {
-                        hc += (hl[d] - 1 + cr % 3) * mul;
-                        cr /= 3;
+                        hc += (hl[d] - 1 + odo[d]) * mul;
                         mul *= hw[d];
+                    }
+                    RCPG_UNROLL
+                    for (int d = 0; d < ND; ++d) {
+                        if (++odo[d] < 3) break;
+                        odo[d] = 0;
                     }
                     const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 1];
                     for (std::uint32_t pp = p0; pp < p1; ++pp) {
@@ -596,8 +610,7 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
                         double xj[ND], D0j;
                         load_pos<ND>(s_pos, pp, xj, D0j);
                         const double Dj = xmul(D0j, kap);
-                        const bool ok = (j > i) ? in_shell<ND>(xi, Di, xj, Dj, g, t_shell)
-                                                : in_shell<ND>(xj, Dj, xi, Di, g, t_shell);
+                        const bool ok = in_shell<ND>(xi, xj, Di, Dj, g.box, g.inv_box, t_shell);
                         if (!ok) continue;
                         if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = j;
                         else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
@@ -657,8 +670,7 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
                             double xj[ND], D0j;
                             load_pos<ND>(a.spos, pp, xj, D0j);
                             const double Dj = xmul(D0j, kap);
-                            const bool ok = (j > i) ? in_shell<ND>(xi, Di, xj, Dj, g, t_shell)
-                                                    : in_shell<ND>(xj, Dj, xi, Di, g, t_shell);
+                            const bool ok = in_shell<ND>(xi, xj, Di, Dj, g.box, g.inv_box, t_shell);
                             if (!ok) continue;
                             if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = j;
                             else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
@@ -750,7 +762,7 @@ __global__ void __launch_bounds__(kForceBlock) k_forces(DevArrays a, int exact_t
     if (i < N) {
         const std::uint64_t t = i;  // row slot
         const std::uint64_t i = a.work ? a.work[t] : t;
-        const Geometry& g = ctl->g;
+        const Geometry g = ctl->g;  // register copy: the loops below store through other pointers
         const double kap = ctl->force_kappa;
         double xi[ND], D0i;
         load_pos<ND>(a.pos, i, xi, D0i);
@@ -835,7 +847,7 @@ __global__ void k_reduce_exact(DevArrays a) {
             s.pair_Fm = xadd(s.pair_Fm, pt.Fm);
         }
     }
-    const Geometry& g = ctl->g;
+    const Geometry g = ctl->g;  // register copy: the loops below store through other pointers
     const double kap = ctl->force_kappa;
     for (std::uint64_t i = 0; i < N; ++i) {
         double xi[ND], D0i, fdummy[ND];

@@ -73,8 +73,9 @@ struct Emu {
             for (std::uint64_t j = 0; j < N; ++j) {
                 if (j == i) continue;
                 const double Dj = D0[j] * kap;
-                const bool ok = (j > i) ? in_shell<ND>(&x[i * ND], Di, &x[j * ND], Dj, g, t_shell)
-                                        : in_shell<ND>(&x[j * ND], Dj, &x[i * ND], Di, g, t_shell);
+                const bool ok = (ND <= 3 || j > i)
+                                    ? in_shell<ND>(&x[i * ND], &x[j * ND], Di, Dj, g.box, g.inv_box, t_shell)
+                                    : in_shell<ND>(&x[i * ND], &x[j * ND], Dj, Di, g.box, g.inv_box, t_shell);
                 if (ok) rows[i].push_back(static_cast<std::uint32_t>(j));
             }
         }
