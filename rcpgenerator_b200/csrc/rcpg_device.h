@@ -46,7 +46,9 @@ struct DevCtl {
     std::uint32_t cap_error_particle;
     std::uint32_t cap_error_cap;
     std::uint32_t nbuilds;        // pair-list builds performed
-    std::uint32_t pad0;
+    std::uint32_t fuse_forces;    // a tiled build also computes the step's forces (graph mode)
+    std::uint32_t forces_done;    // this step's forces were computed by the build
+    std::uint32_t nsum_blocks;    // number of valid entries in block_sums
     std::uint64_t graph_steps;    // steps completed by the controller kernel
 };
 

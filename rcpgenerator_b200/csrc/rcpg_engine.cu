@@ -96,7 +96,9 @@ void Engine::alloc_device() {
     a_.cell_count = static_cast<std::uint32_t*>(dalloc((a_.C_alloc + 1ull) * 4));
     a_.cell_start = static_cast<std::uint32_t*>(dalloc((a_.C_alloc + 1ull) * 4));
     a_.scan_tmp = static_cast<std::uint32_t*>(dalloc(2 * 4096 * 4 + 64));
-    a_.block_sums = static_cast<ForceSums*>(dalloc(force_blocks(N) * sizeof(ForceSums)));
+    // per-block partial sums: one per force block, or one per block of the
+    // persistent tiled build when it computes the forces
+    a_.block_sums = static_cast<ForceSums*>(dalloc(std::max<std::size_t>(force_blocks(N), 4096) * sizeof(ForceSums)));
     a_.pterm_cnt = static_cast<std::uint32_t*>(dalloc(N * 4));
     for (int b = 0; b < 2; ++b) {
         a_.sort_keys[b] = static_cast<std::uint64_t*>(dalloc(N * 8));
@@ -205,6 +207,7 @@ void Engine::publish_step_params() {
     hctl_.build_t_shell = c.t_shell;
     hctl_.build_Dmax = c.Dmax_cur;
     hctl_.theta = c.theta;
+    hctl_.forces_done = 0u;
     if (c.rebuild_mode == REBUILD_FULL) {
         hctl_.rebuild_flag = 1u;
     } else {
@@ -253,6 +256,7 @@ void Engine::upload_initial() {
     hctl_.force_kappa = 1.0;
     hctl_.force_mu = host_c_.mu;
     hctl_.rebuild_flag = 1u;
+    hctl_.fuse_forces = 0u;  // set for the graph loop once the run starts
     push_ctl();
 
     // initial spatial reorder + full build (ENG:4992-5009), initial forces (ENG:5011-5013)
@@ -326,6 +330,7 @@ void Engine::profile_pair_kernel(std::uint32_t reps, double* avg_ms, double* alg
     const DevCtl saved = hctl_;
     hctl_.stopped = 0u;
     hctl_.halted = 0u;
+    hctl_.forces_done = 0u;
     push_ctl();
     // every launch starts from a cold L2: a 256 MiB write evicts the previous
     // launch's lines (L2 is 126 MB), then the launch alone is timed
@@ -383,6 +388,8 @@ void Engine::do_reorder_and_rebuild() {
     hctl_.build_Dmax = xmul(c.D0_max, kp);
     hctl_.rebuild_flag = 1u;
     hctl_.stopped = 0u;
+    const std::uint32_t fuse = hctl_.fuse_forces;
+    hctl_.fuse_forces = 0u;  // this build uses the previous step's diameters
     push_ctl();
     launch_reorder(a_, st_);
     launches_ += 3 + 8 * 4 + 3;
@@ -395,6 +402,8 @@ void Engine::do_reorder_and_rebuild() {
         hctl_.rebuild_flag = 1u;
         push_ctl();
     }
+    hctl_.fuse_forces = fuse;
+    hctl_.forces_done = 0u;
 }
 
 // Target-phi lock (ENG:5783-5832): D0 := D rescaled to the target, kappa := 1.
@@ -592,6 +601,7 @@ bool Engine::advance_graph(std::uint64_t max_new_steps) {
         hctl_.c = c;
         hctl_.stopped = 0u;
         hctl_.halted = 0u;
+        hctl_.fuse_forces = 1u;  // rebuild steps compute their forces in the tiled build
         push_ctl();
         launch_controller(a_, 1, st_);
         ++launches_;

@@ -61,6 +61,61 @@ __device__ __forceinline__ int cell_coord(double x, double scale, int nc) {
     return c >= nc ? nc - 1 : c;
 }
 
+// ---- deterministic reductions of ForceSums ---------------------------------
+__device__ __forceinline__ double shfl_down_d(double v, int o) {
+    return __shfl_down_sync(0xffffffffu, v, o);
+}
+
+__device__ __forceinline__ void warp_reduce_sums(ForceSums& s) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s.pair_U = xadd(s.pair_U, shfl_down_d(s.pair_U, o));
+        s.pair_Lc = xadd(s.pair_Lc, shfl_down_d(s.pair_Lc, o));
+        s.pair_dk = xadd(s.pair_dk, shfl_down_d(s.pair_dk, o));
+        s.pair_Fm = xadd(s.pair_Fm, shfl_down_d(s.pair_Fm, o));
+        s.pair_maxov = fmax(s.pair_maxov, shfl_down_d(s.pair_maxov, o));
+        s.wall_U = xadd(s.wall_U, shfl_down_d(s.wall_U, o));
+        s.wall_dk = xadd(s.wall_dk, shfl_down_d(s.wall_dk, o));
+        s.wall_Fm = xadd(s.wall_Fm, shfl_down_d(s.wall_Fm, o));
+        s.sum_mag = xadd(s.sum_mag, shfl_down_d(s.sum_mag, o));
+        s.sum_D = xadd(s.sum_D, shfl_down_d(s.sum_D, o));
+        s.pair_count += __shfl_down_sync(0xffffffffu, s.pair_count, o);
+        s.wall_count += __shfl_down_sync(0xffffffffu, s.wall_count, o);
+        s.mag_count += __shfl_down_sync(0xffffffffu, s.mag_count, o);
+    }
+}
+
+__device__ __forceinline__ void sums_add(ForceSums& a, const ForceSums& b) {
+    a.pair_U = xadd(a.pair_U, b.pair_U);
+    a.pair_Lc = xadd(a.pair_Lc, b.pair_Lc);
+    a.pair_dk = xadd(a.pair_dk, b.pair_dk);
+    a.pair_Fm = xadd(a.pair_Fm, b.pair_Fm);
+    a.pair_maxov = fmax(a.pair_maxov, b.pair_maxov);
+    a.wall_U = xadd(a.wall_U, b.wall_U);
+    a.wall_dk = xadd(a.wall_dk, b.wall_dk);
+    a.wall_Fm = xadd(a.wall_Fm, b.wall_Fm);
+    a.sum_mag = xadd(a.sum_mag, b.sum_mag);
+    a.sum_D = xadd(a.sum_D, b.sum_D);
+    a.pair_count += b.pair_count;
+    a.wall_count += b.wall_count;
+    a.mag_count += b.mag_count;
+}
+
+// Deterministic block reduction (fixed shuffle tree, warps combined in order).
+template <int NT>
+__device__ __forceinline__ void block_reduce_sums(ForceSums& s, ForceSums* smem) {
+    warp_reduce_sums(s);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) smem[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ForceSums t = smem[0];
+#pragma unroll
+        for (int w = 1; w < NT / 32; ++w) sums_add(t, smem[w]);
+        s = t;
+    }
+}
+
 // ===========================================================================
 // A. ADAM step of the finished step + refresh trigger of the next step
 // ===========================================================================
@@ -143,6 +198,8 @@ __global__ void k_build_prepare(DevArrays a) {
         ctl->ncells = cells;
         // every rebuild re-anchors every particle (x_last is written by k_bin)
         ctl->kappa_min = ctl->build_kappa;
+        // graph mode: the tiled build also computes this step's forces
+        ctl->forces_done = ctl->fuse_forces;
         ctl->row_need = 0u;
         ctl->nbuilds += 1u;
     }
@@ -299,6 +356,7 @@ template <int ND>
 __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
     DevCtl* ctl = a.ctl;
     if (ctl_idle(ctl) || !ctl->rebuild_flag || tiled_build_ok<ND>(ctl)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->forces_done = 0u;
     __shared__ std::uint32_t buf[kSearchSmemRow * kSearchBlock];
     __shared__ std::uint32_t block_need;
     if (threadIdx.x == 0) block_need = 0u;
@@ -425,15 +483,15 @@ template <> struct TileShape<3> {
     static constexpr int stage = 1280;
 };
 constexpr int kTileThreads = 256;
-constexpr int kTileRow = 24;
+constexpr int kTileRow = 32;
 
 // dynamic shared memory of k_build_search_tiled<ND>
 template <int ND>
 constexpr std::size_t tile_smem_bytes() {
     using TS = TileShape<ND <= 3 ? ND : 3>;
     return static_cast<std::size_t>(TS::stage) * pos_stride(ND) * 8 + 2ull * TS::stage * 4 +
-           static_cast<std::size_t>(kTileRow) * kTileThreads * 4 + (TS::halo_cells + 2) * 4 +
-           static_cast<std::size_t>(TS::stage) * 2;
+           (TS::halo_cells + 2) * 4 + 2ull * TS::stage * 2 +
+           static_cast<std::size_t>(kTileRow) * kTileThreads * 2;
 }
 
 template <int ND>
@@ -454,7 +512,7 @@ __device__ __forceinline__ void finish_row(std::uint32_t* mine, int stride, int 
         return;
     }
     nbr_cnt[q] = n;
-    if (n <= static_cast<std::uint32_t>(smem_cap)) {
+    if (smem_cap > 0 && n <= static_cast<std::uint32_t>(smem_cap)) {
         for (std::uint32_t k = 1; k < n; ++k) {
             const std::uint32_t v = mine[k * stride];
             std::uint32_t p = k;
@@ -468,7 +526,7 @@ __device__ __forceinline__ void finish_row(std::uint32_t* mine, int stride, int 
     } else {
         for (std::uint32_t k = 0; k < static_cast<std::uint32_t>(smem_cap); ++k)
             nbr[static_cast<std::uint64_t>(k) * N + q] = mine[k * stride];
-        std::uint32_t* row = nbr + q;
+        std::uint32_t* row = nbr + q;  // insertion sort of the whole row in place
         for (std::uint32_t k = 1; k < n; ++k) {
             const std::uint32_t v = row[static_cast<std::uint64_t>(k) * N];
             std::uint32_t p = k;
@@ -481,8 +539,12 @@ __device__ __forceinline__ void finish_row(std::uint32_t* mine, int stride, int 
     }
 }
 
+// Fused build (graph mode): when a step rebuilds its pair list, the forces of
+// that step are computed right here from the staged (current) positions, in
+// the same ascending-partner order as k_forces, so F is bit-identical and the
+// separate force pass is skipped (ctl->forces_done).
 template <int ND>
-__global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a) {
+__global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArrays a) {
     constexpr int NDT = ND <= 3 ? ND : 3;
     using TS = TileShape<NDT>;
     constexpr int P = pos_stride(ND);
@@ -495,15 +557,18 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
     double* s_pos = reinterpret_cast<double*>(tile_smem);
     std::uint32_t* s_id = reinterpret_cast<std::uint32_t*>(s_pos + STAGE * P);
     std::uint32_t* s_slot = s_id + STAGE;
-    std::uint32_t* s_rows = s_slot + STAGE;
-    std::uint32_t* s_cstart = s_rows + kTileRow * kTileThreads;
-    std::uint16_t* s_cell = reinterpret_cast<std::uint16_t*>(s_cstart + HC + 2);
+    std::uint32_t* s_cstart = s_slot + STAGE;
+    std::uint16_t* s_inner = reinterpret_cast<std::uint16_t*>(s_cstart + HC + 2);
+    std::uint16_t* s_cell = s_inner + STAGE;
+    std::uint16_t* s_rows = s_cell + STAGE;  // [kTileRow][kTileThreads] staged indices
     __shared__ std::uint32_t s_warp[kTileThreads / 32];
-    __shared__ std::uint32_t s_total, s_need;
+    __shared__ std::uint32_t s_need, s_ninner;
+    __shared__ ForceSums s_red[kTileThreads / 32];
     const std::uint64_t N = a.N;
     const std::uint32_t S = a.S;
     const Geometry g = ctl->g;  // register copy: the loops below store through other pointers
     const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
+    const bool fuse = ctl->forces_done != 0u;
     int nc[ND], nt[ND];
     std::uint32_t tiles = 1;
     RCPG_UNROLL
@@ -513,7 +578,10 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
         tiles *= static_cast<std::uint32_t>(nt[d]);
     }
     if (threadIdx.x == 0) s_need = 0u;
-    std::uint32_t* mine = s_rows + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) ctl->nsum_blocks = gridDim.x;
+    std::uint16_t* mine = s_rows + threadIdx.x;
+    ForceSums fs;
+    sums_zero(fs);
     for (std::uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         int t0[ND], hw[ND];
         std::uint32_t rem = tile;
@@ -528,15 +596,18 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
             H *= hw[d];
         }
         __syncthreads();  // the previous tile is done with shared memory
-        // 1. particle count of every halo cell, 2. block scan -> staging offsets
+        // 1. particle count of every halo cell, 2. block scans -> staging offsets
         std::uint32_t cs = 0, cnt = 0;
+        bool inner_cell = false;
         if (static_cast<int>(threadIdx.x) < H) {
             int r = threadIdx.x;
             std::uint32_t c = 0, mul = 1;
+            inner_cell = true;
             RCPG_UNROLL
             for (int d = 0; d < ND; ++d) {
                 const int l = r % hw[d];
                 r /= hw[d];
+                inner_cell = inner_cell && l >= 1 && l <= hw[d] - 2;
                 int gc = t0[d] - 1 + l;
                 if (gc < 0) gc += nc[d];
                 else if (gc >= nc[d]) gc -= nc[d];
@@ -548,13 +619,15 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
         }
         std::uint32_t total;
         const std::uint32_t off = block_exclusive_scan(cnt, s_warp, total);
+        std::uint32_t ninner;
+        const std::uint32_t ioff = block_exclusive_scan(inner_cell ? cnt : 0u, s_warp, ninner);
         if (static_cast<int>(threadIdx.x) < H) s_cstart[threadIdx.x] = off;
         if (threadIdx.x == 0) {
             s_cstart[H] = total;
-            s_total = total;
+            s_ninner = ninner;
         }
         const bool fits = total <= static_cast<std::uint32_t>(STAGE);
-        // 3. stage the halo particles (one thread per halo cell)
+        // 3. stage the halo particles (one thread per halo cell) and list the tile's own
         if (fits && static_cast<int>(threadIdx.x) < H) {
             for (std::uint32_t k = 0; k < cnt; ++k) {
                 const std::uint32_t q = cs + k, dst = off + k;
@@ -565,69 +638,14 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
                 s_id[dst] = a.cell_list[q];
                 s_slot[dst] = q;
                 s_cell[dst] = static_cast<std::uint16_t>(threadIdx.x);
+                if (inner_cell) s_inner[ioff + k] = static_cast<std::uint16_t>(dst);
             }
         }
         __syncthreads();
-        if (fits) {
-            // 4. rows of the tile's own particles, candidates from shared memory
-            for (std::uint32_t k = threadIdx.x; k < total; k += blockDim.x) {
-                int hl[ND];
-                int r = s_cell[k];
-                bool inner = true;
-                RCPG_UNROLL
-                for (int d = 0; d < ND; ++d) {
-                    hl[d] = r % hw[d];
-                    r /= hw[d];
-                    inner = inner && hl[d] >= 1 && hl[d] <= hw[d] - 2;
-                }
-                if (!inner) continue;
-                const std::uint32_t i = s_id[k];
-                const std::uint64_t q = s_slot[k];
-                double xi[ND], D0i;
-                load_pos<ND>(s_pos, k, xi, D0i);
-                const double Di = xmul(D0i, kap);
-                std::uint32_t n = 0, n_half = 0;
-                constexpr int NCOMBO = (ND == 2) ? 9 : 27;
-                int odo[ND];
-                RCPG_UNROLL
-                for (int d = 0; d < ND; ++d) odo[d] = 0;
-                for (int combo = 0; combo < NCOMBO; ++combo) {
-                    int hc = 0, mul = 1;
-                    RCPG_UNROLL
-                    for (int d = 0; d < ND; ++d) {
-                        hc += (hl[d] - 1 + odo[d]) * mul;
-                        mul *= hw[d];
-                    }
-                    RCPG_UNROLL
-                    for (int d = 0; d < ND; ++d) {
-                        if (++odo[d] < 3) break;
-                        odo[d] = 0;
-                    }
-                    const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 1];
-                    for (std::uint32_t pp = p0; pp < p1; ++pp) {
-                        if (pp == k) continue;
-                        const std::uint32_t j = s_id[pp];
-                        double xj[ND], D0j;
-                        load_pos<ND>(s_pos, pp, xj, D0j);
-                        const double Dj = xmul(D0j, kap);
-                        const bool ok = in_shell<ND>(xi, xj, Di, Dj, g.box, g.inv_box, t_shell);
-                        if (!ok) continue;
-                        if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = j;
-                        else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
-                        ++n;
-                        if (j > i) ++n_half;
-                    }
-                }
-                const std::uint32_t cap = a.caps[i];
-                if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-                    ctl->cap_error_particle = i;
-                    ctl->cap_error_cap = cap;
-                }
-                atomicMax(&s_need, n);
-                finish_row(mine, kTileThreads, kTileRow, n, S, a.nbr, a.nbr_cnt, N, q);
-            }
-        } else {
-            // more halo particles than the staging area: rows of this tile from global memory
+        if (!fits) {
+            // more halo particles than the staging area: rows of this tile from
+            // global memory, and the forces of this step by the separate pass
+            if (threadIdx.x == 0) ctl->forces_done = 0u;
             for (int h = threadIdx.x; h < H; h += blockDim.x) {
                 int hl[ND];
                 int r = h;
@@ -651,29 +669,32 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
                     load_pos<ND>(a.spos, q, xi, D0i);
                     const double Di = xmul(D0i, kap);
                     std::uint32_t n = 0, n_half = 0;
+                    int odo[ND];
+                    RCPG_UNROLL
+                    for (int d = 0; d < ND; ++d) odo[d] = 0;
                     constexpr int NCOMBO = (ND == 2) ? 9 : 27;
                     for (int combo = 0; combo < NCOMBO; ++combo) {
-                        int cr = combo;
                         std::uint32_t cn = 0, mm = 1;
                         RCPG_UNROLL
                         for (int d = 0; d < ND; ++d) {
-                            int gc = t0[d] - 1 + hl[d] - 1 + cr % 3;
-                            cr /= 3;
+                            int gc = t0[d] - 1 + hl[d] - 1 + odo[d];
                             if (gc < 0) gc += nc[d];
                             else if (gc >= nc[d]) gc -= nc[d];
                             cn += static_cast<std::uint32_t>(gc) * mm;
                             mm *= static_cast<std::uint32_t>(nc[d]);
+                        }
+                        RCPG_UNROLL
+                        for (int d = 0; d < ND; ++d) {
+                            if (++odo[d] < 3) break;
+                            odo[d] = 0;
                         }
                         for (std::uint32_t pp = a.cell_start[cn]; pp < a.cell_start[cn + 1]; ++pp) {
                             const std::uint32_t j = a.cell_list[pp];
                             if (j == i) continue;
                             double xj[ND], D0j;
                             load_pos<ND>(a.spos, pp, xj, D0j);
-                            const double Dj = xmul(D0j, kap);
-                            const bool ok = in_shell<ND>(xi, xj, Di, Dj, g.box, g.inv_box, t_shell);
-                            if (!ok) continue;
-                            if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = j;
-                            else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
+                            if (!in_shell<ND>(xi, xj, Di, xmul(D0j, kap), g.box, g.inv_box, t_shell)) continue;
+                            if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
                             ++n;
                             if (j > i) ++n_half;
                         }
@@ -684,77 +705,136 @@ __global__ void __launch_bounds__(kTileThreads) k_build_search_tiled(DevArrays a
                         ctl->cap_error_cap = cap;
                     }
                     atomicMax(&s_need, n);
-                    finish_row(mine, kTileThreads, kTileRow, n, S, a.nbr, a.nbr_cnt, N, q);
+                    finish_row(nullptr, 0, 0, n, S, a.nbr, a.nbr_cnt, N, q);
                 }
+            }
+            continue;
+        }
+        // 4. rows (and forces) of the tile's own particles from shared memory
+        for (std::uint32_t u = threadIdx.x; u < s_ninner; u += blockDim.x) {
+            const std::uint32_t k = s_inner[u];
+            int hl[ND];
+            {
+                int r = s_cell[k];
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    hl[d] = r % hw[d];
+                    r /= hw[d];
+                }
+            }
+            const std::uint32_t i = s_id[k];
+            const std::uint64_t q = s_slot[k];
+            double xi[ND], D0i;
+            load_pos<ND>(s_pos, k, xi, D0i);
+            const double Di = xmul(D0i, kap);
+            std::uint32_t n = 0, n_half = 0;
+            int odo[ND];
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) odo[d] = 0;
+            constexpr int NCOMBO = (ND == 2) ? 9 : 27;
+            for (int combo = 0; combo < NCOMBO; ++combo) {
+                int hc = 0, mul = 1;
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    hc += (hl[d] - 1 + odo[d]) * mul;
+                    mul *= hw[d];
+                }
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    if (++odo[d] < 3) break;
+                    odo[d] = 0;
+                }
+                const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 1];
+                for (std::uint32_t pp = p0; pp < p1; ++pp) {
+                    if (pp == k) continue;
+                    double xj[ND], D0j;
+                    load_pos<ND>(s_pos, pp, xj, D0j);
+                    if (!in_shell<ND>(xi, xj, Di, xmul(D0j, kap), g.box, g.inv_box, t_shell)) continue;
+                    const std::uint32_t j = s_id[pp];
+                    if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = static_cast<std::uint16_t>(pp);
+                    else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
+                    ++n;
+                    if (j > i) ++n_half;
+                }
+            }
+            const std::uint32_t cap = a.caps[i];
+            if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
+                ctl->cap_error_particle = i;
+                ctl->cap_error_cap = cap;
+            }
+            atomicMax(&s_need, n);
+            if (n <= static_cast<std::uint32_t>(kTileRow)) {
+                // sort the staged indices by particle id, write the row
+                for (std::uint32_t e = 1; e < n; ++e) {
+                    const std::uint16_t v = mine[e * kTileThreads];
+                    const std::uint32_t vid = s_id[v];
+                    std::uint32_t p = e;
+                    while (p > 0 && s_id[mine[(p - 1) * kTileThreads]] > vid) {
+                        mine[p * kTileThreads] = mine[(p - 1) * kTileThreads];
+                        --p;
+                    }
+                    mine[p * kTileThreads] = v;
+                }
+                a.nbr_cnt[q] = n;
+                for (std::uint32_t e = 0; e < n; ++e)
+                    a.nbr[static_cast<std::uint64_t>(e) * N + q] = s_id[mine[e * kTileThreads]];
+                if (fuse) {
+                    double fi[ND];
+                    RCPG_UNROLL
+                    for (int d = 0; d < ND; ++d) fi[d] = 0.0;
+                    for (std::uint32_t e = 0; e < n; ++e) {
+                        const std::uint32_t pp = mine[e * kTileThreads];
+                        double xj[ND], D0j;
+                        load_pos<ND>(s_pos, pp, xj, D0j);
+                        PairTerms pt;
+                        if (!pair_force<ND>(xi, Di, xj, xmul(D0j, kap), g, fi, pt)) continue;
+                        if (s_id[pp] > i) {
+                            fs.pair_U = xadd(fs.pair_U, pt.U);
+                            fs.pair_Lc = xadd(fs.pair_Lc, pt.Lc);
+                            fs.pair_dk = xadd(fs.pair_dk, pt.dk);
+                            fs.pair_Fm = xadd(fs.pair_Fm, pt.Fm);
+                            fs.pair_maxov = fmax(fs.pair_maxov, pt.U);
+                            fs.pair_count += 1ull;
+                        }
+                    }
+                    wall_forces<ND>(xi, Di, g, fi, fs.wall_U, fs.wall_dk, fs.wall_Fm, fs.wall_count);
+                    const double f2 = force_norm2<ND>(fi);
+                    if (f2 > 1.0E-16) {
+                        fs.sum_mag = xadd(fs.sum_mag, xsqrt(f2));
+                        fs.mag_count += 1ull;
+                    }
+                    fs.sum_D = xadd(fs.sum_D, Di);
+                    RCPG_UNROLL
+                    for (int d = 0; d < ND; ++d) a.F[static_cast<std::uint64_t>(i) * ND + d] = fi[d];
+                }
+            } else {
+                // long row: the first kTileRow entries go to the global row too,
+                // sorted there; its forces come from the separate pass
+                if (n <= S)
+                    for (std::uint32_t e = 0; e < static_cast<std::uint32_t>(kTileRow); ++e)
+                        a.nbr[static_cast<std::uint64_t>(e) * N + q] = s_id[mine[e * kTileThreads]];
+                finish_row(nullptr, 0, 0, n, S, a.nbr, a.nbr_cnt, N, q);
+                ctl->forces_done = 0u;
             }
         }
     }
     __syncthreads();
     if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
+    if (fuse) {
+        block_reduce_sums<kTileThreads>(fs, s_red);
+        if (threadIdx.x == 0) a.block_sums[blockIdx.x] = fs;
+    }
 }
 
 // ===========================================================================
 // C. forces + walls + per-block sums
 // ===========================================================================
-__device__ __forceinline__ double shfl_down_d(double v, int o) {
-    return __shfl_down_sync(0xffffffffu, v, o);
-}
-
-__device__ __forceinline__ void warp_reduce_sums(ForceSums& s) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s.pair_U = xadd(s.pair_U, shfl_down_d(s.pair_U, o));
-        s.pair_Lc = xadd(s.pair_Lc, shfl_down_d(s.pair_Lc, o));
-        s.pair_dk = xadd(s.pair_dk, shfl_down_d(s.pair_dk, o));
-        s.pair_Fm = xadd(s.pair_Fm, shfl_down_d(s.pair_Fm, o));
-        s.pair_maxov = fmax(s.pair_maxov, shfl_down_d(s.pair_maxov, o));
-        s.wall_U = xadd(s.wall_U, shfl_down_d(s.wall_U, o));
-        s.wall_dk = xadd(s.wall_dk, shfl_down_d(s.wall_dk, o));
-        s.wall_Fm = xadd(s.wall_Fm, shfl_down_d(s.wall_Fm, o));
-        s.sum_mag = xadd(s.sum_mag, shfl_down_d(s.sum_mag, o));
-        s.sum_D = xadd(s.sum_D, shfl_down_d(s.sum_D, o));
-        s.pair_count += __shfl_down_sync(0xffffffffu, s.pair_count, o);
-        s.wall_count += __shfl_down_sync(0xffffffffu, s.wall_count, o);
-        s.mag_count += __shfl_down_sync(0xffffffffu, s.mag_count, o);
-    }
-}
-
-__device__ __forceinline__ void sums_add(ForceSums& a, const ForceSums& b) {
-    a.pair_U = xadd(a.pair_U, b.pair_U);
-    a.pair_Lc = xadd(a.pair_Lc, b.pair_Lc);
-    a.pair_dk = xadd(a.pair_dk, b.pair_dk);
-    a.pair_Fm = xadd(a.pair_Fm, b.pair_Fm);
-    a.pair_maxov = fmax(a.pair_maxov, b.pair_maxov);
-    a.wall_U = xadd(a.wall_U, b.wall_U);
-    a.wall_dk = xadd(a.wall_dk, b.wall_dk);
-    a.wall_Fm = xadd(a.wall_Fm, b.wall_Fm);
-    a.sum_mag = xadd(a.sum_mag, b.sum_mag);
-    a.sum_D = xadd(a.sum_D, b.sum_D);
-    a.pair_count += b.pair_count;
-    a.wall_count += b.wall_count;
-    a.mag_count += b.mag_count;
-}
-
-// Deterministic block reduction (fixed shuffle tree, warps combined in order).
-template <int NT>
-__device__ __forceinline__ void block_reduce_sums(ForceSums& s, ForceSums* smem) {
-    warp_reduce_sums(s);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) smem[warp] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ForceSums t = smem[0];
-#pragma unroll
-        for (int w = 1; w < NT / 32; ++w) sums_add(t, smem[w]);
-        s = t;
-    }
-}
-
 template <int ND>
 __global__ void __launch_bounds__(kForceBlock) k_forces(DevArrays a, int exact_terms) {
     const DevCtl* ctl = a.ctl;
     __shared__ ForceSums red[kForceBlock / 32];
-    if (ctl_idle(ctl)) return;
+    if (ctl_idle(ctl) || ctl->forces_done) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->nsum_blocks = gridDim.x;
     const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
     const std::uint64_t N = a.N;
     ForceSums s;
@@ -878,7 +958,7 @@ __global__ void k_reduce_exact(DevArrays a) {
 constexpr int kCtlThreads = 1024;
 
 __device__ void reduce_blocks(const DevArrays& a, ForceSums* smem, ForceSums& out) {
-    const unsigned nb = force_blocks(a.N);
+    const unsigned nb = a.ctl->nsum_blocks;
     ForceSums s;
     sums_zero(s);
     for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) sums_add(s, a.block_sums[b]);
@@ -897,6 +977,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_reduce_fast(DevArrays a) {
 
 // Parameters of the kernels of the step that begin_step() just opened.
 __device__ void publish_step(DevCtl* ctl, const Controller& c, int ndim) {
+    ctl->forces_done = 0u;
     for (int d = 0; d < ndim; ++d) {
         ctl->g.box[d] = c.box[d];
         ctl->g.inv_box[d] = 1.0 / c.box[d];
@@ -1211,6 +1292,7 @@ __global__ void k_refresh_arrays(std::uint64_t N, const double* __restrict__ x, 
 template <int ND>
 __global__ void __launch_bounds__(kForceBlock) k_mean_force_blocks(DevArrays a) {
     __shared__ ForceSums red[kForceBlock / 32];
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->nsum_blocks = gridDim.x;
     const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
     ForceSums s;
     sums_zero(s);
@@ -1258,17 +1340,21 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     k_build_cell_sort<ND><<<(a.C_alloc + 255) / 256, 256, 0, st>>>(a);
     const unsigned sb = static_cast<unsigned>((a.N + kSearchBlock - 1) / kSearchBlock);
     if (ND <= 3) {
-        int dev = 0, sms = 148;
+        // persistent grid: as many blocks as fit on the GPU at once
+        int dev = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         constexpr std::size_t smem = tile_smem_bytes<ND>();
-        static bool attr_set[64][2] = {};
-        if (dev >= 0 && dev < 64 && !attr_set[dev][ND - 2]) {
+        static int grid[64][2] = {};
+        if (dev >= 0 && dev < 64 && grid[dev][ND - 2] == 0) {
             cudaFuncSetAttribute(k_build_search_tiled<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem));
-            attr_set[dev][ND - 2] = true;
+            int sms = 148, per_sm = 1;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_search_tiled<ND>, kTileThreads, smem);
+            grid[dev][ND - 2] = sms * (per_sm > 0 ? per_sm : 1);
         }
-        k_build_search_tiled<ND><<<static_cast<unsigned>(sms) * 3u, kTileThreads, smem, st>>>(a);
+        const int blocks = (dev >= 0 && dev < 64) ? grid[dev][ND - 2] : 148;
+        k_build_search_tiled<ND><<<static_cast<unsigned>(blocks), kTileThreads, smem, st>>>(a);
     }
     k_build_search<ND><<<sb, kSearchBlock, 0, st>>>(a);
 }
