@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
     if (threadIdx.x == 0 && block_need) atomicMax(&ctl->row_need, block_need);
     if (t >= N) return;
     if (n > S) {
-        a.nbr_cnt[t] = S;
+        a.nbr_cnt[t] = 0;  // overflow: empty row, rebuilt after the capacity grows
         return;
     }
     a.nbr_cnt[t] = n;
@@ -508,7 +508,10 @@ __device__ __forceinline__ void finish_row(std::uint32_t* mine, int stride, int 
                                            std::uint32_t n, std::uint32_t S, std::uint32_t* nbr,
                                            std::uint32_t* nbr_cnt, std::uint64_t N, std::uint64_t q) {
     if (n > S) {
-        nbr_cnt[q] = S;
+        // overflow: the row is incomplete. It is published empty, so that no
+        // reader can meet an unwritten entry; the build reports row_need > S
+        // and the caller rebuilds with a larger row capacity.
+        nbr_cnt[q] = 0;
         return;
     }
     nbr_cnt[q] = n;
@@ -539,10 +542,6 @@ __device__ __forceinline__ void finish_row(std::uint32_t* mine, int stride, int 
     }
 }
 
-// Fused build (graph mode): when a step rebuilds its pair list, the forces of
-// that step are computed right here from the staged (current) positions, in
-// the same ascending-partner order as k_forces, so F is bit-identical and the
-// separate force pass is skipped (ctl->forces_done).
 template <int ND>
 __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArrays a) {
     constexpr int NDT = ND <= 3 ? ND : 3;
@@ -763,7 +762,10 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                 ctl->cap_error_cap = cap;
             }
             atomicMax(&s_need, n);
-            if (n <= static_cast<std::uint32_t>(kTileRow)) {
+            if (n > S) {
+                a.nbr_cnt[q] = 0;  // overflow: empty row, rebuilt after the capacity grows
+                ctl->forces_done = 0u;
+            } else if (n <= static_cast<std::uint32_t>(kTileRow)) {
                 // sort the staged indices by particle id, write the row
                 for (std::uint32_t e = 1; e < n; ++e) {
                     const std::uint16_t v = mine[e * kTileThreads];
@@ -808,11 +810,10 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                     for (int d = 0; d < ND; ++d) a.F[static_cast<std::uint64_t>(i) * ND + d] = fi[d];
                 }
             } else {
-                // long row: the first kTileRow entries go to the global row too,
-                // sorted there; its forces come from the separate pass
-                if (n <= S)
-                    for (std::uint32_t e = 0; e < static_cast<std::uint32_t>(kTileRow); ++e)
-                        a.nbr[static_cast<std::uint64_t>(e) * N + q] = s_id[mine[e * kTileThreads]];
+                // long row (kTileRow < n <= S): the first kTileRow entries go to
+                // the global row too, sorted there; its forces come from the separate pass
+                for (std::uint32_t e = 0; e < static_cast<std::uint32_t>(kTileRow); ++e)
+                    a.nbr[static_cast<std::uint64_t>(e) * N + q] = s_id[mine[e * kTileThreads]];
                 finish_row(nullptr, 0, 0, n, S, a.nbr, a.nbr_cnt, N, q);
                 ctl->forces_done = 0u;
             }
@@ -850,7 +851,7 @@ __global__ void __launch_bounds__(kForceBlock) k_forces(DevArrays a, int exact_t
         double fi[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) fi[d] = 0.0;
-        const std::uint32_t n = a.nbr_cnt[t];
+        const std::uint32_t n = min(a.nbr_cnt[t], a.S);
         std::uint32_t nterm = 0;
         // Partners in chunks of kChunk: the row ids and then the partner
         // positions of a chunk are loaded before any of its arithmetic, so a
@@ -865,11 +866,12 @@ __global__ void __launch_bounds__(kForceBlock) k_forces(DevArrays a, int exact_t
                 jj[u] = (k0 + u < n) ? __ldg(a.nbr + static_cast<std::uint64_t>(k0 + u) * N + t) : 0u;
             RCPG_UNROLL
             for (std::uint32_t u = 0; u < kChunk; ++u)
-                if (k0 + u < n) load_pos<ND>(a.pos, jj[u], xj[u], D0j[u]);
+                if (k0 + u < n && jj[u] < N) load_pos<ND>(a.pos, jj[u], xj[u], D0j[u]);
             RCPG_UNROLL
             for (std::uint32_t u = 0; u < kChunk; ++u) {
                 if (k0 + u >= n) break;
                 const std::uint32_t j = jj[u];
+                if (j >= N) continue;
                 PairTerms pt;
                 if (!pair_force<ND>(xi, Di, xj[u], xmul(D0j[u], kap), g, fi, pt)) continue;
                 if (j > i) {
