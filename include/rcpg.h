@@ -177,6 +177,27 @@ int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const dou
                         uint32_t row_capacity, uint32_t* nbr_dev, uint32_t* cnt_dev,
                         uint32_t* row_need_out, void* stream, char* err, size_t errlen);
 
+/* rcpg_pairs_full without device allocation. No counterpart in the reference
+ * (its engine allocates host memory only). For callers that must not
+ * allocate device memory while they run: applications whose device memory is
+ * reserved up front by their own allocator, where an extra cudaMalloc fails or
+ * fragments the pool, and time-critical loops, where cudaMalloc / cudaFree
+ * would synchronise the device and stall other streams. Same arguments and
+ * results as rcpg_pairs_full; the caller still passes every input and output.
+ * The scratch is a fixed 8 MiB array of static device memory that every GPU
+ * loading this library keeps until the process exits. A working set larger
+ * than that -- about N*(16*P + 8*ndim + 20 + 4*row_capacity) bytes plus the
+ * cell grid, P = 4 for ndim <= 3, i.e. roughly 20,000 particles in 3-D at
+ * row_capacity 64 -- is rejected with RCPG_ENOSPC before any work. The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and should be made before any stream capture. All calls share the array and
+ * it keeps the previous call's contents (the build clears what must start at
+ * zero); calls whose GPU work overlaps in time race and must be serialised. */
+int32_t rcpg_pairs_full_noalloc(uint64_t N, int32_t ndim, const double* x_dev, const double* D_dev,
+                                const double* box, const int8_t* walls, double t_shell,
+                                uint32_t row_capacity, uint32_t* nbr_dev, uint32_t* cnt_dev,
+                                uint32_t* row_need_out, void* stream, char* err, size_t errlen);
+
 /* get_forces_nd_3 (rcp_generator.hpp:218-243) on rows from rcpg_pairs_full
  * (any superset of the overlapping pairs gives the same result), followed by
  * compute_mean_force (:150-155). Writes F_dev [N*ndim] and

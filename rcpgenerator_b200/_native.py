@@ -37,6 +37,7 @@ EXPORTED_SYMBOLS = (
     "rcpg_engine_profile_pair_kernel",
     "rcpg_t_shell",
     "rcpg_pairs_full",
+    "rcpg_pairs_full_noalloc",
     "rcpg_forces",
     "rcpg_mean_force",
     "rcpg_adam_step",
@@ -188,6 +189,11 @@ def _load() -> C.CDLL:
         ),
         "rcpg_t_shell": (C.c_double, [_dp, C.c_uint64]),
         "rcpg_pairs_full": (
+            C.c_int32,
+            [C.c_uint64, C.c_int32, vp, vp, _dp, _i8p, C.c_double, C.c_uint32, vp, vp, _u32p, vp,
+             cp, sz],
+        ),
+        "rcpg_pairs_full_noalloc": (
             C.c_int32,
             [C.c_uint64, C.c_int32, vp, vp, _dp, _i8p, C.c_double, C.c_uint32, vp, vp, _u32p, vp,
              cp, sz],
