@@ -71,6 +71,10 @@ KERNEL_CASES = [
                           dist={"type": "mono", "d": 1.0}, seed=8), 500),
 ]
 
+_FH_RNG = np.random.default_rng(60)
+_FH_POS = np.column_stack([_FH_RNG.uniform(0.0, 20.0, 60), _FH_RNG.uniform(0.0, 4.0, 60)])
+_FH_D = np.where(_FH_RNG.uniform(size=60) < 0.5, 1.0, 1.4)
+
 PACK_CASES = [
     ("n4_2d", {"positions": [[0.10, 0.10], [0.35, 0.25], [0.70, 0.55], [0.82, 0.85]],
                "diameters": [0.12, 0.10, 0.09, 0.08]},
@@ -91,6 +95,22 @@ PACK_CASES = [
                           dist={"type": "mono", "d": 1.0}, seed=8), None, {"max_steps": 1500}),
     ("cfg1_n2000_3d", dict(phi=0.08, N=2000, Ndim=3, box=[1.0, 1.0, 1.0], walls=[0, 0, 0],
                            dist={"type": "mono", "d": 1.0}, seed=123), None, {}),
+    # relax() options (PackingRunOptions, rcp_generator.hpp:102-123)
+    ("n64_2d_target_phi", dict(phi=0.1, N=64, Ndim=2, box=[1.0, 1.0], walls=[0, 0],
+                               dist={"type": "bidisperse", "d1": 1.0, "d2": 1.4, "p": 0.5}, seed=5),
+     None, {"max_steps": 2500, "target_phi": 0.7}),
+    ("n64_3d_fix_diameter", dict(phi=0.3, N=64, Ndim=3, box=[1.0, 1.0, 1.0], walls=[0, 0, 0],
+                                 dist={"type": "mono", "d": 1.0}, seed=6),
+     None, {"max_steps": 1500, "fix_diameter": True}),
+    ("n100_2d_mu", dict(phi=0.1, N=100, Ndim=2, box=[1.0, 1.0], walls=[0, 0],
+                        dist={"type": "mono", "d": 1.0}, seed=7), None, {"max_steps": 1500, "mu": 1e-3}),
+    # fix_height: diameters of order one, box height given in units of D[0] (rcp_generator.cpp:4460-4491)
+    ("n60_2d_fix_height_wall", {"positions": _FH_POS.tolist(), "diameters": _FH_D.tolist()},
+     {"box": [20.0, 4.0], "walls": [0, 1], "neighbor_max": 0, "seed": 0, "fix_height": True},
+     {"max_steps": 1500}),
+    ("n80_2d_no_reorder", dict(phi=0.1, N=80, Ndim=2, box=[1.0, 1.0], walls=[0, 0],
+                               dist={"type": "mono", "d": 1.0}, seed=9), None,
+     {"max_steps": 2500, "reorder_interval": 0}),
 ]
 
 
@@ -190,6 +210,9 @@ def main() -> None:
         packs[name + "/box_in"] = np.asarray(cfg["box"], dtype=np.float64)
         packs[name + "/walls_in"] = np.asarray(cfg["walls"], dtype=np.int8)
         packs[name + "/max_steps"] = np.asarray(opts.get("max_steps", 0))
+        packs[name + "/fix_height"] = np.asarray(bool(cfg.get("fix_height", False)))
+        for k, v in opts.items():  # run options, one array per key (PackingRunOptions)
+            packs[name + "/opt/" + k] = np.asarray(v)
         packs[name + "/positions"] = np.asarray(r["positions"], dtype=np.float64)
         packs[name + "/diameters"] = np.asarray(r["diameters"], dtype=np.float64)
         packs[name + "/particle_origin"] = np.asarray(r["particle_origin"], dtype=np.uint64)

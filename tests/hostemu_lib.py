@@ -16,7 +16,8 @@ class HostEmu:
         self.lib = C.CDLL(str(LIB))
         self.lib.hostemu_run_packing.restype = C.c_int
 
-    def run(self, positions, diameters, box, walls, max_steps=0, neighbor_max=0, reorder=2000):
+    def run(self, positions, diameters, box, walls, max_steps=0, neighbor_max=0, reorder=2000,
+            fix_height=False, mu=None, fix_diameter=False):
         pos = np.ascontiguousarray(positions, dtype=np.float64)
         N, nd = pos.shape
         D = np.ascontiguousarray(diameters, dtype=np.float64)
@@ -32,7 +33,8 @@ class HostEmu:
             C.c_uint64(N), C.c_int(nd), pos.ctypes.data_as(_dp), D.ctypes.data_as(_dp),
             box.ctypes.data_as(_dp) if box is not None else None,
             walls.ctypes.data_as(C.POINTER(C.c_int8)) if walls is not None else None,
-            C.c_uint32(neighbor_max), 0, C.c_uint64(max_steps), C.c_double(0.0), 0, 0,
+            C.c_uint32(neighbor_max), int(bool(fix_height)), C.c_uint64(max_steps),
+            C.c_double(0.0 if mu is None else mu), int(mu is not None), int(bool(fix_diameter)),
             C.c_uint64(reorder), po.ctypes.data_as(_dp), do.ctypes.data_as(_dp), ho.ctypes.data_as(_dp),
             C.c_uint64(cap), oo.ctypes.data_as(C.POINTER(C.c_uint64)), so.ctypes.data_as(_dp))
         assert rc == 0

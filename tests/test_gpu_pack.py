@@ -18,7 +18,8 @@ pytestmark = pytest.mark.gpu
 HIST = ("phi_history", "force_history", "energy_history", "max_overlap_history", "mu_history",
         "alpha_history")
 CASES = ["n4_2d", "n16_2d", "n64_3d_bi", "n64_2d_walls_500", "n128_3d_sphere_3000",
-         "n200_2d_disk_2500", "n300_4d_1500", "cfg1_n2000_3d"]
+         "n200_2d_disk_2500", "n300_4d_1500", "cfg1_n2000_3d", "n64_2d_target_phi",
+         "n64_3d_fix_diameter", "n100_2d_mu", "n60_2d_fix_height_wall", "n80_2d_no_reorder"]
 
 
 def digest(a):
@@ -29,11 +30,9 @@ def run(g, case, engine, extra=None):
     import rcpgenerator_b200 as rb
     inp = {"positions": g[f"{case}/input_positions"], "diameters": g[f"{case}/input_diameters"]}
     cfg = {"box": g[f"{case}/box_in"].tolist(), "walls": g[f"{case}/walls_in"].tolist(),
-           "neighbor_max": 0, "engine": engine}
-    opts = {}
-    ms = int(g[f"{case}/max_steps"])
-    if ms:
-        opts["max_steps"] = ms
+           "neighbor_max": 0, "engine": engine, "fix_height": bool(g[f"{case}/fix_height"])}
+    pre = f"{case}/opt/"
+    opts = {k[len(pre):]: g[k][()].item() for k in g.files if k.startswith(pre)}
     opts.update(extra or {})
     return rb.run_packing_observed(inp, cfg, 0, False, 0, None, opts, as_arrays=True)["result"]
 

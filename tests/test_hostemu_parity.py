@@ -12,11 +12,18 @@ import pytest
 HIST = ("phi_history", "force_history", "energy_history", "max_overlap_history", "mu_history",
         "alpha_history")
 FAST = ["n4_2d", "n16_2d", "n64_3d_bi", "n64_2d_walls_500", "n128_3d_sphere_3000",
-        "n200_2d_disk_2500", "n300_4d_1500"]
+        "n200_2d_disk_2500", "n300_4d_1500", "n64_3d_fix_diameter", "n100_2d_mu",
+        "n60_2d_fix_height_wall", "n80_2d_no_reorder"]
 
 
 def digest(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def case_options(g, case):
+    """Run options the golden packing was made with (PackingRunOptions keys)."""
+    pre = f"{case}/opt/"
+    return {k[len(pre):]: g[k][()] for k in g.files if k.startswith(pre)}
 
 
 def check_pack(r, g, case):
@@ -36,6 +43,9 @@ def check_pack(r, g, case):
 @pytest.mark.parametrize("case", FAST)
 def test_emulation_reproduces_reference_pack(hostemu, golden, case):
     g = golden("packs.npz")
+    o = case_options(g, case)
     r = hostemu.run(g[f"{case}/input_positions"], g[f"{case}/input_diameters"], g[f"{case}/box_in"],
-                    g[f"{case}/walls_in"], max_steps=int(g[f"{case}/max_steps"]))
+                    g[f"{case}/walls_in"], max_steps=int(g[f"{case}/max_steps"]),
+                    reorder=int(o.get("reorder_interval", 2000)), fix_height=bool(g[f"{case}/fix_height"]),
+                    mu=float(o["mu"]) if "mu" in o else None, fix_diameter=bool(o.get("fix_diameter", False)))
     check_pack(r, g, case)
