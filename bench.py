@@ -39,6 +39,10 @@ WORKLOAD = dict(phi=0.30, N=1_000_000, Ndim=2, box=[1.0, 1.0], walls=[0, 0],
 PEAKS = REPO / "MEASURED_PEAKS.json"
 
 
+def workload_name(n: int) -> str:
+    return f"bidisperse2d_N{n:.0e}_phi0.30_seed123".replace("e+0", "e")
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -157,7 +161,7 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "bidisperse2d_N1e6_phi0.30_seed123", "N": WORKLOAD["N"], "Ndim": 2,
+        "config": {"workload": workload_name(WORKLOAD["N"]), "N": WORKLOAD["N"], "Ndim": 2,
                    "engine": "reference C++/OpenMP run_packing_observed, portable build",
                    "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
@@ -177,7 +181,13 @@ def main() -> int:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--pair-precision", default="mixed", choices=["mixed", "f64"],
+                    help="pair arithmetic: mixed = FP32 pair terms while the max overlap >= 1e-5 "
+                         "(the workload's stated precision), f64 = FP64 throughout")
+    ap.add_argument("--n", type=int, default=WORKLOAD["N"], help="particles (smaller cases for profiling)")
     args = ap.parse_args()
+    WORKLOAD["N"] = args.n
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -193,9 +203,9 @@ def main() -> int:
 
     pos, dia, init = make_input(rank)
     stream = torch.cuda.Stream()
-    eng = rb.PackingEngine({"positions": pos, "diameters": dia},
-                           {"box": init["box"], "walls": init["walls"], "device": local}, {},
-                           stream=stream.cuda_stream)
+    run_cfg = {"box": init["box"], "walls": init["walls"], "device": local,
+               "pair_precision": args.pair_precision}
+    eng = rb.PackingEngine({"positions": pos, "diameters": dia}, run_cfg, {}, stream=stream.cuda_stream)
     eng.advance(args.warmup)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
@@ -226,12 +236,13 @@ def main() -> int:
 
     # end to end through the public API: host buffers in, results out
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    r2 = rb.run_packing_observed({"positions": pos, "diameters": dia},
-                                 {"box": init["box"], "walls": init["walls"], "device": local},
-                                 0, False, 0, None, {"max_steps": args.steps}, as_arrays=True)["result"]
-    t_e2e = time.perf_counter() - t0
-    e2e_steps = int(r2["steps"])
+    e2e_steps, t_e2e = 0, 0.0
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        r2 = rb.run_packing_observed({"positions": pos, "diameters": dia}, run_cfg,
+                                     0, False, 0, None, {"max_steps": args.steps}, as_arrays=True)["result"]
+        t_e2e = time.perf_counter() - t0
+        e2e_steps = int(r2["steps"])
 
     if rank != 0:
         if world > 1:
@@ -256,9 +267,13 @@ def main() -> int:
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done_steps,
         "warmup": args.warmup, "ms_per_step": ms / max(done_steps, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "bidisperse2d_N1e6_phi0.30_seed123", "N": n, "Ndim": nd,
-                   "engine": "graph", "parallelism": f"replicas{world}",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 state, f32 pair terms" if args.pair_precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": workload_name(n), "N": n, "Ndim": nd,
+                   "engine": "graph", "pair_precision": args.pair_precision,
+                   "fp64_switch_step": int(res["engine_stats"]["fp64_switch_step"]),
+                   "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (~150 MB touched per step)",
                    "pair_builds": int(res["engine_stats"]["pair_builds"]),
                    "row_capacity": int(res["engine_stats"]["row_capacity"])},
@@ -268,7 +283,7 @@ def main() -> int:
                      "alg_bytes_per_launch": prof["alg_bytes"], "avg_launch_ms": prof["avg_ms"],
                      "mean_row": prof["mean_row"]},
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_steps / t_e2e, "unit": UNIT,
+        "e2e": None if args.no_e2e else {"value": e2e_steps / t_e2e, "unit": UNIT,
                 "h2d_bytes_per_step": int((n * (nd + 1) * 8) / max(e2e_steps, 1)),
                 "d2h_bytes_per_step": int((n * (nd + 2) * 8 + e2e_steps * 6 * 8) / max(e2e_steps, 1)),
                 "note": "run_packing_observed(max_steps=K) from host NumPy arrays: setup, K steps, results"},

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define RCPG_ABI_VERSION 1
+#define RCPG_ABI_VERSION 2
 
 #define RCPG_OK 0
 #define RCPG_ERUNTIME (-1)
@@ -75,6 +75,13 @@ typedef struct rcpg_run_options {
     int32_t exact;               /* 1: host-controlled steps + one-thread reduction order */
     int32_t device;              /* CUDA device ordinal */
     int32_t graph_steps;         /* steps per CUDA graph replay (graph mode), 0 = default */
+    /* Pair arithmetic, graph mode only (no counterpart in the reference, which is FP64):
+     * 0 = FP64 (default); 1 = mixed -- FP32 pair terms on FP64 displacements until the
+     * first step whose max overlap (relative, as max_overlap_history) is below
+     * mixed_switch, FP64 from that step on. Positions, ADAM state, diameters and all
+     * global sums stay FP64. */
+    int32_t pair_precision;
+    double mixed_switch;         /* default 1e-5 */
 } rcpg_run_options;
 
 /* PackingObservation (rcp_generator.hpp:92-98). */
@@ -122,6 +129,13 @@ typedef struct rcpg_result {
     uint64_t pair_builds;      /* neighbour-list builds performed */
     uint32_t row_capacity;     /* neighbour row capacity in use at the end */
     uint64_t kernel_launches;  /* kernels launched by this run */
+    /* mixed precision (pair_precision = 1): the step after which the pair terms were
+     * FP64 (0 = never switched), and the relative error, on the final state, of the
+     * pair energy sum and of the forces (max |F32 - F64| / max |F64|) with FP32 pair
+     * terms against FP64 ones on the same rows. NaN when the run was FP64. */
+    uint64_t fp64_switch_step;
+    double pair_energy_rel_error;
+    double pair_force_rel_error;
 } rcpg_result;
 
 const char* rcpg_version(void);

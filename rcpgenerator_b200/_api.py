@@ -159,6 +159,11 @@ class _Inputs:
         ro.exact = 1 if engine == "exact" else 0
         ro.device = int(config.get("device", opts.get("device", 0)))
         ro.graph_steps = int(config.get("graph_steps", opts.get("graph_steps", 32)))
+        prec = str(config.get("pair_precision", opts.get("pair_precision", "f64")))
+        if prec not in ("f64", "mixed"):
+            raise ValueError(f"unknown pair_precision {prec!r} (expected 'f64' or 'mixed')")
+        ro.pair_precision = 1 if prec == "mixed" else 0
+        ro.mixed_switch = float(config.get("mixed_switch", opts.get("mixed_switch", 1e-5)))
         self.ro = ro
 
 
@@ -204,6 +209,9 @@ def result_to_dict(r: N.Result, as_arrays: bool = False) -> dict:
         "pair_builds": int(r.pair_builds),
         "row_capacity": int(r.row_capacity),
         "kernel_launches": int(r.kernel_launches),
+        "fp64_switch_step": int(r.fp64_switch_step),
+        "pair_energy_rel_error": float(r.pair_energy_rel_error),
+        "pair_force_rel_error": float(r.pair_force_rel_error),
     }
     return out
 

@@ -83,6 +83,8 @@ class RunOptions(C.Structure):
         ("exact", C.c_int32),
         ("device", C.c_int32),
         ("graph_steps", C.c_int32),
+        ("pair_precision", C.c_int32),
+        ("mixed_switch", C.c_double),
     ]
 
 
@@ -130,6 +132,9 @@ class Result(C.Structure):
         ("pair_builds", C.c_uint64),
         ("row_capacity", C.c_uint32),
         ("kernel_launches", C.c_uint64),
+        ("fp64_switch_step", C.c_uint64),
+        ("pair_energy_rel_error", C.c_double),
+        ("pair_force_rel_error", C.c_double),
     ]
 
 

@@ -83,6 +83,8 @@ rcpg::EngineInput make_input(const rcpg_packing_input* in, const rcpg_run_option
     e.exact = o.exact != 0;
     e.device = o.device;
     e.graph_steps = o.graph_steps;
+    e.pair_precision = o.pair_precision;
+    e.mixed_switch = o.mixed_switch > 0.0 ? o.mixed_switch : 1e-5;
     return e;
 }
 
@@ -120,6 +122,9 @@ rcpg_result* make_result(const rcpg::EngineResult& r, std::uint64_t N, int ndim,
     out->pair_builds = r.builds;
     out->row_capacity = r.row_capacity;
     out->kernel_launches = launches;
+    out->fp64_switch_step = r.fp64_switch_step;
+    out->pair_energy_rel_error = r.pair_energy_rel_error;
+    out->pair_force_rel_error = r.pair_force_rel_error;
     if (trace && !trace->empty()) {
         const std::size_t T = trace->size();
         out->trace_len = T;
@@ -210,6 +215,8 @@ void rcpg_default_options(rcpg_run_options* opt) {
     opt->reorder_interval = 2000;
     opt->initial_phi_target = 0.55;
     opt->graph_steps = 32;
+    opt->pair_precision = 0;
+    opt->mixed_switch = 1e-5;
 }
 
 int32_t rcpg_run_packing(const rcpg_packing_input* in, const rcpg_run_options* opt,
@@ -347,6 +354,7 @@ int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const dou
         a.nbr = static_cast<std::uint32_t*>(sc.get(static_cast<std::size_t>(row_capacity) * N * 4));
         a.nbr_cnt = static_cast<std::uint32_t*>(sc.get(N * 4));
         a.S = row_capacity;
+        a.sorted_rows = 1;  // the reference's row order
         a.caps = static_cast<std::uint32_t*>(sc.get(N * 4));
         a.cell_of = static_cast<std::uint32_t*>(sc.get(N * 4));
         a.cell_rank = static_cast<std::uint32_t*>(sc.get(N * 4));

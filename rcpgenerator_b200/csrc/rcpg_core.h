@@ -97,6 +97,13 @@ struct Geometry {
 // symmetric bit for bit (the minimum image of -a is exactly -(image of a)),
 // and so is r_c for ndim <= 3; only the ndim > 3 cutoff depends on the order.
 template <int ND>
+RCPG_HD double shell_cut(double D_lo, double D_hi, double t_shell) {
+    if (ND <= 3) return xadd(xmul(xadd(D_lo, D_hi), 0.5), t_shell);
+    const float half_f = static_cast<float>(xmul(D_hi, 0.5));
+    return xadd(xadd(xmul(D_lo, 0.5), t_shell), static_cast<double>(half_f));
+}
+
+template <int ND>
 RCPG_HD bool in_shell(const double* xi, const double* xj, double D_lo, double D_hi,
                       const double* box, const double* inv_box, double t_shell) {
     double d2 = 0.0;
@@ -139,20 +146,24 @@ struct PairTerms {
     double U, Lc, dk, Fm;
 };
 
-// One overlapping pair seen from particle i with partner j (dx = x_j - x_i
-// after MIC). Returns false when the pair does not overlap. ENG:4086-4139.
+// MIC displacement dx = x_j - x_i and its squared length, accumulated in the
+// reference's order (ENG:4097-4104); the shell test and the force share it.
 template <int ND>
-RCPG_HD bool pair_force(const double* xi, double Di, const double* xj, double Dj,
-                        const Geometry& g, double* fi, PairTerms& pt) {
-    const double r_ij = xmul(0.5, xadd(Di, Dj));
-    double dx[ND];
+RCPG_HD double pair_disp(const double* xi, const double* xj, const double* box, const double* inv_box,
+                         double* dx) {
     double d2 = 0.0;
 RCPG_UNROLL
     for (int d = 0; d < ND; ++d) {
-        dx[d] = mic(xsub(xj[d], xi[d]), g.inv_box[d], g.box[d]);
+        dx[d] = mic(xsub(xj[d], xi[d]), inv_box[d], box[d]);
         d2 = xadd(d2, xmul(dx[d], dx[d]));
     }
-    if (!(d2 < xmul(r_ij, r_ij))) return false;
+    return d2;
+}
+
+// Force and scalar terms of an overlapping pair (d2 < r_ij^2) from its
+// displacement, FP64 as in the reference (ENG:4105-4139).
+template <int ND>
+RCPG_HD void pair_terms_f64(const double* dx, double d2, double r_ij, double* fi, PairTerms& pt) {
     const double dist = xsqrt(d2);
     const double F_mag = -xsub(xdiv(r_ij, dist), 1.0);
 RCPG_UNROLL
@@ -161,6 +172,70 @@ RCPG_UNROLL
     pt.Lc = r_ij;
     pt.dk = xmul(r_ij, xsub(dist, r_ij));
     pt.Fm = F_mag;
+}
+
+#if defined(__CUDACC__)
+// ---- mixed-precision pair arithmetic (graph mode, pair_precision = mixed) --
+// Differences are formed in FP64 and rounded to FP32; everything after that
+// is FP32. Both directions of a pair see exactly negated displacements and the
+// same d2, so both agree on membership and overlap and the forces cancel.
+
+// Relative widening of the FP32 shell test (r_c^2): it covers the rounding of
+// d2 and r_c in FP32 (about 1e-6 relative), so a row holds every pair of the
+// FP64 shell; the few extra pairs just outside it are harmless (the forces
+// count overlapping pairs only).
+constexpr float kShellMarginF = 1.00001f;
+
+// dx = x_j - x_i in FP64, rounded to FP32, with the minimum image taken by one
+// box length when |dx| exceeds half the box (pairs never reach 1.5 boxes).
+// Returns d2 in FP32.
+template <int ND>
+__device__ __forceinline__ float mixed_disp(const double* xi, const double* xj, const double* box,
+                                            const float* half_box, float* dxf) {
+    float d2 = 0.0f;
+RCPG_UNROLL
+    for (int d = 0; d < ND; ++d) {
+        double dd = xsub(xj[d], xi[d]);
+        float f = __double2float_rn(dd);
+        if (fabsf(f) > half_box[d]) {
+            dd = f > 0.0f ? xsub(dd, box[d]) : xadd(dd, box[d]);
+            f = __double2float_rn(dd);
+        }
+        dxf[d] = f;
+        d2 = __fmaf_rn(f, f, d2);
+    }
+    return d2;
+}
+
+// Force and scalar terms of an overlapping pair (d2 < rsum^2, rsum = r_ij) in
+// FP32 (ENG:4105-4139 with FP32 operands); the force is added to the FP32
+// per-particle sum fi, the scalar terms go to the FP64 accumulators. The
+// overlap-dependent terms carry a relative error of about 1e-7 / overlap.
+template <int ND>
+__device__ __forceinline__ void pair_terms_mixed(const float* dxf, float d2, float rsum, float* fi,
+                                                 PairTerms& pt) {
+    const float inv_dist = rsqrtf(d2);
+    const float dist = d2 * inv_dist;
+    const float F_mag = __fmaf_rn(-rsum, inv_dist, 1.0f);  // -(r/dist - 1)
+RCPG_UNROLL
+    for (int d = 0; d < ND; ++d) fi[d] = __fmaf_rn(F_mag, dxf[d], fi[d]);
+    pt.U = static_cast<double>(1.0f - __fdividef(dist, rsum));
+    pt.Lc = static_cast<double>(rsum);
+    pt.dk = static_cast<double>(rsum * (dist - rsum));
+    pt.Fm = static_cast<double>(F_mag);
+}
+#endif
+
+// One overlapping pair seen from particle i with partner j (dx = x_j - x_i
+// after MIC). Returns false when the pair does not overlap. ENG:4086-4139.
+template <int ND>
+RCPG_HD bool pair_force(const double* xi, double Di, const double* xj, double Dj,
+                        const Geometry& g, double* fi, PairTerms& pt) {
+    const double r_ij = xmul(0.5, xadd(Di, Dj));
+    double dx[ND];
+    const double d2 = pair_disp<ND>(xi, xj, g.box, g.inv_box, dx);
+    if (!(d2 < xmul(r_ij, r_ij))) return false;
+    pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
     return true;
 }
 
@@ -168,9 +243,9 @@ RCPG_UNROLL
 // force after all pair terms, in the reference's order (ENG:4198-4257:
 // axes ascending, wall 0 then wall 1, then the container). The scalar
 // contributions are added in that same order to the three wall_* sums.
-template <int ND>
+template <int ND, typename CountT>
 RCPG_HD void wall_forces(const double* xi, double Di, const Geometry& g, double* fi,
-                         double& U, double& dk, double& Fm, unsigned long long& count) {
+                         double& U, double& dk, double& Fm, CountT& count) {
     if (g.any_flat_wall) {
 RCPG_UNROLL
         for (int d = 0; d < ND; ++d) {

@@ -50,6 +50,12 @@ struct DevCtl {
     std::uint32_t forces_done;    // this step's forces were computed by the build
     std::uint32_t nsum_blocks;    // number of valid entries in block_sums
     std::uint64_t graph_steps;    // steps completed by the controller kernel
+    // mixed-precision pair arithmetic (graph mode): FP32 pair terms while the
+    // max overlap of the last step is >= mixed_switch, FP64 from then on
+    std::uint32_t pair_fp32;      // the forces of the current step use FP32 pair terms
+    std::uint32_t pad0;
+    double mixed_switch;
+    std::uint64_t fp64_switch_step;  // step whose max overlap fell below mixed_switch (0: none)
 };
 
 struct DevArrays {
@@ -64,7 +70,7 @@ struct DevArrays {
     double* v;              // [N*ndim]
     double* vec_tmp;        // [N*ndim] reorder gather target
     double* x_last;         // [N*ndim] refresh anchor positions
-    std::uint32_t* nbr;     // [S*N] column-major full rows, ascending partner index
+    std::uint32_t* nbr;     // [S*N] column-major full rows (see sorted_rows)
     std::uint32_t* nbr_cnt; // [N]
     // Row slot -> particle map. Row t (nbr[k*N + t], nbr_cnt[t]) belongs to
     // particle work[t]; the engine keeps rows in cell order (work = cell_list)
@@ -72,6 +78,12 @@ struct DevArrays {
     // nullptr = identity (rows in particle order).
     const std::uint32_t* work;
     std::uint32_t S;        // row capacity
+    // 1: rows sorted by partner index (exact mode, pairs_full: the reference's
+    // summation order); 0: rows in the build's fixed scan order (graph mode)
+    int sorted_rows;
+    // 1: the run may use FP32 pair terms (mixed precision), so the force
+    // kernel is launched in both variants; each checks ctl->pair_fp32
+    int mixed;
     std::uint32_t* caps;    // [N] half-row capacity of the reference layout
     std::uint64_t* origin;  // [N] particle_origin
     std::uint64_t* u64_tmp; // [N]

@@ -40,6 +40,8 @@ void Engine::setup_host(const EngineInput& in) {
     // the target-phi lock rescales every diameter on the host, so runs that
     // can lock are host-controlled
     exact_ = in.exact || in.has_target_phi;
+    mixed_ = !exact_ && in.pair_precision == 1;
+    mixed_switch_ = in.mixed_switch;
     graph_steps_ = in.graph_steps > 0 ? in.graph_steps : 32;
     device_ = in.device;
     RunSetup s = prepare_run(in);
@@ -84,6 +86,9 @@ void Engine::alloc_device() {
     a_.cell_rank = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.cell_list = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.work = a_.cell_list;  // rows are kept in the cell order of their build
+    // exact mode sums each row in ascending partner order, as the reference
+    a_.sorted_rows = exact_ ? 1 : 0;
+    a_.mixed = mixed_ ? 1 : 0;
     // cell grid capacity: the grid at the initial (smallest) cutoff
     {
         const double cutoff = (host_c_.Dmax_cur + host_c_.t_shell) * (1.0 + 1e-6);
@@ -257,6 +262,8 @@ void Engine::upload_initial() {
     hctl_.force_mu = host_c_.mu;
     hctl_.rebuild_flag = 1u;
     hctl_.fuse_forces = 0u;  // set for the graph loop once the run starts
+    hctl_.pair_fp32 = 0u;    // the initial energy is FP64; the graph loop may switch to mixed
+    hctl_.mixed_switch = mixed_switch_;
     push_ctl();
 
     // initial spatial reorder + full build (ENG:4992-5009), initial forces (ENG:5011-5013)
@@ -602,6 +609,7 @@ bool Engine::advance_graph(std::uint64_t max_new_steps) {
         hctl_.stopped = 0u;
         hctl_.halted = 0u;
         hctl_.fuse_forces = 1u;  // rebuild steps compute their forces in the tiled build
+        hctl_.pair_fp32 = mixed_ ? 1u : 0u;
         push_ctl();
         launch_controller(a_, 1, st_);
         ++launches_;
@@ -780,7 +788,44 @@ EngineResult Engine::result() {
     pull_ctl();
     r.builds = hctl_.nbuilds;
     r.row_capacity = a_.S;
+    r.fp64_switch_step = hctl_.fp64_switch_step;
+    r.pair_energy_rel_error = r.pair_force_rel_error = std::nan("");
+    if (mixed_) pair_precision_error(&r.pair_energy_rel_error, &r.pair_force_rel_error);
     return r;
+}
+
+void Engine::pair_precision_error(double* energy_rel, double* force_rel) {
+    pull_ctl();
+    const DevCtl saved = hctl_;
+    const std::uint64_t n = N_ * static_cast<std::uint64_t>(ndim_);
+    check(cudaMemcpyAsync(a_.vec_tmp, a_.F, n * 8, cudaMemcpyDeviceToDevice, st_), "save F");
+    std::vector<double> F[2];
+    double U[2] = {0.0, 0.0};
+    for (int prec = 0; prec < 2; ++prec) {  // 0: FP64, 1: FP32 pair terms
+        hctl_ = saved;
+        hctl_.stopped = 0u;
+        hctl_.halted = 0u;
+        hctl_.forces_done = 0u;
+        hctl_.pair_fp32 = static_cast<std::uint32_t>(prec);
+        push_ctl();
+        launch_forces(a_, 0, st_);
+        launch_reduce_fast(a_, st_);
+        launches_ += 2;
+        F[prec].resize(n);
+        check(cudaMemcpyAsync(F[prec].data(), a_.F, n * 8, cudaMemcpyDeviceToHost, st_), "D2H F");
+        pull_ctl();
+        U[prec] = hctl_.sums.pair_U;
+    }
+    double fmax = 0.0, dmax = 0.0;
+    for (std::uint64_t k = 0; k < n; ++k) {
+        fmax = std::max(fmax, std::fabs(F[0][k]));
+        dmax = std::max(dmax, std::fabs(F[1][k] - F[0][k]));
+    }
+    *energy_rel = U[0] != 0.0 ? std::fabs(U[1] - U[0]) / std::fabs(U[0]) : std::fabs(U[1]);
+    *force_rel = fmax > 0.0 ? dmax / fmax : dmax;
+    check(cudaMemcpyAsync(a_.F, a_.vec_tmp, n * 8, cudaMemcpyDeviceToDevice, st_), "restore F");
+    hctl_ = saved;
+    push_ctl();
 }
 
 void Engine::observe(std::uint64_t step, bool capture, const ObserverFn& observer,

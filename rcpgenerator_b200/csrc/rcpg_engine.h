@@ -34,6 +34,11 @@ struct EngineResult {
     // engine statistics
     std::uint64_t builds = 0;
     std::uint32_t row_capacity = 0;
+    // mixed precision: step after which the pair terms were FP64 (0: never
+    // switched), and the relative error of the final state's energy sum and
+    // forces with FP32 pair terms against FP64 ones (NaN when not mixed)
+    std::uint64_t fp64_switch_step = 0;
+    double pair_energy_rel_error = 0.0, pair_force_rel_error = 0.0;
 };
 
 struct TraceSample {
@@ -82,6 +87,10 @@ class Engine {
     // duration and the kernel's algorithmic bytes per launch.
     void profile_pair_kernel(std::uint32_t reps, double* avg_ms, double* alg_bytes,
                              double* mean_row);
+    // Mixed precision: the final state's forces evaluated with FP32 and with
+    // FP64 pair terms on the same rows; relative difference of the pair
+    // energy sum and max |F32 - F64| / max |F64|. Leaves the state unchanged.
+    void pair_precision_error(double* energy_rel, double* force_rel);
 
    private:
     void setup_host(const EngineInput& in);
@@ -112,6 +121,8 @@ class Engine {
     int ndim_ = 0;
     int P_ = 0;
     bool exact_ = false;
+    bool mixed_ = false;          // FP32 pair terms until the max overlap falls below mixed_switch_
+    double mixed_switch_ = 1e-5;
     int graph_steps_ = 32;
     int device_ = 0;
     cudaStream_t st_ = nullptr;

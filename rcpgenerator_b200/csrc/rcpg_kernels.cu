@@ -1,17 +1,19 @@
 // CUDA kernels of the packing step (sm_100a).
 //
-// One thread per particle everywhere except the controller (one warp) and the
+// One thread per particle everywhere except the controller (one block) and the
 // scans / radix sort. The pair list is a full list (both directions) stored
-// column-major, nbr[k*N + i], each row sorted by partner index, so a warp
-// reading entry k of 32 consecutive rows issues one coalesced 128-byte load,
-// and every particle sums its pair forces in ascending partner order -- the
-// order in which the reference's one-thread loop accumulates them -- without
-// atomics. Pair scalars (energy, dkappa, ...) are counted once per pair, by
-// the lower index.
+// column-major, nbr[k*N + t], so a warp reading entry k of 32 consecutive rows
+// issues one coalesced 128-byte load, and every particle sums its own pair
+// forces without atomics. In exact mode each row is sorted by partner index,
+// the order in which the reference's one-thread loop accumulates the forces;
+// in graph mode a row keeps the build's fixed scan order (deterministic run to
+// run). Pair scalars (energy, dkappa, ...) are counted once per pair, by the
+// lower index.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <stdexcept>
+#include <type_traits>
 
 #include "rcpg_device.h"
 
@@ -19,8 +21,19 @@ namespace rcpg {
 
 namespace {
 
+// Early-exit guards. The flags are combined with bitwise operators so that
+// all of their loads are issued before the first branch: one round trip to
+// memory per block instead of one per flag (kernels that have nothing to do
+// in a step otherwise cost several microseconds at N = 1M).
 __device__ __forceinline__ bool ctl_idle(const DevCtl* ctl) {
-    return ctl->stopped != 0u || ctl->halted != 0u;
+    const std::uint32_t st = ctl->stopped, ha = ctl->halted;
+    return (st | ha) != 0u;
+}
+
+// no pair-list build in this step
+__device__ __forceinline__ bool build_off(const DevCtl* ctl) {
+    const std::uint32_t st = ctl->stopped, ha = ctl->halted, rb = ctl->rebuild_flag;
+    return ((st | ha) != 0u) | (rb == 0u);
 }
 
 template <int ND>
@@ -119,45 +132,73 @@ __device__ __forceinline__ void block_reduce_sums(ForceSums& s, ForceSums* smem)
 // ===========================================================================
 // A. ADAM step of the finished step + refresh trigger of the next step
 // ===========================================================================
+// Persistent grid (resident_grid): each thread loads the step's parameters
+// once and then walks the particles with a grid stride, two at a time, so the
+// loads of both are in flight together.
 template <int ND>
 __global__ void __launch_bounds__(256) k_adam_refresh(DevArrays a, int do_adam, int do_refresh) {
-    DevCtl* ctl = a.ctl;
-    if (ctl->halted) return;
-    const bool adam = do_adam && ctl->adam_go;
-    const bool refresh = do_refresh && !ctl->stopped && ctl->c.rebuild_mode == REBUILD_CHECK;
+    const DevCtl* ctl = a.ctl;
+    const std::uint32_t halted = ctl->halted, adam_go = ctl->adam_go, stopped = ctl->stopped;
+    const int mode = ctl->c.rebuild_mode;
+    if (halted) return;
+    const bool adam = do_adam && adam_go;
+    const bool refresh = do_refresh && !stopped && mode == REBUILD_CHECK;
     if (!adam && !refresh) return;
-    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    const double alpha = ctl->adam_alpha, ib1 = ctl->adam_inv_b1, ib2 = ctl->adam_inv_b2;
+    const double fh = ctl->fix_height_scale;
+    const double rk = ctl->refresh_kappa, kmin = ctl->kappa_min, theta = ctl->theta;
+    double abox[ND];
+    RCPG_UNROLL
+    for (int d = 0; d < ND; ++d) abox[d] = ctl->adam_box[d];
+    const std::uint64_t N = a.N;
+    const std::uint64_t stride = static_cast<std::uint64_t>(gridDim.x) * blockDim.x;
     bool trig = false;
-    if (i < a.N) {
-        double x[ND], D0;
-        load_pos<ND>(a.pos, i, x, D0);
-        if (adam) {
-            const double alpha = ctl->adam_alpha, ib1 = ctl->adam_inv_b1, ib2 = ctl->adam_inv_b2;
+    for (std::uint64_t i0 = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x; i0 < N;
+         i0 += 2 * stride) {
+        constexpr int U = 2;
+        double x[U][ND], D0[U], F[U][ND], m[U][ND], v[U][ND], xl[U][ND];
+        RCPG_UNROLL
+        for (int u = 0; u < U; ++u) {
+            const std::uint64_t i = i0 + u * stride;
+            if (i >= N) continue;
+            load_pos<ND>(a.pos, i, x[u], D0[u]);
             RCPG_UNROLL
             for (int d = 0; d < ND; ++d) {
-                const std::uint64_t idx = i * ND + d;
-                double mm = a.m[idx], vv = a.v[idx];
-                x[d] = adam_coord(a.F[idx], mm, vv, x[d], alpha, ib1, ib2, ctl->adam_box[d]);
-                a.m[idx] = mm;
-                a.v[idx] = vv;
+                if (adam) {
+                    F[u][d] = a.F[i * ND + d];
+                    m[u][d] = a.m[i * ND + d];
+                    v[u][d] = a.v[i * ND + d];
+                }
+                if (refresh) xl[u][d] = a.x_last[i * ND + d];
             }
-            if (ctl->fix_height_scale != 1.0) x[ND - 1] = xmul(x[ND - 1], ctl->fix_height_scale);
-            store_pos<ND>(a.pos, i, x, D0);
         }
-        if (refresh) {
-            double d2 = 0.0;
-            RCPG_UNROLL
-            for (int d = 0; d < ND; ++d) {
-                const double dd = xsub(x[d], a.x_last[i * ND + d]);
-                d2 = xadd(d2, xmul(dd, dd));
+        RCPG_UNROLL
+        for (int u = 0; u < U; ++u) {
+            const std::uint64_t i = i0 + u * stride;
+            if (i >= N) continue;
+            if (adam) {
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    x[u][d] = adam_coord(F[u][d], m[u][d], v[u][d], x[u][d], alpha, ib1, ib2, abox[d]);
+                    a.m[i * ND + d] = m[u][d];
+                    a.v[i * ND + d] = v[u][d];
+                }
+                if (fh != 1.0) x[u][ND - 1] = xmul(x[u][ND - 1], fh);
+                store_pos<ND>(a.pos, i, x[u], D0[u]);
             }
-            const double D = xmul(D0, ctl->refresh_kappa);
-            const double D_last = xmul(D0, ctl->kappa_min);
-            trig = refresh_trigger(d2, D, D_last, ctl->theta);
+            if (refresh) {
+                double d2 = 0.0;
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    const double dd = xsub(x[u][d], xl[u][d]);
+                    d2 = xadd(d2, xmul(dd, dd));
+                }
+                trig = trig || refresh_trigger(d2, xmul(D0[u], rk), xmul(D0[u], kmin), theta);
+            }
         }
     }
     // one flag write per block (a million same-address stores would serialise in L2)
-    if (__syncthreads_or(trig) && threadIdx.x == 0) ctl->rebuild_flag = 1u;
+    if (__syncthreads_or(trig) && threadIdx.x == 0) a.ctl->rebuild_flag = 1u;
 }
 
 // ===========================================================================
@@ -165,7 +206,7 @@ __global__ void __launch_bounds__(256) k_adam_refresh(DevArrays a, int do_adam, 
 // ===========================================================================
 __global__ void k_build_prepare(DevArrays a) {
     DevCtl* ctl = a.ctl;
-    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    if (build_off(ctl)) return;
     const std::uint32_t n = a.C_alloc + 1;
     for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
         a.cell_count[k] = 0u;
@@ -199,7 +240,8 @@ __global__ void k_build_prepare(DevArrays a) {
         // every rebuild re-anchors every particle (x_last is written by k_bin)
         ctl->kappa_min = ctl->build_kappa;
         // graph mode: the tiled build also computes this step's forces
-        ctl->forces_done = ctl->fuse_forces;
+        // (only with unsorted rows: a sorted row is summed after its sort)
+        ctl->forces_done = a.sorted_rows ? 0u : ctl->fuse_forces;
         ctl->row_need = 0u;
         ctl->nbuilds += 1u;
     }
@@ -208,7 +250,7 @@ __global__ void k_build_prepare(DevArrays a) {
 template <int ND>
 __global__ void __launch_bounds__(256) k_build_bin(DevArrays a) {
     const DevCtl* ctl = a.ctl;
-    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    if (build_off(ctl)) return;
     const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
     if (i >= a.N) return;
     double x[ND], D0;
@@ -261,7 +303,7 @@ __device__ __forceinline__ std::uint32_t block_exclusive_scan(std::uint32_t v, s
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_tiles(const std::uint32_t* in, std::uint32_t* out, std::uint32_t n,
                  std::uint32_t* block_sums, const DevCtl* gate) {
-    if (gate && (ctl_idle(gate) || !gate->rebuild_flag)) return;
+    if (gate && build_off(gate)) return;
     __shared__ std::uint32_t smem[32];
     const std::uint64_t base = static_cast<std::uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
     std::uint32_t v[kScanItems];
@@ -284,7 +326,7 @@ __global__ void __launch_bounds__(kScanThreads)
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_add(std::uint32_t* out, std::uint32_t n, const std::uint32_t* block_offsets,
                const DevCtl* gate) {
-    if (gate && (ctl_idle(gate) || !gate->rebuild_flag)) return;
+    if (gate && build_off(gate)) return;
     const std::uint32_t add = block_offsets[blockIdx.x];
     const std::uint64_t base = static_cast<std::uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
 #pragma unroll
@@ -308,7 +350,7 @@ void scan_exclusive(const std::uint32_t* in, std::uint32_t* out, std::uint32_t n
 
 __global__ void __launch_bounds__(256) k_build_scatter(DevArrays a) {
     const DevCtl* ctl = a.ctl;
-    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    if (build_off(ctl)) return;
     const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
     if (i >= a.N) return;
     a.cell_list[a.cell_start[a.cell_of[i]] + a.cell_rank[i]] = static_cast<std::uint32_t>(i);
@@ -321,7 +363,7 @@ __global__ void __launch_bounds__(256) k_build_scatter(DevArrays a) {
 template <int ND>
 __global__ void __launch_bounds__(256) k_build_cell_sort(DevArrays a) {
     const DevCtl* ctl = a.ctl;
-    if (ctl_idle(ctl) || !ctl->rebuild_flag) return;
+    if (build_off(ctl)) return;
     const std::uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ctl->ncells) return;
     const std::uint32_t q0 = a.cell_start[c], q1 = a.cell_start[c + 1];
@@ -355,7 +397,7 @@ __device__ __forceinline__ bool tiled_build_ok(const DevCtl* ctl);
 template <int ND>
 __global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
     DevCtl* ctl = a.ctl;
-    if (ctl_idle(ctl) || !ctl->rebuild_flag || tiled_build_ok<ND>(ctl)) return;
+    if (build_off(ctl) | tiled_build_ok<ND>(ctl)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->forces_done = 0u;
     __shared__ std::uint32_t buf[kSearchSmemRow * kSearchBlock];
     __shared__ std::uint32_t block_need;
@@ -485,21 +527,24 @@ template <> struct TileShape<3> {
 constexpr int kTileThreads = 256;
 constexpr int kTileRow = 32;
 
-// dynamic shared memory of k_build_search_tiled<ND>
-template <int ND>
+// dynamic shared memory of k_build_search_tiled<ND, SORT>: the staged rows
+// (SORT only) follow the staged particles
+template <int ND, bool SORT>
 constexpr std::size_t tile_smem_bytes() {
     using TS = TileShape<ND <= 3 ? ND : 3>;
     return static_cast<std::size_t>(TS::stage) * pos_stride(ND) * 8 + 2ull * TS::stage * 4 +
            (TS::halo_cells + 2) * 4 + 2ull * TS::stage * 2 +
-           static_cast<std::size_t>(kTileRow) * kTileThreads * 2;
+           (SORT ? static_cast<std::size_t>(kTileRow) * kTileThreads * 2 : 0);
 }
 
 template <int ND>
 __device__ __forceinline__ bool tiled_build_ok(const DevCtl* ctl) {
     if (ND > 3) return false;
-    for (int d = 0; d < ND; ++d)
-        if (ctl->ncell[d] < TileShape<(ND <= 3 ? ND : 3)>::t(d) + 2) return false;
-    return true;
+    bool ok = true;
+    RCPG_UNROLL
+    for (int d = 0; d < (ND <= 3 ? ND : 3); ++d)
+        ok = ok & (ctl->ncell[d] >= TileShape<(ND <= 3 ? ND : 3)>::t(d) + 2);
+    return ok;
 }
 
 // Sorts a row gathered partly in shared memory (column `mine`, stride kTileThreads)
@@ -542,7 +587,7 @@ __device__ __forceinline__ void finish_row(std::uint32_t* mine, int stride, int 
     }
 }
 
-template <int ND>
+template <int ND, bool SORT>
 __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArrays a) {
     constexpr int NDT = ND <= 3 ? ND : 3;
     using TS = TileShape<NDT>;
@@ -551,7 +596,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     constexpr int HC = TS::halo_cells;
     DevCtl* ctl = a.ctl;
     if (ND > 3) return;
-    if (ctl_idle(ctl) || !ctl->rebuild_flag || !tiled_build_ok<ND>(ctl)) return;
+    if (build_off(ctl) | !tiled_build_ok<ND>(ctl)) return;
     extern __shared__ __align__(16) unsigned char tile_smem[];
     double* s_pos = reinterpret_cast<double*>(tile_smem);
     std::uint32_t* s_id = reinterpret_cast<std::uint32_t*>(s_pos + STAGE * P);
@@ -559,15 +604,32 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     std::uint32_t* s_cstart = s_slot + STAGE;
     std::uint16_t* s_inner = reinterpret_cast<std::uint16_t*>(s_cstart + HC + 2);
     std::uint16_t* s_cell = s_inner + STAGE;
-    std::uint16_t* s_rows = s_cell + STAGE;  // [kTileRow][kTileThreads] staged indices
+    std::uint16_t* s_rows = s_cell + STAGE;  // [kTileRow][kTileThreads] staged indices (SORT)
     __shared__ std::uint32_t s_warp[kTileThreads / 32];
     __shared__ std::uint32_t s_need, s_ninner;
     __shared__ ForceSums s_red[kTileThreads / 32];
     const std::uint64_t N = a.N;
     const std::uint32_t S = a.S;
-    const Geometry g = ctl->g;  // register copy: the loops below store through other pointers
+    // box of the minimum image in shared memory (the loops store through other
+    // pointers, so loads through ctl would be repeated); walls read from ctl
+    __shared__ double bx[ND], ibx[ND];
+    // per-thread sums that change once per particle (fused forces)
+    __shared__ double s_mag[kTileThreads], s_Dsum[kTileThreads];
+    __shared__ std::uint32_t s_magc[kTileThreads];
+    if (threadIdx.x < ND) {
+        bx[threadIdx.x] = ctl->g.box[threadIdx.x];
+        ibx[threadIdx.x] = ctl->g.inv_box[threadIdx.x];
+    }
+    s_mag[threadIdx.x] = 0.0;
+    s_Dsum[threadIdx.x] = 0.0;
+    s_magc[threadIdx.x] = 0u;
+    const Geometry& g = ctl->g;
     const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
-    const bool fuse = ctl->forces_done != 0u;
+    const bool fuse = !SORT && ctl->forces_done != 0u;
+    const bool mixed = ctl->pair_fp32 != 0u;
+    const float kapf = static_cast<float>(kap), tf = static_cast<float>(t_shell);
+    __shared__ float hbf[ND];  // half box, FP32 (mixed minimum image)
+    if (threadIdx.x < ND) hbf[threadIdx.x] = static_cast<float>(0.5 * ctl->g.box[threadIdx.x]);
     int nc[ND], nt[ND];
     std::uint32_t tiles = 1;
     RCPG_UNROLL
@@ -579,8 +641,10 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     if (threadIdx.x == 0) s_need = 0u;
     if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) ctl->nsum_blocks = gridDim.x;
     std::uint16_t* mine = s_rows + threadIdx.x;
-    ForceSums fs;
-    sums_zero(fs);
+    // graph-mode sums of the fused forces; the wall terms join the pair
+    // chains (the reduction adds pair and wall terms anyway)
+    double fU = 0.0, fLc = 0.0, fdk = 0.0, fFm = 0.0, fmaxov = 0.0;
+    std::uint32_t fcount = 0;
     for (std::uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         int t0[ND], hw[ND];
         std::uint32_t rem = tile;
@@ -692,7 +756,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                             if (j == i) continue;
                             double xj[ND], D0j;
                             load_pos<ND>(a.spos, pp, xj, D0j);
-                            if (!in_shell<ND>(xi, xj, Di, xmul(D0j, kap), g.box, g.inv_box, t_shell)) continue;
+                            if (!in_shell<ND>(xi, xj, Di, xmul(D0j, kap), bx, ibx, t_shell)) continue;
                             if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
                             ++n;
                             if (j > i) ++n_half;
@@ -727,35 +791,84 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
             load_pos<ND>(s_pos, k, xi, D0i);
             const double Di = xmul(D0i, kap);
             std::uint32_t n = 0, n_half = 0;
-            int odo[ND];
-            RCPG_UNROLL
-            for (int d = 0; d < ND; ++d) odo[d] = 0;
-            constexpr int NCOMBO = (ND == 2) ? 9 : 27;
-            for (int combo = 0; combo < NCOMBO; ++combo) {
-                int hc = 0, mul = 1;
+            double fi[ND];
+            // the cells x-1, x, x+1 of one halo row are consecutive halo cells,
+            // so their staged particles form one contiguous range: 3^(ndim-1)
+            // ranges, visited in the order of the 3^ndim cells (axis 0 fastest)
+            constexpr int NROW = (ND == 2) ? 3 : 9;
+            const int hbase = hl[0] - 1 + (ND == 2 ? (hl[1] - 1) * hw[0]
+                                                   : (hl[1] - 1) * hw[0] + (hl[ND - 1] - 1) * hw[0] * hw[1]);
+            // candidate loop; MX: mixed precision (graph mode, unsorted rows only)
+            auto scan = [&](auto mixed_tag) {
+                constexpr bool MX = decltype(mixed_tag)::value;
+                float fif[ND];
                 RCPG_UNROLL
                 for (int d = 0; d < ND; ++d) {
-                    hc += (hl[d] - 1 + odo[d]) * mul;
-                    mul *= hw[d];
+                    fi[d] = 0.0;
+                    fif[d] = 0.0f;
                 }
-                RCPG_UNROLL
-                for (int d = 0; d < ND; ++d) {
-                    if (++odo[d] < 3) break;
-                    odo[d] = 0;
+                const float Dif = static_cast<float>(D0i) * kapf;
+                for (int rr = 0; rr < NROW; ++rr) {
+                    const int hc = hbase + (rr % 3) * hw[0] + (ND == 2 ? 0 : (rr / 3) * hw[0] * hw[1]);
+                    const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 3];
+                    for (std::uint32_t pp = p0; pp < p1; ++pp) {
+                        if (pp == k) continue;
+                        double xj[ND], D0j;
+                        load_pos<ND>(s_pos, pp, xj, D0j);
+                        bool overlap;
+                        double dx[ND], d2, Dj;
+                        float dxf[ND], d2f, rsum;
+                        if constexpr (MX) {
+                            // FP32 shell test on the FP64 difference, widened by
+                            // kShellMarginF so that the row holds every pair of the
+                            // FP64 shell (the list only has to contain the overlaps)
+                            d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
+                            rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
+                            const float rc = rsum + tf;
+                            if (!(d2f < rc * rc * kShellMarginF)) continue;
+                            overlap = d2f < rsum * rsum;
+                        } else {
+                            Dj = xmul(D0j, kap);
+                            d2 = pair_disp<ND>(xi, xj, bx, ibx, dx);
+                            const double r_c = shell_cut<ND>(Di, Dj, t_shell);  // ndim <= 3: symmetric
+                            if (!(d2 < xmul(r_c, r_c))) continue;
+                            overlap = false;
+                            if constexpr (!SORT) {
+                                const double r_ij = xmul(0.5, xadd(Di, Dj));
+                                overlap = d2 < xmul(r_ij, r_ij);
+                            }
+                        }
+                        const std::uint32_t j = s_id[pp];
+                        if constexpr (SORT) {
+                            if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = static_cast<std::uint16_t>(pp);
+                            else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
+                        } else {
+                            if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
+                            if (fuse && overlap) {
+                                PairTerms pt;
+                                if constexpr (MX) pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
+                                else pair_terms_f64<ND>(dx, d2, xmul(0.5, xadd(Di, Dj)), fi, pt);
+                                if (j > i) {
+                                    fU = xadd(fU, pt.U);
+                                    fLc = xadd(fLc, pt.Lc);
+                                    fdk = xadd(fdk, pt.dk);
+                                    fFm = xadd(fFm, pt.Fm);
+                                    fmaxov = fmax(fmaxov, pt.U);
+                                    ++fcount;
+                                }
+                            }
+                        }
+                        ++n;
+                        if (j > i) ++n_half;
+                    }
                 }
-                const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 1];
-                for (std::uint32_t pp = p0; pp < p1; ++pp) {
-                    if (pp == k) continue;
-                    double xj[ND], D0j;
-                    load_pos<ND>(s_pos, pp, xj, D0j);
-                    if (!in_shell<ND>(xi, xj, Di, xmul(D0j, kap), g.box, g.inv_box, t_shell)) continue;
-                    const std::uint32_t j = s_id[pp];
-                    if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = static_cast<std::uint16_t>(pp);
-                    else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
-                    ++n;
-                    if (j > i) ++n_half;
+                if constexpr (MX) {
+                    RCPG_UNROLL
+                    for (int d = 0; d < ND; ++d) fi[d] = static_cast<double>(fif[d]);
                 }
-            }
+            };
+            if (!SORT && mixed) scan(std::true_type{});
+            else scan(std::false_type{});
             const std::uint32_t cap = a.caps[i];
             if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
                 ctl->cap_error_particle = i;
@@ -764,7 +877,22 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
             atomicMax(&s_need, n);
             if (n > S) {
                 a.nbr_cnt[q] = 0;  // overflow: empty row, rebuilt after the capacity grows
-                ctl->forces_done = 0u;
+                if (fuse) ctl->forces_done = 0u;
+                continue;
+            }
+            if constexpr (!SORT) {
+                a.nbr_cnt[q] = n;
+                if (fuse) {
+                    wall_forces<ND>(xi, Di, g, fi, fU, fdk, fFm, fcount);
+                    const double f2 = force_norm2<ND>(fi);
+                    if (f2 > 1.0E-16) {
+                        s_mag[threadIdx.x] = xadd(s_mag[threadIdx.x], xsqrt(f2));
+                        ++s_magc[threadIdx.x];
+                    }
+                    s_Dsum[threadIdx.x] = xadd(s_Dsum[threadIdx.x], Di);
+                    RCPG_UNROLL
+                    for (int d = 0; d < ND; ++d) a.F[static_cast<std::uint64_t>(i) * ND + d] = fi[d];
+                }
             } else if (n <= static_cast<std::uint32_t>(kTileRow)) {
                 // sort the staged indices by particle id, write the row
                 for (std::uint32_t e = 1; e < n; ++e) {
@@ -780,48 +908,29 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                 a.nbr_cnt[q] = n;
                 for (std::uint32_t e = 0; e < n; ++e)
                     a.nbr[static_cast<std::uint64_t>(e) * N + q] = s_id[mine[e * kTileThreads]];
-                if (fuse) {
-                    double fi[ND];
-                    RCPG_UNROLL
-                    for (int d = 0; d < ND; ++d) fi[d] = 0.0;
-                    for (std::uint32_t e = 0; e < n; ++e) {
-                        const std::uint32_t pp = mine[e * kTileThreads];
-                        double xj[ND], D0j;
-                        load_pos<ND>(s_pos, pp, xj, D0j);
-                        PairTerms pt;
-                        if (!pair_force<ND>(xi, Di, xj, xmul(D0j, kap), g, fi, pt)) continue;
-                        if (s_id[pp] > i) {
-                            fs.pair_U = xadd(fs.pair_U, pt.U);
-                            fs.pair_Lc = xadd(fs.pair_Lc, pt.Lc);
-                            fs.pair_dk = xadd(fs.pair_dk, pt.dk);
-                            fs.pair_Fm = xadd(fs.pair_Fm, pt.Fm);
-                            fs.pair_maxov = fmax(fs.pair_maxov, pt.U);
-                            fs.pair_count += 1ull;
-                        }
-                    }
-                    wall_forces<ND>(xi, Di, g, fi, fs.wall_U, fs.wall_dk, fs.wall_Fm, fs.wall_count);
-                    const double f2 = force_norm2<ND>(fi);
-                    if (f2 > 1.0E-16) {
-                        fs.sum_mag = xadd(fs.sum_mag, xsqrt(f2));
-                        fs.mag_count += 1ull;
-                    }
-                    fs.sum_D = xadd(fs.sum_D, Di);
-                    RCPG_UNROLL
-                    for (int d = 0; d < ND; ++d) a.F[static_cast<std::uint64_t>(i) * ND + d] = fi[d];
-                }
             } else {
                 // long row (kTileRow < n <= S): the first kTileRow entries go to
-                // the global row too, sorted there; its forces come from the separate pass
+                // the global row too, sorted there
                 for (std::uint32_t e = 0; e < static_cast<std::uint32_t>(kTileRow); ++e)
                     a.nbr[static_cast<std::uint64_t>(e) * N + q] = s_id[mine[e * kTileThreads]];
                 finish_row(nullptr, 0, 0, n, S, a.nbr, a.nbr_cnt, N, q);
-                ctl->forces_done = 0u;
             }
         }
     }
     __syncthreads();
     if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
     if (fuse) {
+        ForceSums fs;
+        sums_zero(fs);
+        fs.pair_U = fU;
+        fs.pair_Lc = fLc;
+        fs.pair_dk = fdk;
+        fs.pair_Fm = fFm;
+        fs.pair_maxov = fmaxov;
+        fs.sum_mag = s_mag[threadIdx.x];
+        fs.sum_D = s_Dsum[threadIdx.x];
+        fs.pair_count = fcount;
+        fs.mag_count = s_magc[threadIdx.x];
         block_reduce_sums<kTileThreads>(fs, s_red);
         if (threadIdx.x == 0) a.block_sums[blockIdx.x] = fs;
     }
@@ -830,77 +939,163 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
 // ===========================================================================
 // C. forces + walls + per-block sums
 // ===========================================================================
-template <int ND>
-__global__ void __launch_bounds__(kForceBlock) k_forces(DevArrays a, int exact_terms) {
+// EXACT: the pair terms of every counted pair are also stored (pterm) for the
+// one-thread-order reduction; the block sums are not used then. Otherwise the
+// block sums are the step's reduction input and the wall terms join the pair
+// chains (the reduction adds pair and wall terms anyway). MIXED: FP32 pair
+// terms; the graph launches both variants and the one that does not match the
+// step's precision returns at once.
+template <int ND, bool EXACT, bool MIXED>
+__global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ? 3 : 2)) k_forces(DevArrays a) {
     const DevCtl* ctl = a.ctl;
     __shared__ ForceSums red[kForceBlock / 32];
-    if (ctl_idle(ctl) || ctl->forces_done) return;
+    {
+        // one round trip for every flag of the early exit
+        const std::uint32_t st = ctl->stopped, ha = ctl->halted, fd = ctl->forces_done, p32 = ctl->pair_fp32;
+        if ((st | ha | fd) != 0u || MIXED != (!EXACT && p32 != 0u)) return;
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->nsum_blocks = gridDim.x;
-    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
     const std::uint64_t N = a.N;
-    ForceSums s;
-    sums_zero(s);
-    if (i < N) {
-        const std::uint64_t t = i;  // row slot
+    const Geometry& g = ctl->g;
+    double bx[ND];
+    RCPG_UNROLL
+    for (int d = 0; d < ND; ++d) bx[d] = g.box[d];
+    const double kap = ctl->force_kappa;
+    // the block's running sums live in shared memory, one column per thread
+    // (they change once per particle); a particle's pair terms are summed in
+    // registers first
+    __shared__ double acc[7][kForceBlock];
+    __shared__ std::uint32_t accn[2][kForceBlock];
+    RCPG_UNROLL
+    for (int f = 0; f < 7; ++f) acc[f][threadIdx.x] = 0.0;
+    accn[0][threadIdx.x] = accn[1][threadIdx.x] = 0u;
+    // persistent grid: row slots t = blockIdx*256 + tid, then strides of the grid
+    for (std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x; t < N;
+         t += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
         const std::uint64_t i = a.work ? a.work[t] : t;
-        const Geometry g = ctl->g;  // register copy: the loops below store through other pointers
-        const double kap = ctl->force_kappa;
         double xi[ND], D0i;
         load_pos<ND>(a.pos, i, xi, D0i);
         const double Di = xmul(D0i, kap);
         double fi[ND];
-#pragma unroll
-        for (int d = 0; d < ND; ++d) fi[d] = 0.0;
         const std::uint32_t n = min(a.nbr_cnt[t], a.S);
-        std::uint32_t nterm = 0;
+        std::uint32_t nterm = 0, scount = 0;
+        using Acc = std::conditional_t<MIXED, float, double>;
+        Acc sU = 0, sLc = 0, sdk = 0, sFm = 0, smax = 0;
         // Partners in chunks of kChunk: the row ids and then the partner
         // positions of a chunk are loaded before any of its arithmetic, so a
         // thread keeps kChunk gathers in flight; the pairs are still summed in
-        // row (ascending partner) order.
-        constexpr std::uint32_t kChunk = 4;
-        for (std::uint32_t k0 = 0; k0 < n; k0 += kChunk) {
-            std::uint32_t jj[kChunk];
-            double xj[kChunk][ND], D0j[kChunk];
+        // row order.
+        auto rows = [&](auto mixed_tag) {
+            constexpr bool MX = decltype(mixed_tag)::value;
+            constexpr std::uint32_t kChunk = 4;
+            float fif[ND], hbf[ND];
+            double ibx[ND];
             RCPG_UNROLL
-            for (std::uint32_t u = 0; u < kChunk; ++u)
-                jj[u] = (k0 + u < n) ? __ldg(a.nbr + static_cast<std::uint64_t>(k0 + u) * N + t) : 0u;
-            RCPG_UNROLL
-            for (std::uint32_t u = 0; u < kChunk; ++u)
-                if (k0 + u < n && jj[u] < N) load_pos<ND>(a.pos, jj[u], xj[u], D0j[u]);
-            RCPG_UNROLL
-            for (std::uint32_t u = 0; u < kChunk; ++u) {
-                if (k0 + u >= n) break;
-                const std::uint32_t j = jj[u];
-                if (j >= N) continue;
-                PairTerms pt;
-                if (!pair_force<ND>(xi, Di, xj[u], xmul(D0j[u], kap), g, fi, pt)) continue;
-                if (j > i) {
-                    s.pair_U = xadd(s.pair_U, pt.U);
-                    s.pair_Lc = xadd(s.pair_Lc, pt.Lc);
-                    s.pair_dk = xadd(s.pair_dk, pt.dk);
-                    s.pair_Fm = xadd(s.pair_Fm, pt.Fm);
-                    s.pair_maxov = fmax(s.pair_maxov, pt.U);
-                    s.pair_count += 1ull;
-                    if (exact_terms) {
-                        a.pterm[static_cast<std::uint64_t>(nterm) * N + i] = pt;
-                        ++nterm;
+            for (int d = 0; d < ND; ++d) {
+                fi[d] = 0.0;
+                fif[d] = 0.0f;
+                hbf[d] = static_cast<float>(0.5 * bx[d]);
+                if constexpr (!MX) ibx[d] = g.inv_box[d];
+            }
+            const float kapf = static_cast<float>(kap);
+            const float Dif = static_cast<float>(D0i) * kapf;
+            for (std::uint32_t k0 = 0; k0 < n; k0 += kChunk) {
+                std::uint32_t jj[kChunk];
+                double xj[kChunk][ND], D0j[kChunk];
+                RCPG_UNROLL
+                for (std::uint32_t u = 0; u < kChunk; ++u)
+                    jj[u] = (k0 + u < n) ? __ldg(a.nbr + static_cast<std::uint64_t>(k0 + u) * N + t) : 0u;
+                RCPG_UNROLL
+                for (std::uint32_t u = 0; u < kChunk; ++u)
+                    if (k0 + u < n && jj[u] < N) load_pos<ND>(a.pos, jj[u], xj[u], D0j[u]);
+                RCPG_UNROLL
+                for (std::uint32_t u = 0; u < kChunk; ++u) {
+                    if (k0 + u >= n) break;
+                    const std::uint32_t j = jj[u];
+                    if (j >= N) continue;
+                    PairTerms pt;
+                    if constexpr (MX) {
+                        float dxf[ND];
+                        const float d2f = mixed_disp<ND>(xi, xj[u], bx, hbf, dxf);
+                        const float rsum = 0.5f * (Dif + static_cast<float>(D0j[u]) * kapf);
+                        if (!(d2f < rsum * rsum)) continue;
+                        pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
+                    } else {
+                        const double r_ij = xmul(0.5, xadd(Di, xmul(D0j[u], kap)));
+                        double dx[ND];
+                        const double d2 = pair_disp<ND>(xi, xj[u], bx, ibx, dx);
+                        if (!(d2 < xmul(r_ij, r_ij))) continue;
+                        pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
+                    }
+                    if (j > i) {
+                        if constexpr (EXACT) {
+                            a.pterm[static_cast<std::uint64_t>(nterm) * N + i] = pt;
+                            ++nterm;
+                        } else if constexpr (MX) {
+                            sU += static_cast<float>(pt.U);
+                            sLc += static_cast<float>(pt.Lc);
+                            sdk += static_cast<float>(pt.dk);
+                            sFm += static_cast<float>(pt.Fm);
+                            smax = fmaxf(smax, static_cast<float>(pt.U));
+                            ++scount;
+                        } else {
+                            sU = xadd(sU, pt.U);
+                            sLc = xadd(sLc, pt.Lc);
+                            sdk = xadd(sdk, pt.dk);
+                            sFm = xadd(sFm, pt.Fm);
+                            smax = fmax(smax, pt.U);
+                            ++scount;
+                        }
                     }
                 }
             }
+            if constexpr (MX) {
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) fi[d] = static_cast<double>(fif[d]);
+            }
+        };
+        rows(std::integral_constant<bool, MIXED>{});
+        if constexpr (EXACT) {
+            a.pterm_cnt[i] = nterm;
+            double wU = 0.0, wdk = 0.0, wFm = 0.0;  // recomputed in order by k_reduce_exact
+            std::uint32_t wc = 0;
+            wall_forces<ND>(xi, Di, g, fi, wU, wdk, wFm, wc);
+        } else {
+            const int c = threadIdx.x;
+            acc[0][c] = xadd(acc[0][c], static_cast<double>(sU));
+            acc[1][c] = xadd(acc[1][c], static_cast<double>(sLc));
+            acc[2][c] = xadd(acc[2][c], static_cast<double>(sdk));
+            acc[3][c] = xadd(acc[3][c], static_cast<double>(sFm));
+            acc[4][c] = fmax(acc[4][c], static_cast<double>(smax));
+            std::uint32_t wc = 0;
+            wall_forces<ND>(xi, Di, g, fi, acc[0][c], acc[2][c], acc[3][c], wc);
+            accn[0][c] += scount + wc;
+            const double f2 = force_norm2<ND>(fi);
+            if (f2 > 1.0E-16) {
+                acc[5][c] = xadd(acc[5][c], xsqrt(f2));
+                ++accn[1][c];
+            }
+            acc[6][c] = xadd(acc[6][c], Di);
         }
-        if (exact_terms) a.pterm_cnt[i] = nterm;
-        wall_forces<ND>(xi, Di, g, fi, s.wall_U, s.wall_dk, s.wall_Fm, s.wall_count);
-        const double f2 = force_norm2<ND>(fi);
-        if (f2 > 1.0E-16) {
-            s.sum_mag = xsqrt(f2);
-            s.mag_count = 1ull;
-        }
-        s.sum_D = Di;
 #pragma unroll
         for (int d = 0; d < ND; ++d) a.F[i * ND + d] = fi[d];
     }
-    block_reduce_sums<kForceBlock>(s, red);
-    if (threadIdx.x == 0) a.block_sums[blockIdx.x] = s;
+    if constexpr (!EXACT) {
+        ForceSums s;
+        sums_zero(s);
+        const int c = threadIdx.x;
+        s.pair_U = acc[0][c];
+        s.pair_Lc = acc[1][c];
+        s.pair_dk = acc[2][c];
+        s.pair_Fm = acc[3][c];
+        s.pair_maxov = acc[4][c];
+        s.sum_mag = acc[5][c];
+        s.sum_D = acc[6][c];
+        s.pair_count = accn[0][c];
+        s.mag_count = accn[1][c];
+        block_reduce_sums<kForceBlock>(s, red);
+        if (threadIdx.x == 0) a.block_sums[blockIdx.x] = s;
+    }
 }
 
 // ===========================================================================
@@ -1038,6 +1233,12 @@ __global__ void __launch_bounds__(kCtlThreads) k_controller(DevArrays a, int ope
                 const StepScalars sc = finalize_sums(s, ctl->force_mu, a.ndim);
                 ctl->scal = sc;
                 end_step(c, a.hist, sc);
+                // mixed precision: FP64 pair terms from the first step whose
+                // (nonzero) max overlap is below the switch, for the rest of the run
+                if (ctl->pair_fp32 && sc.max_overlap > 0.0 && sc.max_overlap < ctl->mixed_switch) {
+                    ctl->pair_fp32 = 0u;
+                    ctl->fp64_switch_step = c.steps;
+                }
                 ctl->graph_steps += 1ull;
                 for (int d = 0; d < a.ndim; ++d) ctl->adam_box[d] = c.box[d];
                 ctl->adam_alpha = c.adam_alpha;
@@ -1331,6 +1532,56 @@ void reorder_impl(const DevArrays& a, cudaStream_t st) {
     k_reorder_commit<ND><<<nb, kForceBlock, 0, st>>>(a);
 }
 
+// Blocks of `Kernel` that are resident on the whole GPU at once (SMs x
+// occupancy), cached per device: the grid of the persistent kernels.
+template <auto Kernel>
+unsigned resident_grid(int threads, std::size_t smem = 0) {
+    static int grid[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148u;
+    if (grid[dev] == 0) {
+        int sms = 148, per_sm = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, Kernel, threads, smem);
+        grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    return static_cast<unsigned>(grid[dev]);
+}
+
+template <int ND>
+void adam_nd(const DevArrays& a, int do_adam, int do_refresh, cudaStream_t st) {
+    const unsigned need = (force_blocks(a.N) + 1) / 2, g = resident_grid<k_adam_refresh<ND>>(kForceBlock);
+    k_adam_refresh<ND><<<need < g ? need : g, kForceBlock, 0, st>>>(a, do_adam, do_refresh);
+}
+
+// persistent force grid: at most the blocks resident at once (the block-sum
+// buffers hold at least force_blocks(N) entries)
+template <int ND, bool EXACT, bool MIXED>
+void forces_nd(const DevArrays& a, cudaStream_t st) {
+    const unsigned need = force_blocks(a.N), g = resident_grid<k_forces<ND, EXACT, MIXED>>(kForceBlock);
+    k_forces<ND, EXACT, MIXED><<<need < g ? need : g, kForceBlock, 0, st>>>(a);
+}
+
+// persistent grid of the tiled build: as many blocks as fit on the GPU at once
+template <int ND, bool SORT>
+void launch_tiled(const DevArrays& a, cudaStream_t st) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    constexpr std::size_t smem = tile_smem_bytes<ND, SORT>();
+    static int grid[64] = {};
+    if (dev >= 0 && dev < 64 && grid[dev] == 0) {
+        cudaFuncSetAttribute(k_build_search_tiled<ND, SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+        int sms = 148, per_sm = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_search_tiled<ND, SORT>, kTileThreads, smem);
+        grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    const int blocks = (dev >= 0 && dev < 64) ? grid[dev] : 148;
+    k_build_search_tiled<ND, SORT><<<static_cast<unsigned>(blocks), kTileThreads, smem, st>>>(a);
+}
+
 template <int ND>
 void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     const unsigned nb = force_blocks(a.N);
@@ -1342,21 +1593,8 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     k_build_cell_sort<ND><<<(a.C_alloc + 255) / 256, 256, 0, st>>>(a);
     const unsigned sb = static_cast<unsigned>((a.N + kSearchBlock - 1) / kSearchBlock);
     if (ND <= 3) {
-        // persistent grid: as many blocks as fit on the GPU at once
-        int dev = 0;
-        cudaGetDevice(&dev);
-        constexpr std::size_t smem = tile_smem_bytes<ND>();
-        static int grid[64][2] = {};
-        if (dev >= 0 && dev < 64 && grid[dev][ND - 2] == 0) {
-            cudaFuncSetAttribute(k_build_search_tiled<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem));
-            int sms = 148, per_sm = 1;
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_search_tiled<ND>, kTileThreads, smem);
-            grid[dev][ND - 2] = sms * (per_sm > 0 ? per_sm : 1);
-        }
-        const int blocks = (dev >= 0 && dev < 64) ? grid[dev][ND - 2] : 148;
-        k_build_search_tiled<ND><<<static_cast<unsigned>(blocks), kTileThreads, smem, st>>>(a);
+        if (a.sorted_rows) launch_tiled<ND, true>(a, st);
+        else launch_tiled<ND, false>(a, st);
     }
     k_build_search<ND><<<sb, kSearchBlock, 0, st>>>(a);
 }
@@ -1376,8 +1614,7 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     }
 
 void launch_adam_refresh(const DevArrays& a, int do_adam, int do_refresh, cudaStream_t st) {
-    const unsigned nb = force_blocks(a.N);
-    RCPG_DISPATCH_ND(a.ndim, (k_adam_refresh<ND><<<nb, kForceBlock, 0, st>>>(a, do_adam, do_refresh)));
+    RCPG_DISPATCH_ND(a.ndim, (adam_nd<ND>(a, do_adam, do_refresh, st)));
 }
 
 void launch_rebuild(const DevArrays& a, cudaStream_t st) {
@@ -1385,8 +1622,12 @@ void launch_rebuild(const DevArrays& a, cudaStream_t st) {
 }
 
 void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st) {
-    const unsigned nb = force_blocks(a.N);
-    RCPG_DISPATCH_ND(a.ndim, (k_forces<ND><<<nb, kForceBlock, 0, st>>>(a, exact_terms)));
+    if (exact_terms) {
+        RCPG_DISPATCH_ND(a.ndim, (forces_nd<ND, true, false>(a, st)));
+    } else {
+        RCPG_DISPATCH_ND(a.ndim, (forces_nd<ND, false, false>(a, st)));
+        if (a.mixed) RCPG_DISPATCH_ND(a.ndim, (forces_nd<ND, false, true>(a, st)));
+    }
 }
 
 void launch_reduce_exact(const DevArrays& a, cudaStream_t st) {

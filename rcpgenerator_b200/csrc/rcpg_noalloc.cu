@@ -137,6 +137,7 @@ extern "C" int32_t rcpg_pairs_full_noalloc(uint64_t N, int32_t ndim, const doubl
     a.nbr = cv.take<std::uint32_t>(static_cast<std::size_t>(row_capacity) * N);
     a.scan_tmp = cv.take<std::uint32_t>(2 * 4096 + 16);
     a.S = row_capacity;
+    a.sorted_rows = 1;  // the reference's row order
     a.work = a.cell_list;
     if (!cv.ok) {
         set_err(err, errlen,

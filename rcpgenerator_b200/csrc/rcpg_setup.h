@@ -36,6 +36,10 @@ struct EngineInput {
     bool exact = false;          // host-controlled steps, one-thread reduction order
     int device = 0;
     int graph_steps = 32;        // steps per captured graph (graph mode)
+    // pair arithmetic (graph mode): 0 = FP64 throughout; 1 = mixed, FP32 pair
+    // terms until the first step whose max overlap falls below mixed_switch
+    int pair_precision = 0;
+    double mixed_switch = 1e-5;
 };
 
 struct RunSetup {
