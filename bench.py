@@ -146,6 +146,123 @@ def reference_sample(pos, dia, box, walls, steps: int, threads: int):
             if stamps else None, "wall_s": t1 - t0}, None
 
 
+# ---- batched workload: many independent small packings (packings/hour) ----
+BATCH_METRIC = "packings/hour"
+
+
+def batch_instances(count: int, seed0: int = 0):
+    """Independent packings drawn like the batched workload: N log-uniform on
+    [64, 16384], ndim from {2, 3, 4}, diameters mono (d=1), bidisperse 50:50
+    with ratio uniform on [1.1, 3.0], or log-normal with std/mean uniform on
+    [0.1, 0.6] truncated to [0.2, 5] x mean; periodic unit boxes at phi 0.10;
+    seeds seed0.. . Positions and diameters from the engine's initializer."""
+    import rcpgenerator_b200 as rb
+    out = []
+    for k in range(count):
+        seed = seed0 + k
+        rng = np.random.default_rng(seed)
+        n = int(round(np.exp(rng.uniform(np.log(64), np.log(16384)))))
+        nd = int(rng.choice([2, 3, 4]))
+        kind = int(rng.integers(3))
+        if kind == 0:
+            dist = {"type": "mono", "d": 1.0}
+        elif kind == 1:
+            dist = {"type": "bidisperse", "d1": 1.0, "d2": float(rng.uniform(1.1, 3.0)), "p": 0.5}
+        else:
+            cv = rng.uniform(0.1, 0.6)
+            s2 = np.log1p(cv * cv)
+            d = rng.lognormal(-0.5 * s2, np.sqrt(s2), size=4 * n)
+            d = d[(d >= 0.2) & (d <= 5.0)][:n]
+            dist = {"type": "custom", "custom": d.tolist()}
+        init = rb.initialize_particles({"phi": 0.10, "N": n, "Ndim": nd, "box": [1.0] * nd,
+                                        "walls": [0] * nd, "dist": dist, "seed": seed})
+        out.append(({"positions": np.asarray(init["positions"]), "diameters": np.asarray(init["diameters"])},
+                    {"box": init["box"], "walls": init["walls"], "neighbor_max": 0, "seed": seed}))
+    return out
+
+
+def _ref_capped(args_):
+    """One capped reference packing in a worker process (one OpenMP thread)."""
+    pos, dia, box, walls, cap = args_
+    sys.path.insert(0, str(REPO / "oracle" / "_ref"))
+    for k in list(os.environ):
+        if k.startswith("RCP_"):
+            del os.environ[k]
+    import _rcpgenerator as ref
+    ref.set_num_threads(1)
+    t0 = time.perf_counter()
+    r = ref.run_packing_observed({"positions": pos.tolist(), "diameters": dia.tolist()},
+                                 {"box": box, "walls": walls, "neighbor_max": 0, "seed": 0},
+                                 0, False, 0, None, {"max_steps": cap})["result"]
+    return len(pos) * int(r["steps"]), time.perf_counter() - t0
+
+
+def reference_batch_rate(items, cap: int, procs: int):
+    """Reference particle-steps/s per core on capped runs of the same packings,
+    one process per core (the reference's own throughput pattern)."""
+    import multiprocessing as mp
+    if not any((REPO / "oracle" / "_ref").glob("_rcpgenerator*.so")):
+        return None
+    work = [(i["positions"], i["diameters"], c["box"], c["walls"], cap) for i, c in items]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_ref_capped, work)
+    ps = sum(r[0] for r in res)
+    t = sum(r[1] for r in res)
+    return ps / t
+
+
+def run_batch_workload(args) -> int:
+    import rcpgenerator_b200 as rb
+    rank, world, local = dist_env()
+    items = batch_instances(args.batch_count, seed0=rank * args.batch_count)
+    run_opts = {"pair_precision": args.pair_precision, "device": local}
+    for _, c in items:
+        c.update({"pair_precision": args.pair_precision, "device": local})
+    # warm-up: load the kernels and the pools
+    rb.run_packing_batch(items[:2], {"max_steps": 50}, concurrency=2)
+    t0 = time.perf_counter()
+    single = rb.run_packing_batch(items[: args.batch_single], run_opts, concurrency=1)
+    t1 = time.perf_counter()
+    res = rb.run_packing_batch(items, run_opts, concurrency=args.concurrency)
+    t2 = time.perf_counter()
+    ps = sum(len(i["positions"]) * r["steps"] for (i, _), r in zip(items, res))
+    steps = [r["steps"] for r in res]
+    value = len(items) / (t2 - t1) * 3600.0
+    single_value = len(single) / (t1 - t0) * 3600.0
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0:
+        procs = os.cpu_count() or 1
+        sample = items[: min(len(items), procs)]
+        rate = reference_batch_rate(sample, args.cpu_cap_steps, procs)
+        if rate:
+            mean_ps = ps / len(items)  # particle-steps per packing, from the engine's own runs
+            cpu = {"value": procs * 3600.0 * rate / mean_ps, "unit": BATCH_METRIC, "cores": procs,
+                   "kind": "reference",
+                   "sample": f"{len(sample)} of the packings capped at {args.cpu_cap_steps} steps, one "
+                             f"process per core: {rate:.3g} particle-steps/s per core, scaled by the "
+                             f"engine's mean {mean_ps:.3g} particle-steps per packing"}
+    line = {
+        "metric": BATCH_METRIC, "value": value, "unit": BATCH_METRIC, "n_gpus": world,
+        "steps": int(sum(steps)), "warmup": 1, "ms_per_step": (t2 - t1) * 1e3 / max(sum(steps), 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 state, f32 pair terms" if args.pair_precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": f"batch{len(items)}_N64-16384_ndim234_phi0.10", "packings": len(items),
+                   "concurrency": args.concurrency, "engine": "graph",
+                   "pair_precision": args.pair_precision, "particle_steps": ps,
+                   "mean_steps": float(np.mean(steps)), "parallelism": f"replicas{world}",
+                   "timing": "host wall clock around run_packing_batch (inputs on the host, results back)"},
+        "plain_engine": {"value": single_value, "unit": BATCH_METRIC, "packings": len(single),
+                         "note": "the same engine one packing at a time (concurrency 1)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": BATCH_METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "the timed region is already end to end (host arrays in, result dicts out)"},
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -186,10 +303,18 @@ def main() -> int:
                     help="pair arithmetic: mixed = FP32 pair terms while the max overlap >= 1e-5 "
                          "(the workload's stated precision), f64 = FP64 throughout")
     ap.add_argument("--n", type=int, default=WORKLOAD["N"], help="particles (smaller cases for profiling)")
+    ap.add_argument("--workload", default="single", choices=["single", "batch"],
+                    help="single: ADAM steps/s of one N=1M packing; batch: packings/hour of many small ones")
+    ap.add_argument("--batch-count", type=int, default=128)
+    ap.add_argument("--batch-single", type=int, default=8, help="packings timed one at a time")
+    ap.add_argument("--concurrency", type=int, default=32)
+    ap.add_argument("--cpu-cap-steps", type=int, default=300)
     args = ap.parse_args()
     WORKLOAD["N"] = args.n
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "batch":
+        return run_batch_workload(args)
 
     import torch
     import torch.distributed as dist

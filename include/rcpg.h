@@ -153,6 +153,18 @@ int32_t rcpg_run_packing(const rcpg_packing_input* in, const rcpg_run_options* o
                          rcpg_result** out, char* err, size_t errlen);
 void rcpg_result_free(rcpg_result* r);
 
+/* Many independent packings (the reference's throughput pattern: one process
+ * per core, rcptools/jobs.py:392-401, each calling run_packing). `concurrency`
+ * host threads each drive one engine at a time on their own CUDA stream of
+ * device opt->device, taking the next packing as theirs finishes, so the
+ * small packings' kernels and graph replays overlap on the GPU. results[k]
+ * receives packing k's result (free each with rcpg_result_free) or NULL, and
+ * status[k] its RCPG_* code. Returns RCPG_OK when every packing succeeded,
+ * else the first failing code, with that packing's index and message in err. */
+int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
+                       int32_t concurrency, rcpg_result** results, int32_t* status, char* err,
+                       size_t errlen);
+
 /* Step-wise control of one packing (the loop of run_packing_observed,
  * rcp_generator.cpp:5511-6662, advanced in slices). */
 typedef struct rcpg_engine rcpg_engine;
@@ -200,7 +212,7 @@ int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const dou
  * results as rcpg_pairs_full; the caller still passes every input and output.
  * The scratch is a fixed 8 MiB array of static device memory that every GPU
  * loading this library keeps until the process exits. A working set larger
- * than that -- about N*(16*P + 8*ndim + 20 + 4*row_capacity) bytes plus the
+ * than that -- about N*(16*P + 8*ndim + 24 + 4*row_capacity) bytes plus the
  * cell grid, P = 4 for ndim <= 3, i.e. roughly 20,000 particles in 3-D at
  * row_capacity 64 -- is rejected with RCPG_ENOSPC before any work. The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress)

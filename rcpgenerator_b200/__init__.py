@@ -11,6 +11,7 @@ from ._api import (
     get_num_threads,
     initialize_particles,
     run_packing,
+    run_packing_batch,
     run_packing_observed,
     set_num_threads,
 )
@@ -22,6 +23,7 @@ __all__ = [
     "get_num_threads",
     "initialize_particles",
     "run_packing",
+    "run_packing_batch",
     "run_packing_observed",
     "set_num_threads",
 ]

@@ -292,6 +292,34 @@ def run_packing_observed(input: dict, config: dict, progress_interval: int = 0,
     return {"result": out, "trace": tr}
 
 
+def run_packing_batch(items: list, options: dict | None = None, concurrency: int = 32,
+                      as_arrays: bool = True) -> list[dict]:
+    """Many independent packings, ``items`` = [(input, config), ...] as for
+    run_packing; the run options (``options`` plus the engine keys ``engine``,
+    ``pair_precision``, ``device``, ... of the first config) are shared. Runs
+    ``concurrency`` packings at a time on their own CUDA streams of one GPU
+    (the reference runs one process per core, rcptools/jobs.py:392-401) and
+    returns the result dicts in input order; a failed packing raises after
+    all have run, naming its index."""
+    items = list(items)
+    if not items:
+        return []
+    ins = [_Inputs(inp, cfg, options) for inp, cfg in items]
+    arr = (N.PackingInput * len(ins))(*[x.pi for x in ins])
+    res = (C.POINTER(N.Result) * len(ins))()
+    status = (C.c_int32 * len(ins))()
+    err = N.errbuf()
+    rc = N.lib.rcpg_run_batch(arr, len(ins), C.byref(ins[0].ro), int(concurrency), res, status,
+                              err, len(err))
+    try:
+        N.raise_for(rc, err)
+        return [result_to_dict(r.contents, as_arrays=as_arrays) for r in res]
+    finally:
+        for r in res:
+            if r:
+                N.lib.rcpg_result_free(r)
+
+
 class PackingEngine:
     """One packing advanced in slices of steps (rcpg_engine_* of the C ABI).
 

@@ -28,6 +28,7 @@ EXPORTED_SYMBOLS = (
     "rcpg_default_options",
     "rcpg_run_packing",
     "rcpg_result_free",
+    "rcpg_run_batch",
     "rcpg_engine_create",
     "rcpg_engine_advance",
     "rcpg_engine_steps",
@@ -180,6 +181,11 @@ def _load() -> C.CDLL:
              OBSERVER, vp, C.POINTER(C.POINTER(Result)), cp, sz],
         ),
         "rcpg_result_free": (None, [C.POINTER(Result)]),
+        "rcpg_run_batch": (
+            C.c_int32,
+            [C.POINTER(PackingInput), C.c_uint64, C.POINTER(RunOptions), C.c_int32,
+             C.POINTER(C.POINTER(Result)), C.POINTER(C.c_int32), cp, sz],
+        ),
         "rcpg_engine_create": (
             C.c_int32,
             [C.POINTER(PackingInput), C.POINTER(RunOptions), vp, C.POINTER(vp), cp, sz],

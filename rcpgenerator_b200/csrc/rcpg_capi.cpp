@@ -4,13 +4,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <exception>
 #include <new>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "rcpg_engine.h"
@@ -245,6 +248,69 @@ int32_t rcpg_run_packing(const rcpg_packing_input* in, const rcpg_run_options* o
     }
 }
 
+int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
+                       int32_t concurrency, rcpg_result** results, int32_t* status, char* err,
+                       size_t errlen) {
+    if ((!inputs && count) || (!results && count))
+        return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: null argument");
+    for (uint64_t k = 0; k < count; ++k) {
+        results[k] = nullptr;
+        if (status) status[k] = RCPG_OK;
+    }
+    if (count == 0) return RCPG_OK;
+    if (!have_device(err, errlen)) return RCPG_ECUDA;
+    rcpg_run_options o;
+    if (opt) o = *opt;
+    else rcpg_default_options(&o);
+    const uint64_t nthreads = std::max<uint64_t>(1, std::min<uint64_t>(count, concurrency > 0 ? concurrency : 1));
+    std::atomic<uint64_t> next{0};
+    std::mutex mu;
+    int32_t first_code = RCPG_OK;
+    uint64_t first_index = 0;
+    std::string first_msg;
+    auto record = [&](uint64_t k, int32_t code, const std::string& msg) {
+        if (status) status[k] = code;
+        std::lock_guard<std::mutex> lk(mu);
+        if (first_code == RCPG_OK || k < first_index) {
+            first_code = code;
+            first_index = k;
+            first_msg = msg;
+        }
+    };
+    auto worker = [&]() {
+        if (cudaSetDevice(o.device) != cudaSuccess) {
+            cudaGetLastError();
+            for (uint64_t k; (k = next.fetch_add(1)) < count;) record(k, RCPG_ECUDA, "rcpgenerator_b200: cudaSetDevice failed");
+            return;
+        }
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            for (uint64_t k; (k = next.fetch_add(1)) < count;) record(k, RCPG_ECUDA, "rcpgenerator_b200: cudaStreamCreate failed");
+            return;
+        }
+        for (uint64_t k; (k = next.fetch_add(1)) < count;) {
+            try {
+                rcpg::Engine eng(make_input(&inputs[k], &o), st);
+                eng.run(0, false, 0, rcpg::ObserverFn(), nullptr);
+                const rcpg::EngineResult r = eng.result();
+                results[k] = make_result(r, eng.N(), eng.ndim(), nullptr, false, eng.launches());
+            } catch (const std::exception& e) {
+                record(k, classify(e), e.what());
+            }
+        }
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    };
+    std::vector<std::thread> pool;
+    pool.reserve(nthreads);
+    for (uint64_t t = 0; t < nthreads; ++t) pool.emplace_back(worker);
+    for (auto& t : pool) t.join();
+    if (first_code != RCPG_OK)
+        return fail(err, errlen, first_code, "packing " + std::to_string(first_index) + ": " + first_msg);
+    return RCPG_OK;
+}
+
 void rcpg_result_free(rcpg_result* r) {
     if (!r) return;
     void* fields[] = {r->positions,       r->diameters,        r->box,           r->walls,
@@ -359,7 +425,7 @@ int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const dou
         a.cell_of = static_cast<std::uint32_t*>(sc.get(N * 4));
         a.cell_rank = static_cast<std::uint32_t*>(sc.get(N * 4));
         a.cell_list = static_cast<std::uint32_t*>(sc.get(N * 4));
-        a.work = a.cell_list;
+        a.work = static_cast<std::uint32_t*>(sc.get(N * 4));
         {
             const double cutoff = (Dmax + t_shell) * (1.0 + 1e-6);
             double cells = 1.0;
@@ -382,7 +448,7 @@ int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const dou
         cuda_ok(cudaMemsetAsync(a.caps, 0xFF, N * 4, st), "memset caps");
         rcpg::launch_pack(N, ndim, x_dev, D_dev, a.pos, st);
         rcpg::launch_rebuild(a, st);
-        rcpg::launch_rows_to_particle_order(N, a.cell_list, a.nbr, a.nbr_cnt, nbr_dev, cnt_dev, st);
+        rcpg::launch_rows_to_particle_order(N, a.work, a.nbr, a.nbr_cnt, nbr_dev, cnt_dev, st);
         cuda_ok(cudaMemcpyAsync(&h, a.ctl, sizeof(h), cudaMemcpyDeviceToHost, st), "D2H ctl");
         cuda_ok(cudaStreamSynchronize(st), "sync");
         cuda_ok(cudaGetLastError(), "kernel launch");

@@ -73,10 +73,11 @@ struct DevArrays {
     std::uint32_t* nbr;     // [S*N] column-major full rows (see sorted_rows)
     std::uint32_t* nbr_cnt; // [N]
     // Row slot -> particle map. Row t (nbr[k*N + t], nbr_cnt[t]) belongs to
-    // particle work[t]; the engine keeps rows in cell order (work = cell_list)
-    // so a warp's particles, and their partners, are spatial neighbours.
-    // nullptr = identity (rows in particle order).
-    const std::uint32_t* work;
+    // particle work[t]; rows are kept in cell order (a build writes work: the
+    // members of each cell in ascending particle order) so a warp's particles,
+    // and their partners, are spatial neighbours. nullptr = identity (rows in
+    // particle order).
+    std::uint32_t* work;
     std::uint32_t S;        // row capacity
     // 1: rows sorted by partner index (exact mode, pairs_full: the reference's
     // summation order); 0: rows in the build's fixed scan order (graph mode)
@@ -91,7 +92,7 @@ struct DevArrays {
     std::uint32_t* cell_rank;  // [N]
     std::uint32_t* cell_count; // [C_alloc + 1]
     std::uint32_t* cell_start; // [C_alloc + 1]
-    std::uint32_t* cell_list;  // [N]
+    std::uint32_t* cell_list;  // [N] members of each cell in arrival order (k_build_scatter)
     std::uint32_t C_alloc;
     std::uint32_t* scan_tmp;   // block sums of the scan
     ForceSums* block_sums;     // [nblocks of the force kernel]
@@ -106,8 +107,6 @@ struct DevArrays {
 };
 
 constexpr int kForceBlock = 256;
-constexpr int kSearchBlock = 128;
-constexpr int kSearchSmemRow = 64;
 
 RCPG_HD unsigned force_blocks(std::uint64_t N) {
     return static_cast<unsigned>((N + kForceBlock - 1) / kForceBlock);

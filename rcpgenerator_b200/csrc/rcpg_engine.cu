@@ -16,15 +16,42 @@
 #include <cerrno>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 
 namespace rcpg {
 
+// Device memory of an engine comes from the device's stream-ordered pool
+// (cudaMallocAsync / cudaFreeAsync on the engine's stream), so creating and
+// destroying engines never synchronises the device: engines on other streams
+// (a batch) keep running. The pinned control block used to read the device
+// controller is recycled through a process-wide free list for the same reason.
 namespace {
-
-constexpr double kPi = 3.14159265358979323846;
-
+std::mutex g_pinned_mu;
+std::vector<DevCtl*> g_pinned_free;
 }  // namespace
+
+DevCtl* pinned_ctl_acquire() {
+    {
+        std::lock_guard<std::mutex> lk(g_pinned_mu);
+        if (!g_pinned_free.empty()) {
+            DevCtl* p = g_pinned_free.back();
+            g_pinned_free.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, sizeof(DevCtl)) != cudaSuccess) {
+        cudaGetLastError();
+        throw EngineError(-2, "rcpgenerator_b200: cudaMallocHost of the control block failed");
+    }
+    return static_cast<DevCtl*>(p);
+}
+
+void pinned_ctl_release(DevCtl* p) {
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    g_pinned_free.push_back(p);
+}
 
 void Engine::check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) {
@@ -63,7 +90,7 @@ void Engine::alloc_device() {
     P_ = pos_stride(nd);
     auto dalloc = [&](std::size_t bytes) -> void* {
         void* p = nullptr;
-        check(cudaMalloc(&p, bytes < 16 ? 16 : bytes), "cudaMalloc");
+        check(cudaMallocAsync(&p, bytes < 16 ? 16 : bytes, st_), "cudaMallocAsync");
         allocs_.push_back(p);
         return p;
     };
@@ -85,7 +112,7 @@ void Engine::alloc_device() {
     a_.cell_of = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.cell_rank = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.cell_list = static_cast<std::uint32_t*>(dalloc(N * 4));
-    a_.work = a_.cell_list;  // rows are kept in the cell order of their build
+    a_.work = static_cast<std::uint32_t*>(dalloc(N * 4));  // row slot -> particle, written by each build
     // exact mode sums each row in ascending partner order, as the reference
     a_.sorted_rows = exact_ ? 1 : 0;
     a_.mixed = mixed_ ? 1 : 0;
@@ -145,7 +172,7 @@ void Engine::alloc_device() {
         hh_ = Histories{h_phi_.data(), h_force_.data(), h_energy_.data(), h_maxov_.data(),
                         h_mu_.data(), h_alpha_.data(), h_muflag_.data()};
     }
-    check(cudaMallocHost(&hctl_pinned_, sizeof(DevCtl)), "cudaMallocHost");
+    hctl_pinned_ = pinned_ctl_acquire();
 }
 
 void Engine::ensure_row_capacity(std::uint32_t need) {
@@ -156,7 +183,7 @@ void Engine::ensure_row_capacity(std::uint32_t need) {
     if (S < need) S = need;
     auto drop = [&](void* p) {
         if (!p) return;
-        cudaFree(p);
+        cudaFreeAsync(p, st_);
         allocs_.erase(std::remove(allocs_.begin(), allocs_.end(), p), allocs_.end());
     };
     drop(a_.nbr);
@@ -164,11 +191,11 @@ void Engine::ensure_row_capacity(std::uint32_t need) {
     a_.nbr = nullptr;
     a_.pterm = nullptr;
     void* p = nullptr;
-    check(cudaMalloc(&p, static_cast<std::size_t>(S) * N_ * 4), "cudaMalloc(nbr)");
+    check(cudaMallocAsync(&p, static_cast<std::size_t>(S) * N_ * 4, st_), "cudaMallocAsync(nbr)");
     allocs_.push_back(p);
     a_.nbr = static_cast<std::uint32_t*>(p);
     if (exact_) {
-        check(cudaMalloc(&p, static_cast<std::size_t>(S) * N_ * sizeof(PairTerms)), "cudaMalloc(pterm)");
+        check(cudaMallocAsync(&p, static_cast<std::size_t>(S) * N_ * sizeof(PairTerms), st_), "cudaMallocAsync(pterm)");
         allocs_.push_back(p);
         a_.pterm = static_cast<PairTerms*>(p);
     }
@@ -178,9 +205,10 @@ void Engine::ensure_row_capacity(std::uint32_t need) {
 
 void Engine::free_device() {
     destroy_graph();
-    for (void* p : allocs_) cudaFree(p);
+    for (void* p : allocs_) cudaFreeAsync(p, st_);
     allocs_.clear();
-    if (hctl_pinned_) cudaFreeHost(hctl_pinned_);
+    if (st_) cudaStreamSynchronize(st_);
+    if (hctl_pinned_) pinned_ctl_release(hctl_pinned_);
     hctl_pinned_ = nullptr;
 }
 

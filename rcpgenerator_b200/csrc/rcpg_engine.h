@@ -50,6 +50,11 @@ struct TraceSample {
 
 using ObserverFn = std::function<void(const Observation&, const std::vector<double>* positions)>;
 
+struct DevCtl;
+// pinned host copies of the control block, recycled across engines
+DevCtl* pinned_ctl_acquire();
+void pinned_ctl_release(DevCtl* p);
+
 class EngineError : public std::runtime_error {
    public:
     EngineError(int code, const std::string& msg) : std::runtime_error(msg), code_(code) {}

@@ -272,29 +272,29 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-__device__ __forceinline__ std::uint32_t block_exclusive_scan(std::uint32_t v, std::uint32_t* smem,
-                                                              std::uint32_t& total) {
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* smem, T& total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    std::uint32_t s = v;
+    T s = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const std::uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+        const T y = __shfl_up_sync(0xffffffffu, s, o);
         if (lane >= o) s += y;
     }
     if (lane == 31) smem[warp] = s;
     __syncthreads();
     if (warp == 0) {
         const int nw = blockDim.x >> 5;
-        std::uint32_t w = lane < nw ? smem[lane] : 0u;
+        T w = lane < nw ? smem[lane] : T(0);
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const std::uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            const T y = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= o) w += y;
         }
         if (lane < nw) smem[lane] = w;
     }
     __syncthreads();
-    const std::uint32_t warp_off = warp ? smem[warp - 1] : 0u;
+    const T warp_off = warp ? smem[warp - 1] : T(0);
     total = smem[(blockDim.x >> 5) - 1];
     __syncthreads();
     return warp_off + s - v;
@@ -356,154 +356,183 @@ __global__ void __launch_bounds__(256) k_build_scatter(DevArrays a) {
     a.cell_list[a.cell_start[a.cell_of[i]] + a.cell_rank[i]] = static_cast<std::uint32_t>(i);
 }
 
-// Members of each cell in ascending particle order (the atomic ranks of
-// k_build_bin are arrival order; row slots and per-block force sums must not
-// depend on it), and a copy of their positions in that order (spos), so the
-// search reads each cell's candidates from contiguous memory.
+template <int ND>
+__device__ __forceinline__ bool tiled_build_ok(const DevCtl* ctl);
+
+// Particles below which the tiled search is not used: a small packing has too
+// few tiles to fill the GPU, and the warp search (k_build_search) spreads one
+// particle over 32 lanes instead.
+constexpr std::uint64_t kTiledMinN = 20000;
+
+template <int ND>
+__device__ __forceinline__ bool use_tiled(const DevCtl* ctl, std::uint64_t N) {
+    return (N >= kTiledMinN) & tiled_build_ok<ND>(ctl);
+}
+
+// Builds without the tiled search: the members of each cell in ascending
+// particle order in work (the atomic ranks of k_build_bin are arrival order;
+// row slots and per-block force sums must not depend on it), and a copy of
+// their positions in that order (spos), so the search reads each cell's
+// candidates from contiguous memory. The tiled search orders its cells itself.
 template <int ND>
 __global__ void __launch_bounds__(256) k_build_cell_sort(DevArrays a) {
     const DevCtl* ctl = a.ctl;
-    if (build_off(ctl)) return;
+    if (build_off(ctl) | use_tiled<ND>(ctl, a.N)) return;
     const std::uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ctl->ncells) return;
     const std::uint32_t q0 = a.cell_start[c], q1 = a.cell_start[c + 1];
-    for (std::uint32_t k = q0 + 1; k < q1; ++k) {
+    for (std::uint32_t k = q0; k < q1; ++k) {
         const std::uint32_t v = a.cell_list[k];
         std::uint32_t p = k;
-        while (p > q0 && a.cell_list[p - 1] > v) {
-            a.cell_list[p] = a.cell_list[p - 1];
+        while (p > q0 && a.work[p - 1] > v) {
+            a.work[p] = a.work[p - 1];
             --p;
         }
-        a.cell_list[p] = v;
+        a.work[p] = v;
     }
     constexpr int P = pos_stride(ND);
     for (std::uint32_t q = q0; q < q1; ++q) {
-        const double2* src = reinterpret_cast<const double2*>(a.pos + static_cast<std::uint64_t>(a.cell_list[q]) * P);
+        const double2* src = reinterpret_cast<const double2*>(a.pos + static_cast<std::uint64_t>(a.work[q]) * P);
         double2* dst = reinterpret_cast<double2*>(a.spos + static_cast<std::uint64_t>(q) * P);
         RCPG_UNROLL
         for (int h = 0; h < P / 2; ++h) dst[h] = src[h];
     }
 }
 
-// Neighbour rows: every j != i in the 3^ndim cell neighbourhood passing the
-// reference's shell test, sorted ascending. Thread t builds row slot t, the
-// row of particle cell_list[t]: the threads of a warp hold neighbouring cells
-// and read the same candidate cells. Rows are gathered in shared memory
-// (kSearchSmemRow per thread, bank = lane); longer rows continue in the
-// global row and are sorted there.
-template <int ND>
-__device__ __forceinline__ bool tiled_build_ok(const DevCtl* ctl);
+// Warp search (every build the tiled search does not take: ndim > 3, small
+// packings, grids narrower than a tile). One warp per row slot t (particle
+// work[t]); its lanes share the 3^ndim neighbour cells, test every member
+// against the reference's shell predicate, and collect the partners in shared
+// memory; the row is then sorted ascending by a bitonic sort in the warp, so
+// it does not depend on the order in which the lanes found its entries.
+constexpr int kWarpSearchWarps = 4;    // warps per block
+constexpr int kWarpRowSmem = 256;      // row entries sorted in shared memory
 
 template <int ND>
-__global__ void __launch_bounds__(kSearchBlock) k_build_search(DevArrays a) {
+__global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArrays a) {
     DevCtl* ctl = a.ctl;
-    if (build_off(ctl) | tiled_build_ok<ND>(ctl)) return;
+    const std::uint64_t N = a.N;
+    if (build_off(ctl) | use_tiled<ND>(ctl, N)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->forces_done = 0u;
-    __shared__ std::uint32_t buf[kSearchSmemRow * kSearchBlock];
+    __shared__ std::uint32_t buf[kWarpSearchWarps][kWarpRowSmem];
+    __shared__ std::uint32_t cnt[kWarpSearchWarps];
     __shared__ std::uint32_t block_need;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (threadIdx.x == 0) block_need = 0u;
     __syncthreads();
-    const std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
-    const std::uint64_t N = a.N;
     const std::uint32_t S = a.S;
-    std::uint32_t n = 0, n_half = 0;
-    std::uint64_t i = 0;
-    std::uint32_t* mine = buf + threadIdx.x;
-    if (t < N) {
-        i = a.cell_list[t];
-        const Geometry g = ctl->g;  // register copy: the loops below store through other pointers
-        const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
+    const Geometry& g = ctl->g;
+    const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
+    double bx[ND], ibx[ND], scale[ND];
+    int nc[ND], nn[ND];
+    int total_combo = 1;
+    RCPG_UNROLL
+    for (int d = 0; d < ND; ++d) {
+        bx[d] = g.box[d];
+        ibx[d] = g.inv_box[d];
+        scale[d] = ctl->cell_scale[d];
+        nc[d] = ctl->ncell[d];
+        nn[d] = nc[d] < 3 ? nc[d] : 3;  // distinct neighbour cells on this axis
+        total_combo *= nn[d];
+    }
+    std::uint32_t* row = buf[w];
+    const std::uint64_t warps = static_cast<std::uint64_t>(gridDim.x) * kWarpSearchWarps;
+    for (std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(kWarpSearchWarps) + w; t < N; t += warps) {
+        const std::uint32_t i = a.work[t];
         double xi[ND], D0i;
         load_pos<ND>(a.spos, t, xi, D0i);
         const double Di = xmul(D0i, kap);
-        int cc[ND], nn[ND], nc[ND];
+        int cc[ND];
         RCPG_UNROLL
-        for (int d = 0; d < ND; ++d) {
-            nc[d] = ctl->ncell[d];
-            cc[d] = cell_coord(xi[d], ctl->cell_scale[d], nc[d]);
-            nn[d] = nc[d] < 3 ? nc[d] : 3;  // distinct neighbour cells on this axis
-        }
-        int total_combo = 1;
-        RCPG_UNROLL
-        for (int d = 0; d < ND; ++d) total_combo *= nn[d];
-        int odo[ND];
-        RCPG_UNROLL
-        for (int d = 0; d < ND; ++d) odo[d] = 0;
-        for (int combo = 0; combo < total_combo; ++combo) {
+        for (int d = 0; d < ND; ++d) cc[d] = cell_coord(xi[d], scale[d], nc[d]);
+        if (lane == 0) cnt[w] = 0u;
+        __syncwarp();
+        std::uint32_t n_half = 0;
+        for (int combo = lane; combo < total_combo; combo += 32) {
             std::uint32_t cell = 0, mul = 1;
+            int r = combo;
             RCPG_UNROLL
             for (int d = 0; d < ND; ++d) {
-                const int k = odo[d];
+                const int k = r % nn[d];
+                r /= nn[d];
                 int c = (nc[d] >= 3) ? cc[d] - 1 + k : k;
                 if (c < 0) c += nc[d];
                 else if (c >= nc[d]) c -= nc[d];
                 cell += static_cast<std::uint32_t>(c) * mul;
                 mul *= static_cast<std::uint32_t>(nc[d]);
             }
-            RCPG_UNROLL
-            for (int d = 0; d < ND; ++d) {
-                if (++odo[d] < nn[d]) break;
-                odo[d] = 0;
-            }
             const std::uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
             for (std::uint32_t q = q0; q < q1; ++q) {
-                const std::uint32_t j = a.cell_list[q];
+                const std::uint32_t j = a.work[q];
                 if (j == i) continue;
                 double xj[ND], D0j;
                 load_pos<ND>(a.spos, q, xj, D0j);
                 const double Dj = xmul(D0j, kap);
-                const bool ok = (ND <= 3 || j > i)
-                                    ? in_shell<ND>(xi, xj, Di, Dj, g.box, g.inv_box, t_shell)
-                                    : in_shell<ND>(xi, xj, Dj, Di, g.box, g.inv_box, t_shell);
+                const bool ok = (ND <= 3 || j > i) ? in_shell<ND>(xi, xj, Di, Dj, bx, ibx, t_shell)
+                                                   : in_shell<ND>(xi, xj, Dj, Di, bx, ibx, t_shell);
                 if (!ok) continue;
-                if (n < kSearchSmemRow) mine[n * kSearchBlock] = j;
-                else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + t] = j;
-                ++n;
+                const std::uint32_t slot = atomicAdd(&cnt[w], 1u);
+                if (slot < static_cast<std::uint32_t>(kWarpRowSmem)) row[slot] = j;
+                else if (slot < S) a.nbr[static_cast<std::uint64_t>(slot) * N + t] = j;
                 if (j > i) ++n_half;
             }
         }
-        const std::uint32_t cap = a.caps[i];
-        if (n_half > cap) {
-            if (atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-                ctl->cap_error_particle = static_cast<std::uint32_t>(i);
+        __syncwarp();
+        const std::uint32_t n = cnt[w];
+        RCPG_UNROLL
+        for (int o = 16; o > 0; o >>= 1) n_half += __shfl_xor_sync(0xffffffffu, n_half, o);
+        if (lane == 0) {
+            const std::uint32_t cap = a.caps[i];
+            if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
+                ctl->cap_error_particle = i;
                 ctl->cap_error_cap = cap;
             }
+            atomicMax(&block_need, n);
+            a.nbr_cnt[t] = n > S ? 0u : n;  // overflow: empty row, rebuilt after the capacity grows
         }
-        atomicMax(&block_need, n);  // shared-memory atomic
+        if (n > S) continue;
+        if (n <= static_cast<std::uint32_t>(kWarpRowSmem)) {
+            // bitonic sort of the row padded to a power of two
+            std::uint32_t p2 = 1;
+            while (p2 < n) p2 <<= 1;
+            for (std::uint32_t e = n + lane; e < p2; e += 32) row[e] = 0xffffffffu;
+            __syncwarp();
+            for (std::uint32_t kk = 2; kk <= p2; kk <<= 1) {
+                for (std::uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
+                    for (std::uint32_t e = lane; e < p2; e += 32) {
+                        const std::uint32_t f = e ^ jj;
+                        if (f > e) {
+                            const std::uint32_t x = row[e], y = row[f];
+                            const bool up = (e & kk) == 0;
+                            if ((x > y) == up) {
+                                row[e] = y;
+                                row[f] = x;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            for (std::uint32_t e = lane; e < n; e += 32) a.nbr[static_cast<std::uint64_t>(e) * N + t] = row[e];
+        } else if (lane == 0) {
+            // longer than the shared buffer: the row in global memory, sorted there
+            for (std::uint32_t e = 0; e < static_cast<std::uint32_t>(kWarpRowSmem); ++e)
+                a.nbr[static_cast<std::uint64_t>(e) * N + t] = row[e];
+            std::uint32_t* gr = a.nbr + t;
+            for (std::uint32_t k = 1; k < n; ++k) {
+                const std::uint32_t v = gr[static_cast<std::uint64_t>(k) * N];
+                std::uint32_t p = k;
+                while (p > 0 && gr[static_cast<std::uint64_t>(p - 1) * N] > v) {
+                    gr[static_cast<std::uint64_t>(p) * N] = gr[static_cast<std::uint64_t>(p - 1) * N];
+                    --p;
+                }
+                gr[static_cast<std::uint64_t>(p) * N] = v;
+            }
+        }
+        __syncwarp();
     }
     __syncthreads();
     if (threadIdx.x == 0 && block_need) atomicMax(&ctl->row_need, block_need);
-    if (t >= N) return;
-    if (n > S) {
-        a.nbr_cnt[t] = 0;  // overflow: empty row, rebuilt after the capacity grows
-        return;
-    }
-    a.nbr_cnt[t] = n;
-    if (n <= static_cast<std::uint32_t>(kSearchSmemRow)) {
-        for (std::uint32_t k = 1; k < n; ++k) {
-            const std::uint32_t v = mine[k * kSearchBlock];
-            std::uint32_t p = k;
-            while (p > 0 && mine[(p - 1) * kSearchBlock] > v) {
-                mine[p * kSearchBlock] = mine[(p - 1) * kSearchBlock];
-                --p;
-            }
-            mine[p * kSearchBlock] = v;
-        }
-        for (std::uint32_t k = 0; k < n; ++k) a.nbr[static_cast<std::uint64_t>(k) * N + t] = mine[k * kSearchBlock];
-    } else {
-        for (std::uint32_t k = 0; k < static_cast<std::uint32_t>(kSearchSmemRow); ++k)
-            a.nbr[static_cast<std::uint64_t>(k) * N + t] = mine[k * kSearchBlock];
-        std::uint32_t* row = a.nbr + t;
-        for (std::uint32_t k = 1; k < n; ++k) {
-            const std::uint32_t v = row[static_cast<std::uint64_t>(k) * N];
-            std::uint32_t p = k;
-            while (p > 0 && row[static_cast<std::uint64_t>(p - 1) * N] > v) {
-                row[static_cast<std::uint64_t>(p) * N] = row[static_cast<std::uint64_t>(p - 1) * N];
-                --p;
-            }
-            row[static_cast<std::uint64_t>(p) * N] = v;
-        }
-    }
 }
 
 // ---- tiled search (ndim 2, 3) ---------------------------------------------
@@ -525,16 +554,18 @@ template <> struct TileShape<3> {
     static constexpr int stage = 1280;
 };
 constexpr int kTileThreads = 256;
-constexpr int kTileRow = 32;
+constexpr int kTileRow = 32;  // staged row entries per thread (sorted rows)
+constexpr int kTileOvl = 16;  // staged overlap candidates per thread (mixed precision)
 
 // dynamic shared memory of k_build_search_tiled<ND, SORT>: the staged rows
 // (SORT only) follow the staged particles
 template <int ND, bool SORT>
 constexpr std::size_t tile_smem_bytes() {
     using TS = TileShape<ND <= 3 ? ND : 3>;
-    return static_cast<std::size_t>(TS::stage) * pos_stride(ND) * 8 + 2ull * TS::stage * 4 +
+    return static_cast<std::size_t>(TS::stage) * pos_stride(ND) * 8 + (SORT ? 0 : 16ull * TS::stage) +
+           2ull * TS::stage * 4 +
            (TS::halo_cells + 2) * 4 + 2ull * TS::stage * 2 +
-           (SORT ? static_cast<std::size_t>(kTileRow) * kTileThreads * 2 : 0);
+           static_cast<std::size_t>(SORT ? kTileRow : kTileOvl) * kTileThreads * 2;
 }
 
 template <int ND>
@@ -596,16 +627,22 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     constexpr int HC = TS::halo_cells;
     DevCtl* ctl = a.ctl;
     if (ND > 3) return;
-    if (build_off(ctl) | !tiled_build_ok<ND>(ctl)) return;
+    if (build_off(ctl) | !use_tiled<ND>(ctl, a.N)) return;
     extern __shared__ __align__(16) unsigned char tile_smem[];
     double* s_pos = reinterpret_cast<double*>(tile_smem);
-    std::uint32_t* s_id = reinterpret_cast<std::uint32_t*>(s_pos + STAGE * P);
+    // mixed precision: FP32 positions relative to the tile's corner (halo
+    // cells across the periodic boundary unwrapped) and the FP32 diameter
+    float4* s_xf = reinterpret_cast<float4*>(s_pos + STAGE * P);
+    std::uint32_t* s_id = reinterpret_cast<std::uint32_t*>(SORT ? reinterpret_cast<unsigned char*>(s_xf)
+                                                                : reinterpret_cast<unsigned char*>(s_xf + STAGE));
     std::uint32_t* s_slot = s_id + STAGE;
     std::uint32_t* s_cstart = s_slot + STAGE;
     std::uint16_t* s_inner = reinterpret_cast<std::uint16_t*>(s_cstart + HC + 2);
     std::uint16_t* s_cell = s_inner + STAGE;
-    std::uint16_t* s_rows = s_cell + STAGE;  // [kTileRow][kTileThreads] staged indices (SORT)
-    __shared__ std::uint32_t s_warp[kTileThreads / 32];
+    // [kTileRow][kTileThreads] staged row entries (SORT) or
+    // [kTileOvl][kTileThreads] staged overlap candidates (mixed precision)
+    std::uint16_t* s_rows = s_cell + STAGE;
+    __shared__ unsigned long long s_warp2[kTileThreads / 32];
     __shared__ std::uint32_t s_need, s_ninner;
     __shared__ ForceSums s_red[kTileThreads / 32];
     const std::uint64_t N = a.N;
@@ -631,10 +668,12 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     __shared__ float hbf[ND];  // half box, FP32 (mixed minimum image)
     if (threadIdx.x < ND) hbf[threadIdx.x] = static_cast<float>(0.5 * ctl->g.box[threadIdx.x]);
     int nc[ND], nt[ND];
+    double cellw[ND];  // origin of a tile's relative coordinates: its first cell's corner
     std::uint32_t tiles = 1;
     RCPG_UNROLL
     for (int d = 0; d < ND; ++d) {
         nc[d] = ctl->ncell[d];
+        cellw[d] = ctl->g.box[d] / static_cast<double>(nc[d]);
         nt[d] = (nc[d] + TS::t(d) - 1) / TS::t(d);
         tiles *= static_cast<std::uint32_t>(nt[d]);
     }
@@ -662,6 +701,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
         // 1. particle count of every halo cell, 2. block scans -> staging offsets
         std::uint32_t cs = 0, cnt = 0;
         bool inner_cell = false;
+        int wrap[ND];  // -1 / +1: halo cell across the lower / upper periodic boundary
         if (static_cast<int>(threadIdx.x) < H) {
             int r = threadIdx.x;
             std::uint32_t c = 0, mul = 1;
@@ -672,18 +712,26 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                 r /= hw[d];
                 inner_cell = inner_cell && l >= 1 && l <= hw[d] - 2;
                 int gc = t0[d] - 1 + l;
-                if (gc < 0) gc += nc[d];
-                else if (gc >= nc[d]) gc -= nc[d];
+                wrap[d] = 0;
+                if (gc < 0) {
+                    gc += nc[d];
+                    wrap[d] = -1;
+                } else if (gc >= nc[d]) {
+                    gc -= nc[d];
+                    wrap[d] = 1;
+                }
                 c += static_cast<std::uint32_t>(gc) * mul;
                 mul *= static_cast<std::uint32_t>(nc[d]);
             }
             cs = a.cell_start[c];
             cnt = a.cell_start[c + 1] - cs;
         }
-        std::uint32_t total;
-        const std::uint32_t off = block_exclusive_scan(cnt, s_warp, total);
-        std::uint32_t ninner;
-        const std::uint32_t ioff = block_exclusive_scan(inner_cell ? cnt : 0u, s_warp, ninner);
+        // one scan of (inner count << 32 | count): staging offsets and inner-list offsets
+        unsigned long long tot2;
+        const unsigned long long off2 = block_exclusive_scan<unsigned long long>(
+            (static_cast<unsigned long long>(inner_cell ? cnt : 0u) << 32) | cnt, s_warp2, tot2);
+        const std::uint32_t off = static_cast<std::uint32_t>(off2), total = static_cast<std::uint32_t>(tot2);
+        const std::uint32_t ioff = static_cast<std::uint32_t>(off2 >> 32), ninner = static_cast<std::uint32_t>(tot2 >> 32);
         if (static_cast<int>(threadIdx.x) < H) s_cstart[threadIdx.x] = off;
         if (threadIdx.x == 0) {
             s_cstart[H] = total;
@@ -692,16 +740,43 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
         const bool fits = total <= static_cast<std::uint32_t>(STAGE);
         // 3. stage the halo particles (one thread per halo cell) and list the tile's own
         if (fits && static_cast<int>(threadIdx.x) < H) {
+            // the cell's members in ascending particle order (the bin's atomic
+            // ranks are arrival order); the owner tile of a cell publishes that
+            // order as the cell's row slots (work)
+            std::uint32_t* ids = s_id + off;
+            for (std::uint32_t k = 0; k < cnt; ++k) {
+                const std::uint32_t v = a.cell_list[cs + k];
+                std::uint32_t p = k;
+                while (p > 0 && ids[p - 1] > v) {
+                    ids[p] = ids[p - 1];
+                    --p;
+                }
+                ids[p] = v;
+            }
             for (std::uint32_t k = 0; k < cnt; ++k) {
                 const std::uint32_t q = cs + k, dst = off + k;
-                const double2* src = reinterpret_cast<const double2*>(a.spos + static_cast<std::uint64_t>(q) * P);
+                const std::uint32_t id = ids[k];
+                const double2* src = reinterpret_cast<const double2*>(a.pos + static_cast<std::uint64_t>(id) * P);
                 double2* sp = reinterpret_cast<double2*>(s_pos + dst * P);
                 RCPG_UNROLL
                 for (int h = 0; h < P / 2; ++h) sp[h] = src[h];
-                s_id[dst] = a.cell_list[q];
+                if (!SORT && mixed) {
+                    double xs[ND], D0s;
+                    load_pos<ND>(s_pos, dst, xs, D0s);
+                    float r4[4] = {0.0f, 0.0f, 0.0f, static_cast<float>(D0s) * kapf};
+                    RCPG_UNROLL
+                    for (int d = 0; d < (ND < 3 ? ND : 3); ++d) {
+                        const double xu = wrap[d] ? xadd(xs[d], wrap[d] * bx[d]) : xs[d];
+                        r4[d] = static_cast<float>(xsub(xu, xmul(static_cast<double>(t0[d]), cellw[d])));
+                    }
+                    s_xf[dst] = make_float4(r4[0], r4[1], r4[2], r4[3]);
+                }
                 s_slot[dst] = q;
                 s_cell[dst] = static_cast<std::uint16_t>(threadIdx.x);
-                if (inner_cell) s_inner[ioff + k] = static_cast<std::uint16_t>(dst);
+                if (inner_cell) {
+                    s_inner[ioff + k] = static_cast<std::uint16_t>(dst);
+                    a.work[q] = id;
+                }
             }
         }
         __syncthreads();
@@ -726,10 +801,21 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                     c += static_cast<std::uint32_t>(t0[d] - 1 + hl[d]) * mul;
                     mul *= static_cast<std::uint32_t>(nc[d]);
                 }
-                for (std::uint32_t q = a.cell_start[c]; q < a.cell_start[c + 1]; ++q) {
-                    const std::uint32_t i = a.cell_list[q];
+                // this tile owns the cell: its members in ascending order as row slots
+                const std::uint32_t q0 = a.cell_start[c], q1 = a.cell_start[c + 1];
+                for (std::uint32_t k = q0; k < q1; ++k) {
+                    const std::uint32_t v = a.cell_list[k];
+                    std::uint32_t p = k;
+                    while (p > q0 && a.work[p - 1] > v) {
+                        a.work[p] = a.work[p - 1];
+                        --p;
+                    }
+                    a.work[p] = v;
+                }
+                for (std::uint32_t q = q0; q < q1; ++q) {
+                    const std::uint32_t i = a.work[q];
                     double xi[ND], D0i;
-                    load_pos<ND>(a.spos, q, xi, D0i);
+                    load_pos<ND>(a.pos, i, xi, D0i);
                     const double Di = xmul(D0i, kap);
                     std::uint32_t n = 0, n_half = 0;
                     int odo[ND];
@@ -752,10 +838,10 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                             odo[d] = 0;
                         }
                         for (std::uint32_t pp = a.cell_start[cn]; pp < a.cell_start[cn + 1]; ++pp) {
-                            const std::uint32_t j = a.cell_list[pp];
+                            const std::uint32_t j = a.cell_list[pp];  // any order: the row is sorted at the end
                             if (j == i) continue;
                             double xj[ND], D0j;
-                            load_pos<ND>(a.spos, pp, xj, D0j);
+                            load_pos<ND>(a.pos, j, xj, D0j);
                             if (!in_shell<ND>(xi, xj, Di, xmul(D0j, kap), bx, ibx, t_shell)) continue;
                             if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
                             ++n;
@@ -813,15 +899,15 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                     const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 3];
                     for (std::uint32_t pp = p0; pp < p1; ++pp) {
                         if (pp == k) continue;
-                        double xj[ND], D0j;
-                        load_pos<ND>(s_pos, pp, xj, D0j);
                         bool overlap;
                         double dx[ND], d2, Dj;
                         float dxf[ND], d2f, rsum;
+                        double xj[ND], D0j;
+                        load_pos<ND>(s_pos, pp, xj, D0j);
                         if constexpr (MX) {
                             // FP32 shell test on the FP64 difference, widened by
                             // kShellMarginF so that the row holds every pair of the
-                            // FP64 shell (the list only has to contain the overlaps)
+                            // FP64 shell (the list only has to hold the overlaps)
                             d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
                             rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
                             const float rc = rsum + tf;
@@ -867,8 +953,71 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                     for (int d = 0; d < ND; ++d) fi[d] = static_cast<double>(fif[d]);
                 }
             };
-            if (!SORT && mixed) scan(std::true_type{});
-            else scan(std::false_type{});
+            // Mixed precision, two passes. 1: every candidate is tested on the
+            // tile-relative FP32 positions (widened by kShellMarginF, so the row
+            // holds every pair of the FP64 shell), the row is written, and the
+            // possible overlaps are staged. 2: the staged candidates are decided
+            // on the FP64 difference -- the test k_forces makes -- and their
+            // forces summed in row order. Separating the passes keeps the lanes
+            // of a warp on the same instructions in the frequent test.
+            auto scan_mixed = [&]() {
+                const float4 pi4 = s_xf[k];
+                std::uint32_t nov = 0;
+                float fif[ND];
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) fif[d] = 0.0f;
+                auto force_of = [&](std::uint32_t pp) {
+                    double xj[ND], D0j;
+                    load_pos<ND>(s_pos, pp, xj, D0j);
+                    float dxf[ND];
+                    const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
+                    const float rsum = 0.5f * (pi4.w + s_xf[pp].w);
+                    if (!(d2f < rsum * rsum)) return;
+                    PairTerms pt;
+                    pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
+                    if (s_id[pp] > i) {
+                        fU = xadd(fU, pt.U);
+                        fLc = xadd(fLc, pt.Lc);
+                        fdk = xadd(fdk, pt.dk);
+                        fFm = xadd(fFm, pt.Fm);
+                        fmaxov = fmax(fmaxov, pt.U);
+                        ++fcount;
+                    }
+                };
+                for (int rr = 0; rr < NROW; ++rr) {
+                    const int hc = hbase + (rr % 3) * hw[0] + (ND == 2 ? 0 : (rr / 3) * hw[0] * hw[1]);
+                    const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 3];
+                    for (std::uint32_t pp = p0; pp < p1; ++pp) {
+                        const float4 pj = s_xf[pp];
+                        const float ex = pj.x - pi4.x, ey = pj.y - pi4.y, ez = ND == 3 ? pj.z - pi4.z : 0.0f;
+                        const float d2r = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, ex * ex));
+                        const float rsum = 0.5f * (pi4.w + pj.w);
+                        const float rc = rsum + tf;
+                        if (!(d2r < rc * rc * kShellMarginF) || pp == k) continue;
+                        const std::uint32_t j = s_id[pp];
+                        if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
+                        ++n;
+                        if (j > i) ++n_half;
+                        if (fuse && d2r < rsum * rsum * kShellMarginF) {
+                            if (nov < static_cast<std::uint32_t>(kTileOvl))
+                                mine[nov * kTileThreads] = static_cast<std::uint16_t>(pp);
+                            else
+                                force_of(pp);  // more possible overlaps than staged: at once
+                            ++nov;
+                        }
+                    }
+                }
+                const std::uint32_t ns = nov < static_cast<std::uint32_t>(kTileOvl) ? nov : kTileOvl;
+                for (std::uint32_t e = 0; e < ns; ++e) force_of(mine[e * kTileThreads]);
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) fi[d] = static_cast<double>(fif[d]);
+            };
+            if constexpr (!SORT) {
+                if (mixed) scan_mixed();
+                else scan(std::false_type{});
+            } else {
+                scan(std::false_type{});
+            }
             const std::uint32_t cap = a.caps[i];
             if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
                 ctl->cap_error_particle = i;
@@ -1591,12 +1740,13 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     scan_exclusive(a.cell_count, a.cell_start, a.C_alloc + 1, a.scan_tmp, a.ctl, st);
     k_build_scatter<<<nb, kForceBlock, 0, st>>>(a);
     k_build_cell_sort<ND><<<(a.C_alloc + 255) / 256, 256, 0, st>>>(a);
-    const unsigned sb = static_cast<unsigned>((a.N + kSearchBlock - 1) / kSearchBlock);
     if (ND <= 3) {
         if (a.sorted_rows) launch_tiled<ND, true>(a, st);
         else launch_tiled<ND, false>(a, st);
     }
-    k_build_search<ND><<<sb, kSearchBlock, 0, st>>>(a);
+    const unsigned need = static_cast<unsigned>((a.N + kWarpSearchWarps - 1) / kWarpSearchWarps),
+                   g = resident_grid<k_build_search<ND>>(32 * kWarpSearchWarps);
+    k_build_search<ND><<<need < g ? need : g, 32 * kWarpSearchWarps, 0, st>>>(a);
 }
 
 }  // namespace

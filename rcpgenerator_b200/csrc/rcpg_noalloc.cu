@@ -133,12 +133,12 @@ extern "C" int32_t rcpg_pairs_full_noalloc(uint64_t N, int32_t ndim, const doubl
     a.cell_of = cv.take<std::uint32_t>(N);
     a.cell_rank = cv.take<std::uint32_t>(N);
     a.cell_list = cv.take<std::uint32_t>(N);
+    a.work = cv.take<std::uint32_t>(N);
     a.nbr_cnt = cv.take<std::uint32_t>(N);
     a.nbr = cv.take<std::uint32_t>(static_cast<std::size_t>(row_capacity) * N);
     a.scan_tmp = cv.take<std::uint32_t>(2 * 4096 + 16);
     a.S = row_capacity;
     a.sorted_rows = 1;  // the reference's row order
-    a.work = a.cell_list;
     if (!cv.ok) {
         set_err(err, errlen,
                 "rcpgenerator_b200: rcpg_pairs_full_noalloc needs more than its fixed 8 MiB "
@@ -186,7 +186,7 @@ extern "C" int32_t rcpg_pairs_full_noalloc(uint64_t N, int32_t ndim, const doubl
     k_noalloc_dmax<<<1, 1024, 0, st>>>(N, D_dev, a.ctl);
     rcpg::launch_pack(N, ndim, x_dev, D_dev, a.pos, st);
     rcpg::launch_rebuild(a, st);
-    rcpg::launch_rows_to_particle_order(N, a.cell_list, a.nbr, a.nbr_cnt, nbr_dev, cnt_dev, st);
+    rcpg::launch_rows_to_particle_order(N, a.work, a.nbr, a.nbr_cnt, nbr_dev, cnt_dev, st);
     std::uint32_t need = 0;
     e = cudaMemcpyAsync(&need, &a.ctl->row_need, sizeof(need), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

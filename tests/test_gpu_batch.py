@@ -1,0 +1,73 @@
+"""Batches of independent packings (rcpg_run_batch / run_packing_batch).
+
+Each packing of a batch runs on one engine of its own, on the stream of the
+worker thread that took it, so its result must not depend on the batch: in
+the exact engine a batch of golden packings reproduces the reference bit for
+bit, and in the graph engine every packing equals the same packing run alone.
+"""
+
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["n16_2d", "n64_3d_bi", "n64_2d_walls_500", "n128_3d_sphere_3000", "n200_2d_disk_2500",
+         "n300_4d_1500"]
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def item(g, case, engine):
+    inp = {"positions": g[f"{case}/input_positions"], "diameters": g[f"{case}/input_diameters"]}
+    cfg = {"box": g[f"{case}/box_in"].tolist(), "walls": g[f"{case}/walls_in"].tolist(),
+           "neighbor_max": 0, "engine": engine}
+    return inp, cfg
+
+
+def test_exact_batch_reproduces_reference(cuda_device, golden):
+    import rcpgenerator_b200 as rb
+    g = golden("packs.npz")
+    # the golden cases with a step cap share it through the batch options only
+    # when equal, so run the uncapped ones and the capped ones separately
+    groups: dict[int, list[str]] = {}
+    for c in CASES:
+        groups.setdefault(int(g[f"{c}/max_steps"]), []).append(c)
+    for ms, cases in groups.items():
+        opts = {"max_steps": ms} if ms else {}
+        out = rb.run_packing_batch([item(g, c, "exact") for c in cases], opts, concurrency=3)
+        for c, r in zip(cases, out):
+            sc = g[f"{c}/scalars"]
+            assert r["steps"] == int(sc[0]), c
+            assert np.array_equal(r["positions"], g[f"{c}/positions"]), c
+            assert digest(r["phi_history"]) == str(g[f"{c}/phi_history_sha256"]), c
+
+
+def test_graph_batch_equals_single_runs(cuda_device, golden):
+    import rcpgenerator_b200 as rb
+    g = golden("packs.npz")
+    cases = ["n16_2d", "n64_3d_bi", "n200_2d_disk_2500"]
+    opts = {"max_steps": 1500}
+    out = rb.run_packing_batch([item(g, c, "graph") for c in cases] * 2, opts, concurrency=4)
+    for k, c in enumerate(cases):
+        inp, cfg = item(g, c, "graph")
+        alone = rb.run_packing_observed(inp, cfg, 0, False, 0, None, opts, as_arrays=True)["result"]
+        for r in (out[k], out[k + len(cases)]):
+            assert r["steps"] == alone["steps"]
+            assert np.array_equal(r["positions"], alone["positions"])
+            assert np.array_equal(r["phi_history"], alone["phi_history"])
+
+
+def test_batch_reports_the_failing_packing(cuda_device, golden):
+    import rcpgenerator_b200 as rb
+    g = golden("packs.npz")
+    good = item(g, "n16_2d", "graph")
+    bad_inp, bad_cfg = item(g, "n16_2d", "graph")
+    bad_cfg = dict(bad_cfg, box=[1.0, 1.0, 1.0])  # box length != ndim: the reference's error
+    with pytest.raises((ValueError, RuntimeError), match="packing 1"):
+        rb.run_packing_batch([good, (bad_inp, bad_cfg), good], {"max_steps": 50}, concurrency=2)
