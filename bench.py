@@ -219,7 +219,7 @@ def run_batch_workload(args) -> int:
     for _, c in items:
         c.update({"pair_precision": args.pair_precision, "device": local})
     # warm-up: load the kernels and the pools
-    rb.run_packing_batch(items[:2], {"max_steps": 50}, concurrency=2)
+    rb.run_packing_batch(items[:2], {"max_steps": 50}, concurrency=args.concurrency)
     t0 = time.perf_counter()
     single = rb.run_packing_batch(items[: args.batch_single], run_opts, concurrency=1)
     t1 = time.perf_counter()
@@ -248,7 +248,8 @@ def run_batch_workload(args) -> int:
         "dtype": "f64 state, f32 pair terms" if args.pair_precision == "mixed" else "f64",
         "data": "synthetic",
         "config": {"workload": f"batch{len(items)}_N64-16384_ndim234_phi0.10", "packings": len(items),
-                   "concurrency": args.concurrency, "engine": "graph",
+                   "concurrency": args.concurrency,
+                   "engine": "persistent batch kernel" if args.concurrency <= 0 else "graph engines on streams",
                    "pair_precision": args.pair_precision, "particle_steps": ps,
                    "mean_steps": float(np.mean(steps)), "parallelism": f"replicas{world}",
                    "timing": "host wall clock around run_packing_batch (inputs on the host, results back)"},
@@ -307,7 +308,8 @@ def main() -> int:
                     help="single: ADAM steps/s of one N=1M packing; batch: packings/hour of many small ones")
     ap.add_argument("--batch-count", type=int, default=128)
     ap.add_argument("--batch-single", type=int, default=8, help="packings timed one at a time")
-    ap.add_argument("--concurrency", type=int, default=32)
+    ap.add_argument("--concurrency", type=int, default=0,
+                    help="0: persistent batch engine (one launch, a thread block per packing); k: k engines on streams")
     ap.add_argument("--cpu-cap-steps", type=int, default=300)
     args = ap.parse_args()
     WORKLOAD["N"] = args.n

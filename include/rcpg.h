@@ -154,13 +154,18 @@ int32_t rcpg_run_packing(const rcpg_packing_input* in, const rcpg_run_options* o
 void rcpg_result_free(rcpg_result* r);
 
 /* Many independent packings (the reference's throughput pattern: one process
- * per core, rcptools/jobs.py:392-401, each calling run_packing). `concurrency`
- * host threads each drive one engine at a time on their own CUDA stream of
- * device opt->device, taking the next packing as theirs finishes, so the
- * small packings' kernels and graph replays overlap on the GPU. results[k]
- * receives packing k's result (free each with rcpg_result_free) or NULL, and
- * status[k] its RCPG_* code. Returns RCPG_OK when every packing succeeded,
- * else the first failing code, with that packing's index and message in err. */
+ * per core, rcptools/jobs.py:392-401, each calling run_packing), all with the
+ * run options `opt` (graph engine).
+ *   concurrency <= 0: the persistent batch engine -- one kernel per ndim in
+ *     which every thread block runs whole packings taken from a queue (no
+ *     kernel launch per step); packings that can reach a target-phi lock, and
+ *     exact runs, are refused with RCPG_EINVAL.
+ *   concurrency > 0: that many host threads each drive one ordinary engine at
+ *     a time on their own CUDA stream of device opt->device.
+ * results[k] receives packing k's result (free each with rcpg_result_free) or
+ * NULL, and status[k] its RCPG_* code. Returns RCPG_OK when every packing
+ * succeeded, else the first failing code, with that packing's index and
+ * message in err. */
 int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
                        int32_t concurrency, rcpg_result** results, int32_t* status, char* err,
                        size_t errlen);

@@ -292,15 +292,17 @@ def run_packing_observed(input: dict, config: dict, progress_interval: int = 0,
     return {"result": out, "trace": tr}
 
 
-def run_packing_batch(items: list, options: dict | None = None, concurrency: int = 32,
+def run_packing_batch(items: list, options: dict | None = None, concurrency: int = 0,
                       as_arrays: bool = True) -> list[dict]:
     """Many independent packings, ``items`` = [(input, config), ...] as for
     run_packing; the run options (``options`` plus the engine keys ``engine``,
-    ``pair_precision``, ``device``, ... of the first config) are shared. Runs
-    ``concurrency`` packings at a time on their own CUDA streams of one GPU
-    (the reference runs one process per core, rcptools/jobs.py:392-401) and
-    returns the result dicts in input order; a failed packing raises after
-    all have run, naming its index."""
+    ``pair_precision``, ``device``, ... of the first config) are shared.
+    ``concurrency`` 0 runs them in the persistent batch engine (one launch per
+    ndim, each thread block running whole packings); ``concurrency`` k > 0 runs
+    k ordinary engines at a time on their own CUDA streams (the reference runs
+    one process per core, rcptools/jobs.py:392-401). Returns the result dicts
+    in input order; a failed packing raises after all have run, naming its
+    index."""
     items = list(items)
     if not items:
         return []

@@ -1,0 +1,61 @@
+// Persistent batch engine (rcpg_batch.cu): many independent packings of one
+// ndim run by one kernel, each thread block taking whole packings from a queue.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rcpg_device.h"
+#include "rcpg_engine.h"
+#include "rcpg_setup.h"
+
+namespace rcpg {
+
+// One packing of a batch: where its arrays start in the concatenated buffers.
+struct BatchInst {
+    std::uint64_t off;       // first particle
+    std::uint64_t nbr_off;   // first row entry (S*N entries, column-major in the packing)
+    std::uint64_t cell_off;  // first cell counter (C_alloc + 1 entries)
+    std::uint64_t hist_off;  // first history entry (step_cap + 1 entries)
+    std::uint32_t N, S, C_alloc;
+    // 0 not started, 1 running, 2 finished, 3 rows outgrew S (run again with a
+    // larger S), 4 half row beyond the reference capacity, 5 needs a target-phi lock
+    std::uint32_t status;
+};
+
+// The concatenated device arrays of one launch (same layouts as DevArrays).
+struct BatchArrays {
+    double *pos, *spos, *F, *m, *v, *x_last, *pos_tmp, *vec_tmp;
+    std::uint32_t *nbr, *nbr_cnt, *caps, *cell_of, *cell_rank, *cell_list, *work, *cell_count, *cell_start;
+    std::uint64_t *origin, *u64_tmp, *keys0, *keys1;
+    std::uint32_t *vals0, *vals1;
+    double *h_phi, *h_force, *h_energy, *h_maxov, *h_mu, *h_alpha;
+    std::int8_t* h_muflag;
+    DevCtl* ctl;              // [instances]
+    BatchInst* inst;          // [instances]
+    std::uint32_t* active;    // indices of the instances this launch advances
+    std::uint32_t nactive;
+    std::uint32_t* queue;     // next entry of `active` to take
+};
+
+void launch_batch(const BatchArrays& B, int ndim, std::uint32_t chunk, int mixed, int device,
+                  cudaStream_t st);
+
+// Outcome of one packing of run_batch_persistent.
+struct BatchOutcome {
+    int code = 0;             // 0 ok, else an RCPG_* error code
+    std::string message;
+    EngineResult result;
+    std::uint64_t N = 0;
+    int ndim = 0;
+};
+
+// Runs every packing to completion in persistent launches of at most `chunk`
+// steps per packing. All share the run options of `ins[k]` (graph engine;
+// packings that can reach a target-phi lock are reported as unsupported).
+std::vector<BatchOutcome> run_batch_persistent(const std::vector<EngineInput>& ins, std::uint32_t chunk);
+
+}  // namespace rcpg

@@ -16,6 +16,7 @@
 #include <thread>
 #include <vector>
 
+#include "rcpg_batch.h"
 #include "rcpg_engine.h"
 #include "rcpg_init.h"
 
@@ -262,7 +263,36 @@ int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const r
     rcpg_run_options o;
     if (opt) o = *opt;
     else rcpg_default_options(&o);
-    const uint64_t nthreads = std::max<uint64_t>(1, std::min<uint64_t>(count, concurrency > 0 ? concurrency : 1));
+    if (concurrency <= 0) {
+        // one persistent launch per ndim: each thread block runs whole packings
+        try {
+            std::vector<rcpg::EngineInput> ins;
+            ins.reserve(count);
+            for (uint64_t k = 0; k < count; ++k) ins.push_back(make_input(&inputs[k], &o));
+            const std::vector<rcpg::BatchOutcome> res = rcpg::run_batch_persistent(ins, 2048u);
+            int32_t first = RCPG_OK;
+            std::string msg;
+            for (uint64_t k = 0; k < count; ++k) {
+                const rcpg::BatchOutcome& b = res[k];
+                int32_t code = RCPG_OK;
+                if (b.code == -22) code = RCPG_EINVAL;
+                else if (b.code == -2) code = RCPG_ECUDA;
+                else if (b.code != 0) code = RCPG_ERUNTIME;
+                if (status) status[k] = code;
+                if (code == RCPG_OK) {
+                    results[k] = make_result(b.result, b.N, b.ndim, nullptr, false, 0);
+                } else if (first == RCPG_OK) {
+                    first = code;
+                    msg = "packing " + std::to_string(k) + ": " + b.message;
+                }
+            }
+            if (first != RCPG_OK) return fail(err, errlen, first, msg);
+            return RCPG_OK;
+        } catch (const std::exception& e) {
+            return fail(err, errlen, classify(e), e.what());
+        }
+    }
+    const uint64_t nthreads = std::max<uint64_t>(1, std::min<uint64_t>(count, static_cast<uint64_t>(concurrency)));
     std::atomic<uint64_t> next{0};
     std::mutex mu;
     int32_t first_code = RCPG_OK;

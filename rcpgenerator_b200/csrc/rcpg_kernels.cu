@@ -16,6 +16,7 @@
 #include <type_traits>
 
 #include "rcpg_device.h"
+#include "rcpg_devutil.cuh"
 
 namespace rcpg {
 
@@ -34,99 +35,6 @@ __device__ __forceinline__ bool ctl_idle(const DevCtl* ctl) {
 __device__ __forceinline__ bool build_off(const DevCtl* ctl) {
     const std::uint32_t st = ctl->stopped, ha = ctl->halted, rb = ctl->rebuild_flag;
     return ((st | ha) != 0u) | (rb == 0u);
-}
-
-template <int ND>
-__device__ __forceinline__ void load_pos(const double* __restrict__ pos, std::uint64_t i,
-                                         double* x, double& D0) {
-    constexpr int P = pos_stride(ND);
-    const double2* p2 = reinterpret_cast<const double2*>(pos + i * P);
-#pragma unroll
-    for (int h = 0; h < P / 2; ++h) {
-        const double2 w = p2[h];
-        if (2 * h < ND) x[2 * h] = w.x;
-        else if (2 * h == ND) D0 = w.x;
-        if (2 * h + 1 < ND) x[2 * h + 1] = w.y;
-        else if (2 * h + 1 == ND) D0 = w.y;
-    }
-}
-
-template <int ND>
-__device__ __forceinline__ void store_pos(double* __restrict__ pos, std::uint64_t i,
-                                          const double* x, double D0) {
-    constexpr int P = pos_stride(ND);
-    double2* p2 = reinterpret_cast<double2*>(pos + i * P);
-#pragma unroll
-    for (int h = 0; h < P / 2; ++h) {
-        double2 w;
-        w.x = (2 * h < ND) ? x[2 * h] : ((2 * h == ND) ? D0 : 0.0);
-        w.y = (2 * h + 1 < ND) ? x[2 * h + 1] : ((2 * h + 1 == ND) ? D0 : 0.0);
-        p2[h] = w;
-    }
-}
-
-// Cell coordinate of one axis; the grid cell is at least as wide as the
-// largest pair cutoff, so partners sit in the 3^ndim neighbourhood.
-__device__ __forceinline__ int cell_coord(double x, double scale, int nc) {
-    double s = x * scale;
-    if (!(s > 0.0)) return 0;  // negative, zero or NaN
-    int c = static_cast<int>(s);
-    return c >= nc ? nc - 1 : c;
-}
-
-// ---- deterministic reductions of ForceSums ---------------------------------
-__device__ __forceinline__ double shfl_down_d(double v, int o) {
-    return __shfl_down_sync(0xffffffffu, v, o);
-}
-
-__device__ __forceinline__ void warp_reduce_sums(ForceSums& s) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s.pair_U = xadd(s.pair_U, shfl_down_d(s.pair_U, o));
-        s.pair_Lc = xadd(s.pair_Lc, shfl_down_d(s.pair_Lc, o));
-        s.pair_dk = xadd(s.pair_dk, shfl_down_d(s.pair_dk, o));
-        s.pair_Fm = xadd(s.pair_Fm, shfl_down_d(s.pair_Fm, o));
-        s.pair_maxov = fmax(s.pair_maxov, shfl_down_d(s.pair_maxov, o));
-        s.wall_U = xadd(s.wall_U, shfl_down_d(s.wall_U, o));
-        s.wall_dk = xadd(s.wall_dk, shfl_down_d(s.wall_dk, o));
-        s.wall_Fm = xadd(s.wall_Fm, shfl_down_d(s.wall_Fm, o));
-        s.sum_mag = xadd(s.sum_mag, shfl_down_d(s.sum_mag, o));
-        s.sum_D = xadd(s.sum_D, shfl_down_d(s.sum_D, o));
-        s.pair_count += __shfl_down_sync(0xffffffffu, s.pair_count, o);
-        s.wall_count += __shfl_down_sync(0xffffffffu, s.wall_count, o);
-        s.mag_count += __shfl_down_sync(0xffffffffu, s.mag_count, o);
-    }
-}
-
-__device__ __forceinline__ void sums_add(ForceSums& a, const ForceSums& b) {
-    a.pair_U = xadd(a.pair_U, b.pair_U);
-    a.pair_Lc = xadd(a.pair_Lc, b.pair_Lc);
-    a.pair_dk = xadd(a.pair_dk, b.pair_dk);
-    a.pair_Fm = xadd(a.pair_Fm, b.pair_Fm);
-    a.pair_maxov = fmax(a.pair_maxov, b.pair_maxov);
-    a.wall_U = xadd(a.wall_U, b.wall_U);
-    a.wall_dk = xadd(a.wall_dk, b.wall_dk);
-    a.wall_Fm = xadd(a.wall_Fm, b.wall_Fm);
-    a.sum_mag = xadd(a.sum_mag, b.sum_mag);
-    a.sum_D = xadd(a.sum_D, b.sum_D);
-    a.pair_count += b.pair_count;
-    a.wall_count += b.wall_count;
-    a.mag_count += b.mag_count;
-}
-
-// Deterministic block reduction (fixed shuffle tree, warps combined in order).
-template <int NT>
-__device__ __forceinline__ void block_reduce_sums(ForceSums& s, ForceSums* smem) {
-    warp_reduce_sums(s);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) smem[warp] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ForceSums t = smem[0];
-#pragma unroll
-        for (int w = 1; w < NT / 32; ++w) sums_add(t, smem[w]);
-        s = t;
-    }
 }
 
 // ===========================================================================
@@ -271,34 +179,6 @@ __global__ void __launch_bounds__(256) k_build_bin(DevArrays a) {
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
-
-template <typename T>
-__device__ __forceinline__ T block_exclusive_scan(T v, T* smem, T& total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    T s = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const T y = __shfl_up_sync(0xffffffffu, s, o);
-        if (lane >= o) s += y;
-    }
-    if (lane == 31) smem[warp] = s;
-    __syncthreads();
-    if (warp == 0) {
-        const int nw = blockDim.x >> 5;
-        T w = lane < nw ? smem[lane] : T(0);
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const T y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        if (lane < nw) smem[lane] = w;
-    }
-    __syncthreads();
-    const T warp_off = warp ? smem[warp - 1] : T(0);
-    total = smem[(blockDim.x >> 5) - 1];
-    __syncthreads();
-    return warp_off + s - v;
-}
 
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_tiles(const std::uint32_t* in, std::uint32_t* out, std::uint32_t n,
@@ -1319,28 +1199,6 @@ __global__ void __launch_bounds__(kCtlThreads) k_reduce_fast(DevArrays a) {
     ForceSums s;
     reduce_blocks(a, red, s);
     if (threadIdx.x == 0) ctl->sums = s;
-}
-
-// Parameters of the kernels of the step that begin_step() just opened.
-__device__ void publish_step(DevCtl* ctl, const Controller& c, int ndim) {
-    ctl->forces_done = 0u;
-    for (int d = 0; d < ndim; ++d) {
-        ctl->g.box[d] = c.box[d];
-        ctl->g.inv_box[d] = 1.0 / c.box[d];
-    }
-    ctl->refresh_kappa = c.kappa_D;
-    ctl->force_kappa = c.kappa_D;
-    ctl->force_mu = c.mu_eff;
-    ctl->build_kappa = c.kappa_D;
-    ctl->build_t_shell = c.t_shell;
-    ctl->build_Dmax = c.Dmax_cur;
-    ctl->theta = c.theta;
-    if (c.rebuild_mode == REBUILD_FULL) {
-        ctl->rebuild_flag = 1u;
-    } else {
-        ctl->rebuild_flag = 0u;
-        ctl->kappa_min = fmin(ctl->kappa_min, c.kappa_D);
-    }
 }
 
 // Graph-mode controller: reduce, finish step s (end_step), open step s+1

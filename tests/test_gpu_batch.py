@@ -71,3 +71,58 @@ def test_batch_reports_the_failing_packing(cuda_device, golden):
     bad_cfg = dict(bad_cfg, box=[1.0, 1.0, 1.0])  # box length != ndim: the reference's error
     with pytest.raises((ValueError, RuntimeError), match="packing 1"):
         rb.run_packing_batch([good, (bad_inp, bad_cfg), good], {"max_steps": 50}, concurrency=2)
+
+
+# ---- persistent batch engine (concurrency=0): one thread block per packing ----
+
+def cfg1_item(seed, precision="f64"):
+    import rcpgenerator_b200 as rb
+    init = rb.initialize_particles({"phi": 0.08, "N": 2000, "Ndim": 3, "box": [1.0, 1.0, 1.0],
+                                    "walls": [0, 0, 0], "dist": {"type": "mono", "d": 1.0},
+                                    "seed": seed})
+    return ({"positions": np.asarray(init["positions"]), "diameters": np.asarray(init["diameters"])},
+            {"box": init["box"], "walls": init["walls"], "neighbor_max": 0, "seed": seed,
+             "pair_precision": precision})
+
+
+def test_persistent_batch_is_deterministic_and_independent_of_its_batch(cuda_device, golden):
+    """A packing is run by one thread block from start to end, so its result
+    does not depend on the other packings of the launch or on the run."""
+    import rcpgenerator_b200 as rb
+    g = golden("packs.npz")
+    items = [item(g, c, "graph") for c in ("n16_2d", "n200_2d_disk_2500", "n64_2d_walls_500")]
+    opts = {"max_steps": 2500}
+    a = rb.run_packing_batch(items, opts)
+    b = rb.run_packing_batch(items[::-1], opts)[::-1]
+    alone = rb.run_packing_batch(items[1:2], opts)[0]
+    for ra, rb_ in zip(a, b):
+        assert ra["steps"] == rb_["steps"]
+        assert np.array_equal(ra["positions"], rb_["positions"])
+        assert np.array_equal(ra["phi_history"], rb_["phi_history"])
+    assert np.array_equal(a[1]["positions"], alone["positions"])
+
+
+def test_persistent_batch_mixed_ndim_converges(cuda_device, golden):
+    import rcpgenerator_b200 as rb
+    g = golden("packs.npz")
+    cases = ["n16_2d", "n64_3d_bi", "n300_4d_1500", "n128_3d_sphere_3000"]
+    out = rb.run_packing_batch([item(g, c, "graph") for c in cases], {})
+    for c, r in zip(cases, out):
+        assert np.isfinite(r["positions"]).all(), c
+        assert len(r["phi_history"]) == r["steps"]
+        assert r["max_min_dist"] < 5e-4 or r["steps"] >= 60000, c
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_persistent_batch_config1_phiJ_distribution_64_seeds(cuda_device, golden, precision):
+    """BASELINE config 1 over 64 seeds in one persistent launch against the
+    reference's distribution on the same seeds: |mean phi_J - reference| <= 1e-3,
+    mean step count within 5 %, every packing under the reference's gate."""
+    import rcpgenerator_b200 as rb
+    g = golden("cfg1_seeds.npz")
+    out = rb.run_packing_batch([cfg1_item(int(s), precision) for s in g["seed"].tolist()], {})
+    phis = np.asarray([r["phi"] for r in out])
+    steps = np.asarray([r["steps"] for r in out])
+    assert abs(phis.mean() - g["phi"].mean()) <= 1e-3
+    assert abs(steps.mean() - g["steps"].mean()) <= 0.05 * g["steps"].mean()
+    assert (np.asarray([r["max_min_dist"] for r in out]) < 5e-4).all()
