@@ -249,7 +249,8 @@ def run_batch_workload(args) -> int:
         "data": "synthetic",
         "config": {"workload": f"batch{len(items)}_N64-16384_ndim234_phi0.10", "packings": len(items),
                    "concurrency": args.concurrency,
-                   "engine": "persistent batch kernel" if args.concurrency <= 0 else "graph engines on streams",
+                   "engine": {0: "persistent batch kernel for the small packings + engines on 32 streams"}.get(
+                       args.concurrency, "persistent batch kernel" if args.concurrency < 0 else "graph engines on streams"),
                    "pair_precision": args.pair_precision, "particle_steps": ps,
                    "mean_steps": float(np.mean(steps)), "parallelism": f"replicas{world}",
                    "timing": "host wall clock around run_packing_batch (inputs on the host, results back)"},
@@ -309,7 +310,7 @@ def main() -> int:
     ap.add_argument("--batch-count", type=int, default=128)
     ap.add_argument("--batch-single", type=int, default=8, help="packings timed one at a time")
     ap.add_argument("--concurrency", type=int, default=0,
-                    help="0: persistent batch engine (one launch, a thread block per packing); k: k engines on streams")
+                    help="-1: persistent batch kernel; 0: persistent for small packings + 32 streams; k: k streams")
     ap.add_argument("--cpu-cap-steps", type=int, default=300)
     args = ap.parse_args()
     WORKLOAD["N"] = args.n

@@ -156,12 +156,16 @@ void rcpg_result_free(rcpg_result* r);
 /* Many independent packings (the reference's throughput pattern: one process
  * per core, rcptools/jobs.py:392-401, each calling run_packing), all with the
  * run options `opt` (graph engine).
- *   concurrency <= 0: the persistent batch engine -- one kernel per ndim in
+ *   concurrency < 0: the persistent batch engine -- one kernel per ndim in
  *     which every thread block runs whole packings taken from a queue (no
- *     kernel launch per step); packings that can reach a target-phi lock, and
- *     exact runs, are refused with RCPG_EINVAL.
+ *     kernel launch per step).
+ *   concurrency = 0: the persistent engine for the cheap packings (N x 3^ndim
+ *     up to 3e4) and 32 ordinary engines on CUDA streams for the others, at the
+ *     same time.
  *   concurrency > 0: that many host threads each drive one ordinary engine at
  *     a time on their own CUDA stream of device opt->device.
+ * Exact runs and runs that can reach a target-phi lock always take the stream
+ * path.
  * results[k] receives packing k's result (free each with rcpg_result_free) or
  * NULL, and status[k] its RCPG_* code. Returns RCPG_OK when every packing
  * succeeded, else the first failing code, with that packing's index and

@@ -297,12 +297,13 @@ def run_packing_batch(items: list, options: dict | None = None, concurrency: int
     """Many independent packings, ``items`` = [(input, config), ...] as for
     run_packing; the run options (``options`` plus the engine keys ``engine``,
     ``pair_precision``, ``device``, ... of the first config) are shared.
-    ``concurrency`` 0 runs them in the persistent batch engine (one launch per
-    ndim, each thread block running whole packings); ``concurrency`` k > 0 runs
-    k ordinary engines at a time on their own CUDA streams (the reference runs
-    one process per core, rcptools/jobs.py:392-401). Returns the result dicts
-    in input order; a failed packing raises after all have run, naming its
-    index."""
+    ``concurrency`` < 0 runs them in the persistent batch engine (one launch
+    per ndim, each thread block running whole packings); 0 sends the cheap
+    ones there and the others to 32 ordinary engines on CUDA streams at the
+    same time; k > 0 runs k ordinary engines at a time on their own streams
+    (the reference runs one process per core, rcptools/jobs.py:392-401).
+    Returns the result dicts in input order; a failed packing raises after all
+    have run, naming its index."""
     items = list(items)
     if not items:
         return []

@@ -31,9 +31,8 @@ namespace rcpg {
 
 namespace {
 
-constexpr int kBT = 256;            // threads per block
+constexpr int kBT = 256;            // threads per block (one per digit of the reorder's radix sort)
 constexpr int kBW = kBT / 32;       // warps per block
-constexpr int kBRow = 256;          // row entries sorted in shared memory per warp
 
 // One instance's arrays (pointers already offset to the instance).
 struct View {
@@ -92,8 +91,6 @@ struct Shared {
     ForceSums red[kBW];
     std::uint32_t wsum[kBW];
     unsigned long long wsum64[kBW];
-    std::uint32_t row[kBW][kBRow];
-    std::uint32_t cnt[kBW];
     std::uint32_t hist[256];
     std::uint32_t base[256];
     std::uint32_t wcnt[kBW][256];
@@ -245,8 +242,9 @@ __device__ void b_build(const View& V, Shared& sh) {
         }
     }
     __syncthreads();
-    // warp search: one warp per row slot (as k_build_search)
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    // search: one thread per row slot, partners in the fixed scan order (cells
+    // of the 3^ndim neighbourhood in odometer order, members ascending), so the
+    // rows are deterministic without a sort
     const std::uint32_t S = V.S;
     const Geometry& g = ctl->g;
     const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
@@ -260,8 +258,8 @@ __device__ void b_build(const View& V, Shared& sh) {
         nn[d] = nc[d] < 3 ? nc[d] : 3;
         total_combo *= nn[d];
     }
-    std::uint32_t* row = sh.row[w];
-    for (std::uint64_t t = w; t < N; t += kBW) {
+    std::uint32_t need = 0;
+    for (std::uint64_t t = threadIdx.x; t < N; t += kBT) {
         const std::uint32_t i = V.work[t];
         double xi[ND], D0i;
         load_pos<ND>(V.spos, t, xi, D0i);
@@ -269,10 +267,8 @@ __device__ void b_build(const View& V, Shared& sh) {
         int cc[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) cc[d] = cell_coord(xi[d], scale[d], nc[d]);
-        if (lane == 0) sh.cnt[w] = 0u;
-        __syncwarp();
-        std::uint32_t n_half = 0;
-        for (int combo = lane; combo < total_combo; combo += 32) {
+        std::uint32_t n = 0, n_half = 0;
+        for (int combo = 0; combo < total_combo; ++combo) {
             std::uint32_t cell = 0, mul = 1;
             int r = combo;
 #pragma unroll
@@ -288,71 +284,27 @@ __device__ void b_build(const View& V, Shared& sh) {
             const std::uint32_t q0 = V.cell_start[cell], q1 = V.cell_start[cell + 1];
             for (std::uint32_t q = q0; q < q1; ++q) {
                 const std::uint32_t j = V.work[q];
-                if (j == i) continue;
                 double xj[ND], D0j;
                 load_pos<ND>(V.spos, q, xj, D0j);
+                if (j == i) continue;
                 const double Dj = xmul(D0j, kap);
                 const bool ok = (ND <= 3 || j > i) ? in_shell<ND>(xi, xj, Di, Dj, bx, ibx, t_shell)
                                                    : in_shell<ND>(xi, xj, Dj, Di, bx, ibx, t_shell);
                 if (!ok) continue;
-                const std::uint32_t slot = atomicAdd(&sh.cnt[w], 1u);
-                if (slot < static_cast<std::uint32_t>(kBRow)) row[slot] = j;
-                else if (slot < S) V.nbr[static_cast<std::uint64_t>(slot) * N + t] = j;
+                if (n < S) V.nbr[static_cast<std::uint64_t>(n) * N + t] = j;
+                ++n;
                 if (j > i) ++n_half;
             }
         }
-        __syncwarp();
-        const std::uint32_t n = sh.cnt[w];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) n_half += __shfl_xor_sync(0xffffffffu, n_half, o);
-        if (lane == 0) {
-            const std::uint32_t cap = V.caps[i];
-            if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-                ctl->cap_error_particle = i;
-                ctl->cap_error_cap = cap;
-            }
-            atomicMax(&sh.need, n);
-            V.nbr_cnt[t] = n > S ? 0u : n;
+        const std::uint32_t cap = V.caps[i];
+        if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
+            ctl->cap_error_particle = i;
+            ctl->cap_error_cap = cap;
         }
-        if (n <= S) {
-            if (n <= static_cast<std::uint32_t>(kBRow)) {
-                std::uint32_t p2 = 1;
-                while (p2 < n) p2 <<= 1;
-                for (std::uint32_t e = n + lane; e < p2; e += 32) row[e] = 0xffffffffu;
-                __syncwarp();
-                for (std::uint32_t kk = 2; kk <= p2; kk <<= 1) {
-                    for (std::uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
-                        for (std::uint32_t e = lane; e < p2; e += 32) {
-                            const std::uint32_t f = e ^ jj;
-                            if (f > e) {
-                                const std::uint32_t x = row[e], y = row[f];
-                                if ((x > y) == ((e & kk) == 0)) {
-                                    row[e] = y;
-                                    row[f] = x;
-                                }
-                            }
-                        }
-                        __syncwarp();
-                    }
-                }
-                for (std::uint32_t e = lane; e < n; e += 32) V.nbr[static_cast<std::uint64_t>(e) * N + t] = row[e];
-            } else if (lane == 0) {
-                for (std::uint32_t e = 0; e < static_cast<std::uint32_t>(kBRow); ++e)
-                    V.nbr[static_cast<std::uint64_t>(e) * N + t] = row[e];
-                std::uint32_t* gr = V.nbr + t;
-                for (std::uint32_t k = 1; k < n; ++k) {
-                    const std::uint32_t v = gr[static_cast<std::uint64_t>(k) * N];
-                    std::uint32_t p = k;
-                    while (p > 0 && gr[static_cast<std::uint64_t>(p - 1) * N] > v) {
-                        gr[static_cast<std::uint64_t>(p) * N] = gr[static_cast<std::uint64_t>(p - 1) * N];
-                        --p;
-                    }
-                    gr[static_cast<std::uint64_t>(p) * N] = v;
-                }
-            }
-        }
-        __syncwarp();
+        need = need > n ? need : n;
+        V.nbr_cnt[t] = n > S ? 0u : n;
     }
+    atomicMax(&sh.need, need);
     __syncthreads();
     if (threadIdx.x == 0) {
         ctl->row_need = sh.need;
@@ -377,8 +329,9 @@ __device__ ForceSums b_forces(const View& V, Shared& sh, bool mixed) {
     }
     const double kap = ctl->force_kappa;
     const float kapf = static_cast<float>(kap);
-    ForceSums s;
-    sums_zero(s);
+    // the wall terms join the pair chains (the finalisation adds them anyway)
+    double sU = 0.0, sLc = 0.0, sdk = 0.0, sFm = 0.0, smax = 0.0, smag = 0.0, sD = 0.0;
+    std::uint32_t scount = 0, smagc = 0;
     for (std::uint64_t t = threadIdx.x; t < N; t += kBT) {
         const std::uint64_t i = V.work[t];
         double xi[ND], D0i;
@@ -393,11 +346,24 @@ __device__ ForceSums b_forces(const View& V, Shared& sh, bool mixed) {
             fif[d] = 0.0f;
         }
         const std::uint32_t n = min(V.nbr_cnt[t], V.S);
-        for (std::uint32_t k = 0; k < n; ++k) {
-            const std::uint32_t j = V.nbr[static_cast<std::uint64_t>(k) * N + t];
+        // partners in chunks: the ids, then the positions of a chunk are loaded
+        // before its arithmetic (several gathers in flight per thread)
+        constexpr std::uint32_t kC = 2;
+        for (std::uint32_t k0 = 0; k0 < n; k0 += kC) {
+          std::uint32_t jj[kC];
+          double xjc[kC][ND], D0c[kC];
+#pragma unroll
+          for (std::uint32_t u = 0; u < kC; ++u)
+              jj[u] = (k0 + u < n) ? V.nbr[static_cast<std::uint64_t>(k0 + u) * N + t] : 0xffffffffu;
+#pragma unroll
+          for (std::uint32_t u = 0; u < kC; ++u)
+              if (jj[u] < N) load_pos<ND>(V.pos, jj[u], xjc[u], D0c[u]);
+#pragma unroll
+          for (std::uint32_t u = 0; u < kC; ++u) {
+            const std::uint32_t j = jj[u];
             if (j >= N) continue;
-            double xj[ND], D0j;
-            load_pos<ND>(V.pos, j, xj, D0j);
+            const double* xj = xjc[u];
+            const double D0j = D0c[u];
             PairTerms pt;
             if (mixed) {
                 float dxf[ND];
@@ -413,28 +379,40 @@ __device__ ForceSums b_forces(const View& V, Shared& sh, bool mixed) {
                 pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
             }
             if (j > i) {
-                s.pair_U = xadd(s.pair_U, pt.U);
-                s.pair_Lc = xadd(s.pair_Lc, pt.Lc);
-                s.pair_dk = xadd(s.pair_dk, pt.dk);
-                s.pair_Fm = xadd(s.pair_Fm, pt.Fm);
-                s.pair_maxov = fmax(s.pair_maxov, pt.U);
-                s.pair_count += 1ull;
+                sU = xadd(sU, pt.U);
+                sLc = xadd(sLc, pt.Lc);
+                sdk = xadd(sdk, pt.dk);
+                sFm = xadd(sFm, pt.Fm);
+                smax = fmax(smax, pt.U);
+                ++scount;
             }
+          }
         }
         if (mixed) {
 #pragma unroll
             for (int d = 0; d < ND; ++d) fi[d] = static_cast<double>(fif[d]);
         }
-        wall_forces<ND>(xi, Di, g, fi, s.wall_U, s.wall_dk, s.wall_Fm, s.wall_count);
+        wall_forces<ND>(xi, Di, g, fi, sU, sdk, sFm, scount);
         const double f2 = force_norm2<ND>(fi);
         if (f2 > 1.0E-16) {
-            s.sum_mag = xadd(s.sum_mag, xsqrt(f2));
-            s.mag_count += 1ull;
+            smag = xadd(smag, xsqrt(f2));
+            ++smagc;
         }
-        s.sum_D = xadd(s.sum_D, Di);
+        sD = xadd(sD, Di);
 #pragma unroll
         for (int d = 0; d < ND; ++d) V.F[i * ND + d] = fi[d];
     }
+    ForceSums s;
+    sums_zero(s);
+    s.pair_U = sU;
+    s.pair_Lc = sLc;
+    s.pair_dk = sdk;
+    s.pair_Fm = sFm;
+    s.pair_maxov = smax;
+    s.pair_count = scount;
+    s.sum_mag = smag;
+    s.mag_count = smagc;
+    s.sum_D = sD;
     block_reduce_sums<kBT>(s, sh.red);
     __syncthreads();
     if (threadIdx.x == 0) sh.red[0] = s;
@@ -743,7 +721,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(BatchArrays B, std::uint32_t c
 }  // namespace
 
 void launch_batch(const BatchArrays& B, int ndim, std::uint32_t chunk, int mixed, int device,
-                  cudaStream_t st) {
+                  int blocks_per_sm, cudaStream_t st) {
     const std::size_t smem = sizeof(Shared);
     int sms = 148, per = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -752,6 +730,7 @@ void launch_batch(const BatchArrays& B, int ndim, std::uint32_t chunk, int mixed
     case D: {                                                                                       \
         cudaFuncSetAttribute(k_batch<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)); \
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch<D>, kBT, smem);                 \
+        if (per > blocks_per_sm) per = blocks_per_sm;                                               \
         const unsigned grid = static_cast<unsigned>(sms * (per > 0 ? per : 1));                     \
         k_batch<D><<<grid, kBT, smem, st>>>(B, chunk, mixed);                                       \
     } break;
@@ -816,7 +795,8 @@ void ck(cudaError_t e, const char* what) {
 // final status of each.
 std::vector<std::uint32_t> run_group(const std::vector<EngineInput>& ins, const std::vector<RunSetup>& su,
                                      const std::vector<std::size_t>& idx, std::uint32_t mult,
-                                     std::uint32_t chunk, cudaStream_t st, std::vector<BatchOutcome>& out) {
+                                     std::uint32_t chunk, int blocks_per_sm, cudaStream_t st,
+                                     std::vector<BatchOutcome>& out) {
     const int nd = su[idx[0]].ndim;
     const int P = pos_stride(nd);
     const std::size_t K = idx.size();
@@ -942,7 +922,7 @@ std::vector<std::uint32_t> run_group(const std::vector<EngineInput>& ins, const 
         ck(cudaMemcpyAsync(B.active, active.data(), active.size() * 4, cudaMemcpyHostToDevice, st), "H2D active");
         ck(cudaMemsetAsync(B.queue, 0, 4, st), "memset");
         B.nactive = static_cast<std::uint32_t>(active.size());
-        launch_batch(B, nd, chunk, mixed ? 1 : 0, device, st);
+        launch_batch(B, nd, chunk, mixed ? 1 : 0, device, blocks_per_sm, st);
         ck(cudaGetLastError(), "batch launch");
         ck(cudaMemcpyAsync(now.data(), B.inst, K * sizeof(BatchInst), cudaMemcpyDeviceToHost, st), "D2H inst");
         ck(cudaStreamSynchronize(st), "batch kernel");
@@ -1007,7 +987,8 @@ std::vector<std::uint32_t> run_group(const std::vector<EngineInput>& ins, const 
 
 }  // namespace
 
-std::vector<BatchOutcome> run_batch_persistent(const std::vector<EngineInput>& ins, std::uint32_t chunk) {
+std::vector<BatchOutcome> run_batch_persistent(const std::vector<EngineInput>& ins, std::uint32_t chunk,
+                                               int blocks_per_sm) {
     std::vector<BatchOutcome> out(ins.size());
     if (ins.empty()) return out;
     std::vector<RunSetup> su(ins.size());
@@ -1039,7 +1020,7 @@ std::vector<BatchOutcome> run_batch_persistent(const std::vector<EngineInput>& i
                 for (std::size_t k : pending)
                     if (su[k].ndim == nd) grp.push_back(k);
                 if (grp.empty()) continue;
-                const std::vector<std::uint32_t> st_k = run_group(ins, su, grp, mult, chunk, st, out);
+                const std::vector<std::uint32_t> st_k = run_group(ins, su, grp, mult, chunk, blocks_per_sm, st, out);
                 for (std::size_t q = 0; q < grp.size(); ++q) {
                     const std::size_t k = grp[q];
                     if (st_k[q] == 2u) continue;

@@ -42,7 +42,7 @@ struct BatchArrays {
 };
 
 void launch_batch(const BatchArrays& B, int ndim, std::uint32_t chunk, int mixed, int device,
-                  cudaStream_t st);
+                  int blocks_per_sm, cudaStream_t st);
 
 // Outcome of one packing of run_batch_persistent.
 struct BatchOutcome {
@@ -54,8 +54,19 @@ struct BatchOutcome {
 };
 
 // Runs every packing to completion in persistent launches of at most `chunk`
-// steps per packing. All share the run options of `ins[k]` (graph engine;
-// packings that can reach a target-phi lock are reported as unsupported).
-std::vector<BatchOutcome> run_batch_persistent(const std::vector<EngineInput>& ins, std::uint32_t chunk);
+// steps per packing, with at most `blocks_per_sm` resident blocks per SM. All
+// share the run options of `ins[k]` (graph engine; packings that can reach a
+// target-phi lock are reported as unsupported).
+std::vector<BatchOutcome> run_batch_persistent(const std::vector<EngineInput>& ins, std::uint32_t chunk,
+                                               int blocks_per_sm);
+
+// Work of one build step of a packing in the persistent kernel, in candidate
+// tests (N x 3^ndim x members per cell): the batch sends the packings above a
+// budget to engines on streams, which spread one packing over the GPU.
+inline double batch_cost(std::uint64_t N, int ndim) {
+    double c = static_cast<double>(N);
+    for (int d = 0; d < ndim; ++d) c *= 3.0;
+    return c;
+}
 
 }  // namespace rcpg

@@ -263,37 +263,6 @@ int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const r
     rcpg_run_options o;
     if (opt) o = *opt;
     else rcpg_default_options(&o);
-    if (concurrency <= 0) {
-        // one persistent launch per ndim: each thread block runs whole packings
-        try {
-            std::vector<rcpg::EngineInput> ins;
-            ins.reserve(count);
-            for (uint64_t k = 0; k < count; ++k) ins.push_back(make_input(&inputs[k], &o));
-            const std::vector<rcpg::BatchOutcome> res = rcpg::run_batch_persistent(ins, 2048u);
-            int32_t first = RCPG_OK;
-            std::string msg;
-            for (uint64_t k = 0; k < count; ++k) {
-                const rcpg::BatchOutcome& b = res[k];
-                int32_t code = RCPG_OK;
-                if (b.code == -22) code = RCPG_EINVAL;
-                else if (b.code == -2) code = RCPG_ECUDA;
-                else if (b.code != 0) code = RCPG_ERUNTIME;
-                if (status) status[k] = code;
-                if (code == RCPG_OK) {
-                    results[k] = make_result(b.result, b.N, b.ndim, nullptr, false, 0);
-                } else if (first == RCPG_OK) {
-                    first = code;
-                    msg = "packing " + std::to_string(k) + ": " + b.message;
-                }
-            }
-            if (first != RCPG_OK) return fail(err, errlen, first, msg);
-            return RCPG_OK;
-        } catch (const std::exception& e) {
-            return fail(err, errlen, classify(e), e.what());
-        }
-    }
-    const uint64_t nthreads = std::max<uint64_t>(1, std::min<uint64_t>(count, static_cast<uint64_t>(concurrency)));
-    std::atomic<uint64_t> next{0};
     std::mutex mu;
     int32_t first_code = RCPG_OK;
     uint64_t first_index = 0;
@@ -307,19 +276,60 @@ int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const r
             first_msg = msg;
         }
     };
+    // concurrency 0: the cheap packings (graph engine, no target-phi lock, a
+    // build step below kPersistentBudget candidate tests) go to the persistent
+    // kernel, which runs on its own host thread with one block per SM, the
+    // others to 32 engines on streams at the same time; concurrency < 0: every
+    // eligible packing to the persistent kernel
+    constexpr double kPersistentBudget = 3e4;
+    std::vector<uint64_t> on_streams, persistent;
+    for (uint64_t k = 0; k < count; ++k) {
+        const bool eligible = concurrency <= 0 && !o.exact && !o.has_target_phi;
+        const bool ok = eligible && (concurrency < 0 ||
+                                     rcpg::batch_cost(inputs[k].N, inputs[k].ndim) <= kPersistentBudget);
+        (ok ? persistent : on_streams).push_back(k);
+    }
+    std::thread pthread;
+    if (!persistent.empty()) {
+        pthread = std::thread([&]() {
+            try {
+                std::vector<rcpg::EngineInput> ins;
+                ins.reserve(persistent.size());
+                for (uint64_t k : persistent) ins.push_back(make_input(&inputs[k], &o));
+                const std::vector<rcpg::BatchOutcome> res =
+                    rcpg::run_batch_persistent(ins, 2048u, on_streams.empty() ? 2 : 1);
+                for (std::size_t q = 0; q < persistent.size(); ++q) {
+                    const uint64_t k = persistent[q];
+                    const rcpg::BatchOutcome& b = res[q];
+                    if (b.code == 0) {
+                        results[k] = make_result(b.result, b.N, b.ndim, nullptr, false, 0);
+                    } else {
+                        record(k, b.code == -22 ? RCPG_EINVAL : (b.code == -2 ? RCPG_ECUDA : RCPG_ERUNTIME),
+                               b.message);
+                    }
+                }
+            } catch (const std::exception& e) {
+                for (uint64_t k : persistent) record(k, classify(e), e.what());
+            }
+        });
+    }
+    const uint64_t ns = on_streams.size();
+    const uint64_t nthreads = ns ? std::max<uint64_t>(1, std::min<uint64_t>(ns, concurrency > 0 ? concurrency : 32)) : 0;
+    std::atomic<uint64_t> next{0};
     auto worker = [&]() {
         if (cudaSetDevice(o.device) != cudaSuccess) {
             cudaGetLastError();
-            for (uint64_t k; (k = next.fetch_add(1)) < count;) record(k, RCPG_ECUDA, "rcpgenerator_b200: cudaSetDevice failed");
+            for (uint64_t q; (q = next.fetch_add(1)) < ns;) record(on_streams[q], RCPG_ECUDA, "rcpgenerator_b200: cudaSetDevice failed");
             return;
         }
         cudaStream_t st = nullptr;
         if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
             cudaGetLastError();
-            for (uint64_t k; (k = next.fetch_add(1)) < count;) record(k, RCPG_ECUDA, "rcpgenerator_b200: cudaStreamCreate failed");
+            for (uint64_t q; (q = next.fetch_add(1)) < ns;) record(on_streams[q], RCPG_ECUDA, "rcpgenerator_b200: cudaStreamCreate failed");
             return;
         }
-        for (uint64_t k; (k = next.fetch_add(1)) < count;) {
+        for (uint64_t q; (q = next.fetch_add(1)) < ns;) {
+            const uint64_t k = on_streams[q];
             try {
                 rcpg::Engine eng(make_input(&inputs[k], &o), st);
                 eng.run(0, false, 0, rcpg::ObserverFn(), nullptr);
@@ -336,6 +346,7 @@ int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const r
     pool.reserve(nthreads);
     for (uint64_t t = 0; t < nthreads; ++t) pool.emplace_back(worker);
     for (auto& t : pool) t.join();
+    if (pthread.joinable()) pthread.join();
     if (first_code != RCPG_OK)
         return fail(err, errlen, first_code, "packing " + std::to_string(first_index) + ": " + first_msg);
     return RCPG_OK;

@@ -1598,7 +1598,7 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     scan_exclusive(a.cell_count, a.cell_start, a.C_alloc + 1, a.scan_tmp, a.ctl, st);
     k_build_scatter<<<nb, kForceBlock, 0, st>>>(a);
     k_build_cell_sort<ND><<<(a.C_alloc + 255) / 256, 256, 0, st>>>(a);
-    if (ND <= 3) {
+    if (ND <= 3 && a.N >= kTiledMinN) {  // smaller packings never take the tiled path
         if (a.sorted_rows) launch_tiled<ND, true>(a, st);
         else launch_tiled<ND, false>(a, st);
     }

@@ -63,6 +63,21 @@ def test_graph_batch_equals_single_runs(cuda_device, golden):
             assert np.array_equal(r["phi_history"], alone["phi_history"])
 
 
+def test_hybrid_batch_matches_its_parts(cuda_device, golden):
+    """concurrency=0 sends each packing to the persistent kernel or to an engine
+    on a stream by its size; either way a packing's result equals the one of
+    that path run alone."""
+    import rcpgenerator_b200 as rb
+    g = golden("packs.npz")
+    items = [item(g, c, "graph") for c in ("n16_2d", "n64_3d_bi", "cfg1_n2000_3d")]
+    opts = {"max_steps": 1200}
+    mixed = rb.run_packing_batch(items, opts, concurrency=0)
+    small = rb.run_packing_batch(items[:2], opts, concurrency=-1)
+    large = rb.run_packing_batch(items[2:], opts, concurrency=1)
+    for r, ref in zip(mixed, small + large):
+        assert np.array_equal(r["positions"], ref["positions"])
+
+
 def test_batch_reports_the_failing_packing(cuda_device, golden):
     import rcpgenerator_b200 as rb
     g = golden("packs.npz")
@@ -73,7 +88,7 @@ def test_batch_reports_the_failing_packing(cuda_device, golden):
         rb.run_packing_batch([good, (bad_inp, bad_cfg), good], {"max_steps": 50}, concurrency=2)
 
 
-# ---- persistent batch engine (concurrency=0): one thread block per packing ----
+# ---- persistent batch engine (concurrency=-1): one thread block per packing ----
 
 def cfg1_item(seed, precision="f64"):
     import rcpgenerator_b200 as rb
@@ -92,9 +107,9 @@ def test_persistent_batch_is_deterministic_and_independent_of_its_batch(cuda_dev
     g = golden("packs.npz")
     items = [item(g, c, "graph") for c in ("n16_2d", "n200_2d_disk_2500", "n64_2d_walls_500")]
     opts = {"max_steps": 2500}
-    a = rb.run_packing_batch(items, opts)
-    b = rb.run_packing_batch(items[::-1], opts)[::-1]
-    alone = rb.run_packing_batch(items[1:2], opts)[0]
+    a = rb.run_packing_batch(items, opts, concurrency=-1)
+    b = rb.run_packing_batch(items[::-1], opts, concurrency=-1)[::-1]
+    alone = rb.run_packing_batch(items[1:2], opts, concurrency=-1)[0]
     for ra, rb_ in zip(a, b):
         assert ra["steps"] == rb_["steps"]
         assert np.array_equal(ra["positions"], rb_["positions"])
@@ -106,7 +121,7 @@ def test_persistent_batch_mixed_ndim_converges(cuda_device, golden):
     import rcpgenerator_b200 as rb
     g = golden("packs.npz")
     cases = ["n16_2d", "n64_3d_bi", "n300_4d_1500", "n128_3d_sphere_3000"]
-    out = rb.run_packing_batch([item(g, c, "graph") for c in cases], {})
+    out = rb.run_packing_batch([item(g, c, "graph") for c in cases], {}, concurrency=-1)
     for c, r in zip(cases, out):
         assert np.isfinite(r["positions"]).all(), c
         assert len(r["phi_history"]) == r["steps"]
@@ -120,7 +135,8 @@ def test_persistent_batch_config1_phiJ_distribution_64_seeds(cuda_device, golden
     mean step count within 5 %, every packing under the reference's gate."""
     import rcpgenerator_b200 as rb
     g = golden("cfg1_seeds.npz")
-    out = rb.run_packing_batch([cfg1_item(int(s), precision) for s in g["seed"].tolist()], {})
+    out = rb.run_packing_batch([cfg1_item(int(s), precision) for s in g["seed"].tolist()], {},
+                               concurrency=-1)
     phis = np.asarray([r["phi"] for r in out])
     steps = np.asarray([r["steps"] for r in out])
     assert abs(phis.mean() - g["phi"].mean()) <= 1e-3
