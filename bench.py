@@ -37,6 +37,10 @@ UNIT = "ADAM steps/s"
 WORKLOAD = dict(phi=0.30, N=1_000_000, Ndim=2, box=[1.0, 1.0], walls=[0, 0],
                 dist={"type": "bidisperse", "d1": 1.0, "d2": 1.4, "p": 0.5}, seed=123)
 PEAKS = REPO / "MEASURED_PEAKS.json"
+# DRAM bytes (read + write) per algorithmic byte of k_forces from one ncu capture
+# (profiles/k_forces_bidisperse2d_n3e5_mixed.md: 24.2 MB for 20.1 MB at N = 300k);
+# the N = 1M launch is too large to capture with the full metric set
+FORCES_TRAFFIC_PER_ALG_BYTE = 24.2 / 20.1
 
 
 def workload_name(n: int) -> str:
@@ -407,7 +411,9 @@ def main() -> int:
                    "row_capacity": int(res["engine_stats"]["row_capacity"])},
         "roofline": {"bound": "hbm", "kernel": "k_forces (pair energy/gradient, full rows)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None,
+                     "peak_kind": peak_kind,
+                     "traffic": prof["alg_bytes"] * FORCES_TRAFFIC_PER_ALG_BYTE,
+                     "traffic_note": "ncu DRAM bytes per algorithmic byte at N=300k (profiles/), scaled",
                      "alg_bytes_per_launch": prof["alg_bytes"], "avg_launch_ms": prof["avg_ms"],
                      "mean_row": prof["mean_row"]},
         "cpu_baseline": cpu,
