@@ -10,6 +10,8 @@
 
 namespace rcpg {
 
+constexpr int kMaxClass = 8;
+
 // Scalars the particle kernels read, plus status words they write. Lives in
 // device memory; in exact (host-controlled) mode the host rewrites it every
 // step, in graph mode the controller kernel does.
@@ -32,10 +34,19 @@ struct DevCtl {
     double theta;          // budget
     double force_kappa;    // D = D0 * force_kappa in the forces
     double force_mu;       // mu fed to the forces
-    // cell grid of the current build
+    // cell grid of the current build (one grid, or class 0's of several)
     int ncell[kMaxDim];
     double cell_scale[kMaxDim];
-    std::uint32_t ncells;
+    std::uint32_t ncells;         // cells of all grids
+    // Size classes (wide size distributions): class k holds the particles with
+    // D0 in [class_d0[k], class_d0[k+1]) and has its own grid, as wide as the
+    // pair cutoff of its largest member (class_d0max[k]); nclass <= 1: one grid
+    int nclass;
+    double class_d0[kMaxClass + 1];
+    double class_d0max[kMaxClass];
+    int cls_ncell[kMaxClass][kMaxDim];
+    double cls_scale[kMaxClass][kMaxDim];
+    std::uint32_t cls_base[kMaxClass + 1];  // first cell of class k
     // control words
     std::uint32_t rebuild_flag;   // rebuild the pair list before the forces
     std::uint32_t adam_go;        // ADAM pass of the finished step is pending

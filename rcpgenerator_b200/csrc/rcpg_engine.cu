@@ -53,6 +53,32 @@ void pinned_ctl_release(DevCtl* p) {
     g_pinned_free.push_back(p);
 }
 
+// Size classes of the cell grids for a wide size distribution: class k holds
+// D0 in [D0min*2^k, D0min*2^(k+1)) (the last class is unbounded); each class's
+// grid is as wide as the cutoff of its largest member, so a small particle
+// does not scan cells sized for the largest one. One class when
+// D0max/D0min <= kClassRatio.
+static void set_size_classes(const std::vector<double>& D0, DevCtl& h) {
+    constexpr double kClassRatio = 2.5;
+    double lo = D0.empty() ? 1.0 : D0[0], hi = lo;
+    for (double v : D0) {
+        lo = std::min(lo, v);
+        hi = std::max(hi, v);
+    }
+    int K = 1;
+    if (lo > 0.0 && hi / lo > kClassRatio) K = std::min(kMaxClass, static_cast<int>(std::ceil(std::log2(hi / lo))));
+    h.nclass = K;
+    for (int k = 0; k <= K; ++k) h.class_d0[k] = (k == 0) ? 0.0 : (k == K ? HUGE_VAL : lo * std::ldexp(1.0, k));
+    for (int k = 0; k < K; ++k) h.class_d0max[k] = 0.0;
+    for (double v : D0) {
+        int k = 0;
+        while (k + 1 < K && v >= h.class_d0[k + 1]) ++k;
+        h.class_d0max[k] = std::max(h.class_d0max[k], v);
+    }
+    for (int k = 0; k < K; ++k)
+        if (h.class_d0max[k] <= 0.0) h.class_d0max[k] = k + 1 < K ? h.class_d0[k + 1] : hi;
+}
+
 void Engine::check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) {
         throw EngineError(-2, std::string("rcpgenerator_b200: CUDA error in ") + what + ": " +
@@ -116,11 +142,18 @@ void Engine::alloc_device() {
     // exact mode sums each row in ascending partner order, as the reference
     a_.sorted_rows = exact_ ? 1 : 0;
     a_.mixed = mixed_ ? 1 : 0;
-    // cell grid capacity: the grid at the initial (smallest) cutoff
+    // cell grid capacity: the grids at the initial (smallest) cutoffs
     {
-        const double cutoff = (host_c_.Dmax_cur + host_c_.t_shell) * (1.0 + 1e-6);
-        double cells = 1.0;
-        for (int d = 0; d < nd; ++d) cells *= std::max(1.0, std::floor(host_c_.box[d] / cutoff));
+        DevCtl cls{};
+        set_size_classes(D0_, cls);
+        double cells = 0.0;
+        for (int k = 0; k < cls.nclass; ++k) {
+            const double dmax = cls.nclass > 1 ? cls.class_d0max[k] : host_c_.Dmax_cur;
+            const double cutoff = (dmax + host_c_.t_shell) * (1.0 + 1e-6);
+            double ck = 1.0;
+            for (int d = 0; d < nd; ++d) ck *= std::max(1.0, std::floor(host_c_.box[d] / cutoff));
+            cells += ck;
+        }
         double cap = std::min(cells * 1.5 + 64.0, 8.0 * static_cast<double>(N) + 1024.0);
         cap = std::min(cap, 2.0e9);
         a_.C_alloc = static_cast<std::uint32_t>(cap);
@@ -268,6 +301,7 @@ void Engine::upload_initial() {
     check(cudaStreamSynchronize(st_), "sync");
 
     std::memset(&hctl_, 0, sizeof(hctl_));
+    set_size_classes(D0_, hctl_);
     Geometry& g = hctl_.g;
     g.ndim = nd;
     g.circle_k = walls_[0] < 0 ? -walls_[0] : 0;
@@ -481,6 +515,7 @@ void Engine::do_target_lock(std::uint64_t step) {
         check(cudaMemcpyAsync(a_.caps, caps_.data(), N * 4, cudaMemcpyHostToDevice, st_), "H2D caps");
     }
     finish_lock(c, hh_, step, D0min, D0max, D0med, S);
+    set_size_classes(Dn, hctl_);
     // full rebuild with the new diameters, re-anchor everything
     hctl_.build_kappa = 1.0;
     hctl_.build_t_shell = shell_of(D0min, D0med, D0max);

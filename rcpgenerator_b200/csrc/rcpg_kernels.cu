@@ -120,29 +120,54 @@ __global__ void k_build_prepare(DevArrays a) {
         a.cell_count[k] = 0u;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const int nd = a.ndim;
-        const double cutoff = (ctl->build_Dmax + ctl->build_t_shell) * (1.0 + 1e-6);
-        long long nc[kMaxDim];
-        double total = 1.0;
-        for (int d = 0; d < nd; ++d) {
-            double q = floor(ctl->g.box[d] / cutoff);
-            if (!(q >= 1.0)) q = 1.0;
-            if (q > 1048576.0) q = 1048576.0;
-            nc[d] = static_cast<long long>(q);
-            total *= q;
+        const int K = ctl->nclass > 1 ? ctl->nclass : 1;
+        // per class: cells at least one largest-member cutoff wide
+        long long nc[kMaxClass][kMaxDim];
+        double cells_k[kMaxClass];
+        double total = 0.0;
+        for (int k = 0; k < K; ++k) {
+            const double dmax = K > 1 ? xmul(ctl->class_d0max[k], ctl->build_kappa) : ctl->build_Dmax;
+            const double cutoff = (dmax + ctl->build_t_shell) * (1.0 + 1e-6);
+            cells_k[k] = 1.0;
+            for (int d = 0; d < nd; ++d) {
+                double q = floor(ctl->g.box[d] / cutoff);
+                if (!(q >= 1.0)) q = 1.0;
+                if (q > 1048576.0) q = 1048576.0;
+                nc[k][d] = static_cast<long long>(q);
+                cells_k[k] *= q;
+            }
+            total += cells_k[k];
         }
+        // coarsen the class with the most cells until all fit
         while (total > static_cast<double>(a.C_alloc)) {
+            int km = 0;
+            for (int k = 1; k < K; ++k)
+                if (cells_k[k] > cells_k[km]) km = k;
             int dm = 0;
             for (int d = 1; d < nd; ++d)
-                if (nc[d] > nc[dm]) dm = d;
-            const long long nn = (nc[dm] * 3) / 4;
-            total = total / static_cast<double>(nc[dm]) * static_cast<double>(nn < 1 ? 1 : nn);
-            nc[dm] = nn < 1 ? 1 : nn;
+                if (nc[km][d] > nc[km][dm]) dm = d;
+            const long long nn = (nc[km][dm] * 3) / 4;
+            total -= cells_k[km];
+            cells_k[km] = cells_k[km] / static_cast<double>(nc[km][dm]) * static_cast<double>(nn < 1 ? 1 : nn);
+            total += cells_k[km];
+            nc[km][dm] = nn < 1 ? 1 : nn;
+            if (cells_k[km] <= 1.0 && total > static_cast<double>(a.C_alloc)) break;
         }
-        std::uint32_t cells = 1;
+        std::uint32_t cells = 0;
+        for (int k = 0; k < K; ++k) {
+            ctl->cls_base[k] = cells;
+            std::uint32_t ck = 1;
+            for (int d = 0; d < nd; ++d) {
+                ctl->cls_ncell[k][d] = static_cast<int>(nc[k][d]);
+                ctl->cls_scale[k][d] = static_cast<double>(nc[k][d]) / ctl->g.box[d];
+                ck *= static_cast<std::uint32_t>(nc[k][d]);
+            }
+            cells += ck;
+        }
+        ctl->cls_base[K] = cells;
         for (int d = 0; d < nd; ++d) {
-            ctl->ncell[d] = static_cast<int>(nc[d]);
-            ctl->cell_scale[d] = static_cast<double>(nc[d]) / ctl->g.box[d];
-            cells *= static_cast<std::uint32_t>(nc[d]);
+            ctl->ncell[d] = ctl->cls_ncell[0][d];
+            ctl->cell_scale[d] = ctl->cls_scale[0][d];
         }
         ctl->ncells = cells;
         // every rebuild re-anchors every particle (x_last is written by k_bin)
@@ -163,12 +188,14 @@ __global__ void __launch_bounds__(256) k_build_bin(DevArrays a) {
     if (i >= a.N) return;
     double x[ND], D0;
     load_pos<ND>(a.pos, i, x, D0);
-    std::uint32_t c = 0, mul = 1;
+    int k = 0;  // size class
+    while (k + 1 < ctl->nclass && D0 >= ctl->class_d0[k + 1]) ++k;
+    std::uint32_t c = ctl->cls_base[k], mul = 1;
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
-        const int cd = cell_coord(x[d], ctl->cell_scale[d], ctl->ncell[d]);
+        const int cd = cell_coord(x[d], ctl->cls_scale[k][d], ctl->cls_ncell[k][d]);
         c += static_cast<std::uint32_t>(cd) * mul;
-        mul *= static_cast<std::uint32_t>(ctl->ncell[d]);
+        mul *= static_cast<std::uint32_t>(ctl->cls_ncell[k][d]);
         a.x_last[i * ND + d] = x[d];
     }
     a.cell_of[i] = c;
@@ -303,18 +330,13 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
     const std::uint32_t S = a.S;
     const Geometry& g = ctl->g;
     const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
-    double bx[ND], ibx[ND], scale[ND];
-    int nc[ND], nn[ND];
-    int total_combo = 1;
+    double bx[ND], ibx[ND];
     RCPG_UNROLL
     for (int d = 0; d < ND; ++d) {
         bx[d] = g.box[d];
         ibx[d] = g.inv_box[d];
-        scale[d] = ctl->cell_scale[d];
-        nc[d] = ctl->ncell[d];
-        nn[d] = nc[d] < 3 ? nc[d] : 3;  // distinct neighbour cells on this axis
-        total_combo *= nn[d];
     }
+    const int K = ctl->nclass > 1 ? ctl->nclass : 1;
     std::uint32_t* row = buf[w];
     const std::uint64_t warps = static_cast<std::uint64_t>(gridDim.x) * kWarpSearchWarps;
     for (std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(kWarpSearchWarps) + w; t < N; t += warps) {
@@ -322,39 +344,67 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
         double xi[ND], D0i;
         load_pos<ND>(a.spos, t, xi, D0i);
         const double Di = xmul(D0i, kap);
-        int cc[ND];
-        RCPG_UNROLL
-        for (int d = 0; d < ND; ++d) cc[d] = cell_coord(xi[d], scale[d], nc[d]);
         if (lane == 0) cnt[w] = 0u;
         __syncwarp();
         std::uint32_t n_half = 0;
-        for (int combo = lane; combo < total_combo; combo += 32) {
-            std::uint32_t cell = 0, mul = 1;
-            int r = combo;
+        // every grid: cells within the largest cutoff of particle i and a member
+        // of the class (one cell for its own and smaller classes, more for
+        // classes of smaller particles than i, whose cells are narrower)
+        for (int kc = 0; kc < K; ++kc) {
+            int nc[ND], nn[ND], lo[ND];
+            int total_combo = 1;
+            const double dmax = K > 1 ? xmul(ctl->class_d0max[kc], kap) : ctl->build_Dmax;
+            const double rcut = (Di + dmax) * 0.5 + t_shell;
             RCPG_UNROLL
             for (int d = 0; d < ND; ++d) {
-                const int k = r % nn[d];
-                r /= nn[d];
-                int c = (nc[d] >= 3) ? cc[d] - 1 + k : k;
-                if (c < 0) c += nc[d];
-                else if (c >= nc[d]) c -= nc[d];
-                cell += static_cast<std::uint32_t>(c) * mul;
-                mul *= static_cast<std::uint32_t>(nc[d]);
+                const double scale = ctl->cls_scale[kc][d];
+                nc[d] = ctl->cls_ncell[kc][d];
+                // cells per cutoff on this axis: 1 with one grid (cells are at
+                // least one cutoff wide), computed per class otherwise
+                double mm = 1.0;
+                if (K > 1) {
+                    mm = ceil(rcut * scale * (1.0 + 1e-6));
+                    if (!(mm >= 1.0)) mm = 1.0;
+                }
+                if (!(2.0 * mm + 1.0 <= static_cast<double>(nc[d]))) {
+                    nn[d] = nc[d];  // every cell of the axis, once
+                    lo[d] = 0;
+                } else {
+                    const int m = static_cast<int>(mm);
+                    nn[d] = 2 * m + 1;
+                    lo[d] = cell_coord(xi[d], scale, nc[d]) - m;
+                }
+                total_combo *= nn[d];
             }
-            const std::uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
-            for (std::uint32_t q = q0; q < q1; ++q) {
-                const std::uint32_t j = a.work[q];
-                if (j == i) continue;
-                double xj[ND], D0j;
-                load_pos<ND>(a.spos, q, xj, D0j);
-                const double Dj = xmul(D0j, kap);
-                const bool ok = (ND <= 3 || j > i) ? in_shell<ND>(xi, xj, Di, Dj, bx, ibx, t_shell)
-                                                   : in_shell<ND>(xi, xj, Dj, Di, bx, ibx, t_shell);
-                if (!ok) continue;
-                const std::uint32_t slot = atomicAdd(&cnt[w], 1u);
-                if (slot < static_cast<std::uint32_t>(kWarpRowSmem)) row[slot] = j;
-                else if (slot < S) a.nbr[static_cast<std::uint64_t>(slot) * N + t] = j;
-                if (j > i) ++n_half;
+            const std::uint32_t base = ctl->cls_base[kc];
+            for (int combo = lane; combo < total_combo; combo += 32) {
+                std::uint32_t cell = base, mul = 1;
+                int r = combo;
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    const int kk = r % nn[d];
+                    r /= nn[d];
+                    int c = lo[d] + kk;
+                    if (c < 0) c += nc[d];
+                    else if (c >= nc[d]) c -= nc[d];
+                    cell += static_cast<std::uint32_t>(c) * mul;
+                    mul *= static_cast<std::uint32_t>(nc[d]);
+                }
+                const std::uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
+                for (std::uint32_t q = q0; q < q1; ++q) {
+                    const std::uint32_t j = a.work[q];
+                    if (j == i) continue;
+                    double xj[ND], D0j;
+                    load_pos<ND>(a.spos, q, xj, D0j);
+                    const double Dj = xmul(D0j, kap);
+                    const bool ok = (ND <= 3 || j > i) ? in_shell<ND>(xi, xj, Di, Dj, bx, ibx, t_shell)
+                                                       : in_shell<ND>(xi, xj, Dj, Di, bx, ibx, t_shell);
+                    if (!ok) continue;
+                    const std::uint32_t slot = atomicAdd(&cnt[w], 1u);
+                    if (slot < static_cast<std::uint32_t>(kWarpRowSmem)) row[slot] = j;
+                    else if (slot < S) a.nbr[static_cast<std::uint64_t>(slot) * N + t] = j;
+                    if (j > i) ++n_half;
+                }
             }
         }
         __syncwarp();
@@ -451,7 +501,7 @@ constexpr std::size_t tile_smem_bytes() {
 template <int ND>
 __device__ __forceinline__ bool tiled_build_ok(const DevCtl* ctl) {
     if (ND > 3) return false;
-    bool ok = true;
+    bool ok = ctl->nclass <= 1;
     RCPG_UNROLL
     for (int d = 0; d < (ND <= 3 ? ND : 3); ++d)
         ok = ok & (ctl->ncell[d] >= TileShape<(ND <= 3 ? ND : 3)>::t(d) + 2);

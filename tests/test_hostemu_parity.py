@@ -13,7 +13,7 @@ HIST = ("phi_history", "force_history", "energy_history", "max_overlap_history",
         "alpha_history")
 FAST = ["n4_2d", "n16_2d", "n64_3d_bi", "n64_2d_walls_500", "n128_3d_sphere_3000",
         "n200_2d_disk_2500", "n300_4d_1500", "n64_3d_fix_diameter", "n100_2d_mu",
-        "n60_2d_fix_height_wall", "n80_2d_no_reorder"]
+        "n60_2d_fix_height_wall", "n600_3d_powerlaw10_sphere_1500", "n80_2d_no_reorder"]
 
 
 def digest(a):
