@@ -160,8 +160,8 @@ void rcpg_result_free(rcpg_result* r);
  *     which every thread block runs whole packings taken from a queue (no
  *     kernel launch per step).
  *   concurrency = 0: the persistent engine for the cheap packings (N x 3^ndim
- *     up to 3e4) and 32 ordinary engines on CUDA streams for the others, at the
- *     same time.
+ *     up to 3e4, diameters within a factor 2.5) and 32 ordinary engines on CUDA
+ *     streams for the others, at the same time.
  *   concurrency > 0: that many host threads each drive one ordinary engine at
  *     a time on their own CUDA stream of device opt->device.
  * Exact runs and runs that can reach a target-phi lock always take the stream
@@ -194,6 +194,13 @@ void rcpg_engine_destroy(rcpg_engine* e);
 int32_t rcpg_engine_profile_pair_kernel(rcpg_engine* e, uint32_t reps, double* avg_ms,
                                         double* alg_bytes, double* mean_row, char* err,
                                         size_t errlen);
+/* The same for the neighbour build's search kernel (the rebuild of
+ * get_pairs_kdtree, ENG:2758-3526; in graph mode the tiled build with the
+ * step's forces fused): `reps` full rebuilds of the current state, each from a
+ * cold L2, timed around the search kernel only. The rows are left rebuilt for
+ * the current positions; the control block is restored. */
+int32_t rcpg_engine_profile_build_kernel(rcpg_engine* e, uint32_t reps, double* avg_ms,
+                                         double* alg_bytes, char* err, size_t errlen);
 
 /* ---- per-step kernels on device buffers ---------------------------------- */
 

@@ -374,6 +374,17 @@ class PackingEngine:
         N.raise_for(rc, err)
         return {"avg_ms": ms.value, "alg_bytes": b.value, "mean_row": row.value}
 
+    def profile_build_kernel(self, reps: int = 10) -> dict:
+        """Mean launch time of the neighbour build's search kernel (graph mode:
+        the tiled build with the forces fused) on full rebuilds of the current
+        state, and its algorithmic bytes per launch."""
+        ms, b = C.c_double(), C.c_double()
+        err = N.errbuf()
+        rc = N.lib.rcpg_engine_profile_build_kernel(self._h, int(reps), C.byref(ms), C.byref(b),
+                                                    err, len(err))
+        N.raise_for(rc, err)
+        return {"avg_ms": ms.value, "alg_bytes": b.value}
+
     def close(self) -> None:
         if self._h:
             N.lib.rcpg_engine_destroy(self._h)

@@ -36,6 +36,7 @@ EXPORTED_SYMBOLS = (
     "rcpg_engine_result",
     "rcpg_engine_destroy",
     "rcpg_engine_profile_pair_kernel",
+    "rcpg_engine_profile_build_kernel",
     "rcpg_t_shell",
     "rcpg_pairs_full",
     "rcpg_pairs_full_noalloc",
@@ -195,6 +196,7 @@ def _load() -> C.CDLL:
         "rcpg_engine_kernel_launches": (C.c_uint64, [vp]),
         "rcpg_engine_result": (C.c_int32, [vp, C.POINTER(C.POINTER(Result)), cp, sz]),
         "rcpg_engine_destroy": (None, [vp]),
+        "rcpg_engine_profile_build_kernel": (C.c_int32, [vp, C.c_uint32, _dp, _dp, cp, sz]),
         "rcpg_engine_profile_pair_kernel": (
             C.c_int32, [vp, C.c_uint32, _dp, _dp, _dp, cp, sz]
         ),

@@ -285,8 +285,19 @@ int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const r
     std::vector<uint64_t> on_streams, persistent;
     for (uint64_t k = 0; k < count; ++k) {
         const bool eligible = concurrency <= 0 && !o.exact && !o.has_target_phi;
+        // the persistent kernel keeps one cell grid: wide size distributions
+        // (the engines' size-class grids) stay on the streams in the automatic split
+        double dlo = 0.0, dhi = 0.0;
+        if (inputs[k].diameters && inputs[k].N) {
+            dlo = dhi = inputs[k].diameters[0];
+            for (uint64_t i = 1; i < inputs[k].N; ++i) {
+                dlo = std::min(dlo, inputs[k].diameters[i]);
+                dhi = std::max(dhi, inputs[k].diameters[i]);
+            }
+        }
+        const bool narrow = dlo > 0.0 && dhi <= 2.5 * dlo;
         const bool ok = eligible && (concurrency < 0 ||
-                                     rcpg::batch_cost(inputs[k].N, inputs[k].ndim) <= kPersistentBudget);
+                                     (narrow && rcpg::batch_cost(inputs[k].N, inputs[k].ndim) <= kPersistentBudget));
         (ok ? persistent : on_streams).push_back(k);
     }
     std::thread pthread;
@@ -411,6 +422,18 @@ int32_t rcpg_engine_profile_pair_kernel(rcpg_engine* e, uint32_t reps, double* a
         return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: null argument");
     try {
         e->eng->profile_pair_kernel(reps, avg_ms, alg_bytes, mean_row);
+        return RCPG_OK;
+    } catch (const std::exception& ex) {
+        return fail(err, errlen, classify(ex), ex.what());
+    }
+}
+
+int32_t rcpg_engine_profile_build_kernel(rcpg_engine* e, uint32_t reps, double* avg_ms,
+                                         double* alg_bytes, char* err, size_t errlen) {
+    if (!e || !avg_ms || !alg_bytes)
+        return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: null argument");
+    try {
+        e->eng->profile_build_kernel(reps, avg_ms, alg_bytes);
         return RCPG_OK;
     } catch (const std::exception& ex) {
         return fail(err, errlen, classify(ex), ex.what());

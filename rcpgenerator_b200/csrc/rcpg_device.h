@@ -127,6 +127,9 @@ RCPG_HD unsigned force_blocks(std::uint64_t N) {
 // All take the device arrays by value and enqueue on `st`.
 void launch_adam_refresh(const DevArrays& a, int do_adam, int do_refresh, cudaStream_t st);
 void launch_rebuild(const DevArrays& a, cudaStream_t st);
+// the same, with e0 / e1 recorded just before and after the search kernels
+// (the tiled build and the warp search; the one that has nothing to do returns)
+void launch_rebuild_timed(const DevArrays& a, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1);
 void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st);
 void launch_reduce_exact(const DevArrays& a, cudaStream_t st);
 void launch_reduce_fast(const DevArrays& a, cudaStream_t st);

@@ -393,6 +393,48 @@ std::uint64_t Engine::builds() {
     return hctl_.nbuilds;
 }
 
+void Engine::profile_build_kernel(std::uint32_t reps, double* avg_ms, double* alg_bytes) {
+    pull_ctl();
+    const DevCtl saved = hctl_;
+    const std::size_t flush_bytes = std::size_t{256} << 20;
+    void* flush = nullptr;
+    check(cudaMallocAsync(&flush, flush_bytes, st_), "cudaMallocAsync(flush)");
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    double total_ms = 0.0;
+    for (std::uint32_t k = 0; k <= reps; ++k) {  // launch 0 warms up
+        hctl_ = saved;
+        hctl_.stopped = 0u;
+        hctl_.halted = 0u;
+        hctl_.rebuild_flag = 1u;
+        hctl_.fuse_forces = exact_ ? 0u : 1u;
+        push_ctl();
+        check(cudaMemsetAsync(flush, static_cast<int>(k & 0xFF), flush_bytes, st_), "flush");
+        launch_rebuild_timed(a_, st_, e0, e1);
+        check(cudaEventSynchronize(e1), "sync");
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+        if (k > 0) total_ms += ms;
+        launches_ += 9;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check(cudaFreeAsync(flush, st_), "cudaFreeAsync(flush)");
+    std::vector<std::uint32_t> cnt(N_);
+    check(cudaMemcpyAsync(cnt.data(), a_.nbr_cnt, N_ * 4, cudaMemcpyDeviceToHost, st_), "D2H cnt");
+    check(cudaStreamSynchronize(st_), "sync");
+    double total = 0.0;
+    for (std::uint32_t c : cnt) total += c;
+    // per particle: staged record (8P), id and row slot (8), row length (4),
+    // row entries (4k), and in graph mode the fused force F_i (8*ndim)
+    const double per = 8.0 * P_ + 12.0 + (exact_ ? 0.0 : 8.0 * ndim_);
+    *avg_ms = reps ? total_ms / reps : 0.0;
+    *alg_bytes = static_cast<double>(N_) * per + 4.0 * total;
+    hctl_ = saved;
+    push_ctl();
+}
+
 void Engine::profile_pair_kernel(std::uint32_t reps, double* avg_ms, double* alg_bytes,
                                  double* mean_row) {
     pull_ctl();

@@ -92,6 +92,11 @@ class Engine {
     // duration and the kernel's algorithmic bytes per launch.
     void profile_pair_kernel(std::uint32_t reps, double* avg_ms, double* alg_bytes,
                              double* mean_row);
+    // The same for the neighbour build's search (graph mode: the tiled build
+    // with the step's forces fused), each launch after the binning stages of a
+    // full rebuild of the current state and a cold L2. Leaves the rows rebuilt
+    // for the current positions; the control block is restored.
+    void profile_build_kernel(std::uint32_t reps, double* avg_ms, double* alg_bytes);
     // Mixed precision: the final state's forces evaluated with FP32 and with
     // FP64 pair terms on the same rows; relative difference of the pair
     // energy sum and max |F32 - F64| / max |F64|. Leaves the state unchanged.

@@ -1639,8 +1639,9 @@ void launch_tiled(const DevArrays& a, cudaStream_t st) {
     k_build_search_tiled<ND, SORT><<<static_cast<unsigned>(blocks), kTileThreads, smem, st>>>(a);
 }
 
+// e0 / e1 (optional): events recorded around the search kernels only
 template <int ND>
-void rebuild_impl(const DevArrays& a, cudaStream_t st) {
+void rebuild_impl(const DevArrays& a, cudaStream_t st, cudaEvent_t e0 = nullptr, cudaEvent_t e1 = nullptr) {
     const unsigned nb = force_blocks(a.N);
     const unsigned cb = (a.C_alloc + 1 + 255) / 256;
     k_build_prepare<<<cb < 1024 ? cb : 1024, 256, 0, st>>>(a);
@@ -1648,6 +1649,7 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     scan_exclusive(a.cell_count, a.cell_start, a.C_alloc + 1, a.scan_tmp, a.ctl, st);
     k_build_scatter<<<nb, kForceBlock, 0, st>>>(a);
     k_build_cell_sort<ND><<<(a.C_alloc + 255) / 256, 256, 0, st>>>(a);
+    if (e0) cudaEventRecord(e0, st);
     if (ND <= 3 && a.N >= kTiledMinN) {  // smaller packings never take the tiled path
         if (a.sorted_rows) launch_tiled<ND, true>(a, st);
         else launch_tiled<ND, false>(a, st);
@@ -1655,6 +1657,7 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st) {
     const unsigned need = static_cast<unsigned>((a.N + kWarpSearchWarps - 1) / kWarpSearchWarps),
                    g = resident_grid<k_build_search<ND>>(32 * kWarpSearchWarps);
     k_build_search<ND><<<need < g ? need : g, 32 * kWarpSearchWarps, 0, st>>>(a);
+    if (e1) cudaEventRecord(e1, st);
 }
 
 }  // namespace
@@ -1677,6 +1680,10 @@ void launch_adam_refresh(const DevArrays& a, int do_adam, int do_refresh, cudaSt
 
 void launch_rebuild(const DevArrays& a, cudaStream_t st) {
     RCPG_DISPATCH_ND(a.ndim, (rebuild_impl<ND>(a, st)));
+}
+
+void launch_rebuild_timed(const DevArrays& a, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
+    RCPG_DISPATCH_ND(a.ndim, (rebuild_impl<ND>(a, st, e0, e1)));
 }
 
 void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st) {
