@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define RCPG_ABI_VERSION 2
+#define RCPG_ABI_VERSION 3
 
 #define RCPG_OK 0
 #define RCPG_ERUNTIME (-1)
@@ -82,6 +82,10 @@ typedef struct rcpg_run_options {
      * global sums stay FP64. */
     int32_t pair_precision;
     double mixed_switch;         /* default 1e-5 */
+    /* Length in steps of the growth rung (mu_flag = 1, rcp_generator.cpp:5834-5931);
+     * 0 = the reference's deadline 6000 + 9*sqrt(N*ndim) (at least 1500). Set by a
+     * warm start from its predicted growth curve; no counterpart in the reference. */
+    uint64_t growth_steps;
 } rcpg_run_options;
 
 /* PackingObservation (rcp_generator.hpp:92-98). */
@@ -173,6 +177,12 @@ void rcpg_result_free(rcpg_result* r);
 int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
                        int32_t concurrency, rcpg_result** results, int32_t* status, char* err,
                        size_t errlen);
+/* rcpg_run_batch with a growth-rung length per packing (growth_steps[k],
+ * 0 = the reference's deadline), overriding opt->growth_steps: the batch form
+ * of a learned warm start. No counterpart in the reference. */
+int32_t rcpg_run_batch_growth(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
+                              const uint64_t* growth_steps, int32_t concurrency, rcpg_result** results,
+                              int32_t* status, char* err, size_t errlen);
 
 /* Step-wise control of one packing (the loop of run_packing_observed,
  * rcp_generator.cpp:5511-6662, advanced in slices). */
@@ -296,6 +306,37 @@ int32_t rcpg_initialize_particles(double phi, uint64_t N, int32_t ndim, const do
                                   uint64_t seed, double* positions_out, double* diameters_out,
                                   double* box_out, int8_t* walls_out, double* scale_factor_out,
                                   double* phi_modifier_out, char* err, size_t errlen);
+
+/* ---- learned warm start (no counterpart in the reference) ----------------
+ *
+ * A fully connected network with layer widths widths[0..layers]: hidden
+ * layers GELU(z) = 0.5 z (1 + erf(z / sqrt 2)), linear output. Parameters are
+ * one FP32 array (the master copy) and a BF16 copy of the same layout: for
+ * layer l, W_l [widths[l+1] x widths[l]] row-major, then b_l [widths[l+1]].
+ * Inputs X [batch x widths[0]] and targets T [batch x widths[layers]] are
+ * FP32, row-major. The kernels multiply BF16 weights and BF16 activations with
+ * FP32 accumulation; pre-activations, gradients and the loss are FP32. All
+ * pointers except `widths` are device pointers; `workspace` holds at least
+ * rcpg_mlp_workspace_bytes(...) bytes, 256-byte aligned. Calls are
+ * asynchronous on `stream`. */
+uint64_t rcpg_mlp_param_count(const int32_t* widths, int32_t layers);
+uint64_t rcpg_mlp_workspace_bytes(const int32_t* widths, int32_t layers, int32_t batch);
+/* Y [batch x widths[layers]] = network(X). */
+int32_t rcpg_mlp_forward(const int32_t* widths, int32_t layers, int32_t batch, const void* w_bf16,
+                         const float* w_fp32, const float* X, float* Y, void* workspace,
+                         uint64_t workspace_bytes, void* stream, char* err, size_t errlen);
+/* One training step on the loss L = sum_{b,o} out_weight[o] (Y[b,o] - T[b,o])^2 / (batch * widths[layers])
+ * (out_weight NULL = all ones): grad [param_count] = dL/dparams (FP32), and
+ * loss_terms [batch x widths[layers]] (optional) the summands. With lr > 0 and
+ * adam_m / adam_v non-NULL, Adam (beta 0.9 / 0.999, eps 1e-8, bias correction
+ * at `step` >= 1) updates w_fp32 and refreshes w_bf16. */
+int32_t rcpg_mlp_train_step(const int32_t* widths, int32_t layers, int32_t batch, float* w_fp32,
+                            void* w_bf16, float* adam_m, float* adam_v, float* grad, const float* X,
+                            const float* T, const float* out_weight, float lr, int32_t step,
+                            float* loss_terms, void* workspace, uint64_t workspace_bytes, void* stream,
+                            char* err, size_t errlen);
+/* y = BF16(x), round to nearest even; n elements. */
+int32_t rcpg_mlp_to_bf16(uint64_t n, const float* x, void* y, void* stream);
 
 #ifdef __cplusplus
 }

@@ -153,6 +153,8 @@ class _Inputs:
         if "initial_phi_target" in opts:
             ro.has_initial_phi_target = 1
             ro.initial_phi_target = float(opts["initial_phi_target"])
+        if "growth_steps" in opts:
+            ro.growth_steps = int(opts["growth_steps"])
         engine = str(config.get("engine", opts.get("engine", "graph")))
         if engine not in ("graph", "exact"):
             raise ValueError(f"unknown engine {engine!r} (expected 'graph' or 'exact')")
@@ -293,7 +295,7 @@ def run_packing_observed(input: dict, config: dict, progress_interval: int = 0,
 
 
 def run_packing_batch(items: list, options: dict | None = None, concurrency: int = 0,
-                      as_arrays: bool = True) -> list[dict]:
+                      as_arrays: bool = True, growth_steps=None) -> list[dict]:
     """Many independent packings, ``items`` = [(input, config), ...] as for
     run_packing; the run options (``options`` plus the engine keys ``engine``,
     ``pair_precision``, ``device``, ... of the first config) are shared.
@@ -302,6 +304,8 @@ def run_packing_batch(items: list, options: dict | None = None, concurrency: int
     ones there and the others to 32 ordinary engines on CUDA streams at the
     same time; k > 0 runs k ordinary engines at a time on their own streams
     (the reference runs one process per core, rcptools/jobs.py:392-401).
+    ``growth_steps`` (optional, one int per item, 0 = the reference's deadline)
+    sets each packing's growth-rung length, as a warm start does.
     Returns the result dicts in input order; a failed packing raises after all
     have run, naming its index."""
     items = list(items)
@@ -312,8 +316,16 @@ def run_packing_batch(items: list, options: dict | None = None, concurrency: int
     res = (C.POINTER(N.Result) * len(ins))()
     status = (C.c_int32 * len(ins))()
     err = N.errbuf()
-    rc = N.lib.rcpg_run_batch(arr, len(ins), C.byref(ins[0].ro), int(concurrency), res, status,
-                              err, len(err))
+    if growth_steps is None:
+        rc = N.lib.rcpg_run_batch(arr, len(ins), C.byref(ins[0].ro), int(concurrency), res, status,
+                                  err, len(err))
+    else:
+        gs = np.ascontiguousarray(np.asarray(growth_steps, dtype=np.uint64))
+        if gs.shape != (len(ins),):
+            raise ValueError("growth_steps needs one entry per packing")
+        rc = N.lib.rcpg_run_batch_growth(arr, len(ins), C.byref(ins[0].ro),
+                                         gs.ctypes.data_as(N._u64p), int(concurrency), res, status,
+                                         err, len(err))
     try:
         N.raise_for(rc, err)
         return [result_to_dict(r.contents, as_arrays=as_arrays) for r in res]

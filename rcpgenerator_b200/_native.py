@@ -29,6 +29,7 @@ EXPORTED_SYMBOLS = (
     "rcpg_run_packing",
     "rcpg_result_free",
     "rcpg_run_batch",
+    "rcpg_run_batch_growth",
     "rcpg_engine_create",
     "rcpg_engine_advance",
     "rcpg_engine_steps",
@@ -46,6 +47,11 @@ EXPORTED_SYMBOLS = (
     "rcpg_refresh_check",
     "rcpg_scale_diameters_nd",
     "rcpg_initialize_particles",
+    "rcpg_mlp_param_count",
+    "rcpg_mlp_workspace_bytes",
+    "rcpg_mlp_forward",
+    "rcpg_mlp_train_step",
+    "rcpg_mlp_to_bf16",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -53,6 +59,7 @@ _u32p = C.POINTER(C.c_uint32)
 _u64p = C.POINTER(C.c_uint64)
 _i8p = C.POINTER(C.c_int8)
 _u8p = C.POINTER(C.c_uint8)
+_i32p = C.POINTER(C.c_int32)
 
 
 class PackingInput(C.Structure):
@@ -87,6 +94,7 @@ class RunOptions(C.Structure):
         ("graph_steps", C.c_int32),
         ("pair_precision", C.c_int32),
         ("mixed_switch", C.c_double),
+        ("growth_steps", C.c_uint64),
     ]
 
 
@@ -182,6 +190,11 @@ def _load() -> C.CDLL:
              OBSERVER, vp, C.POINTER(C.POINTER(Result)), cp, sz],
         ),
         "rcpg_result_free": (None, [C.POINTER(Result)]),
+        "rcpg_run_batch_growth": (
+            C.c_int32,
+            [C.POINTER(PackingInput), C.c_uint64, C.POINTER(RunOptions), _u64p, C.c_int32,
+             C.POINTER(C.POINTER(Result)), C.POINTER(C.c_int32), cp, sz],
+        ),
         "rcpg_run_batch": (
             C.c_int32,
             [C.POINTER(PackingInput), C.c_uint64, C.POINTER(RunOptions), C.c_int32,
@@ -233,6 +246,18 @@ def _load() -> C.CDLL:
             [C.c_double, C.c_uint64, C.c_int32, _dp, C.c_int32, _i8p, C.c_int32, C.c_int32,
              C.POINTER(Distribution), C.c_uint64, _dp, _dp, _dp, _i8p, _dp, _dp, cp, sz],
         ),
+        "rcpg_mlp_param_count": (C.c_uint64, [_i32p, C.c_int32]),
+        "rcpg_mlp_workspace_bytes": (C.c_uint64, [_i32p, C.c_int32, C.c_int32]),
+        "rcpg_mlp_forward": (
+            C.c_int32,
+            [_i32p, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_uint64, vp, cp, sz],
+        ),
+        "rcpg_mlp_train_step": (
+            C.c_int32,
+            [_i32p, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp, vp, C.c_float, C.c_int32,
+             vp, vp, C.c_uint64, vp, cp, sz],
+        ),
+        "rcpg_mlp_to_bf16": (C.c_int32, [C.c_uint64, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -84,6 +84,7 @@ rcpg::EngineInput make_input(const rcpg_packing_input* in, const rcpg_run_option
     e.reorder_interval = o.reorder_interval;
     e.has_initial_phi_target = o.has_initial_phi_target != 0;
     e.initial_phi_target = o.initial_phi_target;
+    e.growth_steps = o.growth_steps;
     e.exact = o.exact != 0;
     e.device = o.device;
     e.graph_steps = o.graph_steps;
@@ -249,9 +250,11 @@ int32_t rcpg_run_packing(const rcpg_packing_input* in, const rcpg_run_options* o
     }
 }
 
-int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
-                       int32_t concurrency, rcpg_result** results, int32_t* status, char* err,
-                       size_t errlen) {
+namespace {
+
+int32_t run_batch_impl(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
+                       const uint64_t* growth_steps, int32_t concurrency, rcpg_result** results,
+                       int32_t* status, char* err, size_t errlen) {
     if ((!inputs && count) || (!results && count))
         return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: null argument");
     for (uint64_t k = 0; k < count; ++k) {
@@ -275,6 +278,11 @@ int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const r
             first_index = k;
             first_msg = msg;
         }
+    };
+    auto input_of = [&](uint64_t k) {
+        rcpg::EngineInput e = make_input(&inputs[k], &o);
+        if (growth_steps) e.growth_steps = growth_steps[k];
+        return e;
     };
     // concurrency 0: the cheap packings (graph engine, no target-phi lock, a
     // build step below kPersistentBudget candidate tests) go to the persistent
@@ -306,7 +314,7 @@ int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const r
             try {
                 std::vector<rcpg::EngineInput> ins;
                 ins.reserve(persistent.size());
-                for (uint64_t k : persistent) ins.push_back(make_input(&inputs[k], &o));
+                for (uint64_t k : persistent) ins.push_back(input_of(k));
                 const std::vector<rcpg::BatchOutcome> res =
                     rcpg::run_batch_persistent(ins, 2048u, on_streams.empty() ? 2 : 1);
                 for (std::size_t q = 0; q < persistent.size(); ++q) {
@@ -342,7 +350,7 @@ int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const r
         for (uint64_t q; (q = next.fetch_add(1)) < ns;) {
             const uint64_t k = on_streams[q];
             try {
-                rcpg::Engine eng(make_input(&inputs[k], &o), st);
+                rcpg::Engine eng(input_of(k), st);
                 eng.run(0, false, 0, rcpg::ObserverFn(), nullptr);
                 const rcpg::EngineResult r = eng.result();
                 results[k] = make_result(r, eng.N(), eng.ndim(), nullptr, false, eng.launches());
@@ -361,6 +369,20 @@ int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const r
     if (first_code != RCPG_OK)
         return fail(err, errlen, first_code, "packing " + std::to_string(first_index) + ": " + first_msg);
     return RCPG_OK;
+}
+
+}  // namespace
+
+int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
+                       int32_t concurrency, rcpg_result** results, int32_t* status, char* err,
+                       size_t errlen) {
+    return run_batch_impl(inputs, count, opt, nullptr, concurrency, results, status, err, errlen);
+}
+
+int32_t rcpg_run_batch_growth(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
+                              const uint64_t* growth_steps, int32_t concurrency, rcpg_result** results,
+                              int32_t* status, char* err, size_t errlen) {
+    return run_batch_impl(inputs, count, opt, growth_steps, concurrency, results, status, err, errlen);
 }
 
 void rcpg_result_free(rcpg_result* r) {

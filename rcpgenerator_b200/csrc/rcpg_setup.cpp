@@ -146,6 +146,8 @@ RunSetup prepare_run(const EngineInput& in) {
         double dl = 2.0 * 4000.0 + 9.0 * std::sqrt(static_cast<double>(N) * static_cast<double>(nd)) - 2000.0;
         if (dl < 1500.0) dl = 1500.0;
         rung1_deadline = static_cast<std::uint64_t>(dl);
+        // a warm start may shorten (or lengthen) the growth rung; no reference counterpart
+        if (in.growth_steps > 0) rung1_deadline = in.growth_steps;
     }
     std::uint64_t step_cap;
     if (in.max_steps > 0) {

@@ -40,6 +40,8 @@ struct EngineInput {
     // terms until the first step whose max overlap falls below mixed_switch
     int pair_precision = 0;
     double mixed_switch = 1e-5;
+    // length of the growth rung (mu_flag = 1); 0 = the reference's deadline
+    std::uint64_t growth_steps = 0;
 };
 
 struct RunSetup {

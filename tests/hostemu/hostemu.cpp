@@ -269,7 +269,7 @@ extern "C" int hostemu_run_packing(std::uint64_t N, int ndim, const double* posi
                                    int fix_diameter, std::uint64_t reorder_interval,
                                    double* pos_out, double* dia_out, double* hist_out,
                                    std::uint64_t hist_cap, std::uint64_t* origin_out,
-                                   double* scal_out) {
+                                   double* scal_out, std::uint64_t growth_steps) {
     EngineInput in;
     in.N = N;
     in.ndim = ndim;
@@ -284,6 +284,7 @@ extern "C" int hostemu_run_packing(std::uint64_t N, int ndim, const double* posi
     in.mu_override = mu;
     in.fix_diameter = fix_diameter != 0;
     in.reorder_interval = reorder_interval;
+    in.growth_steps = growth_steps;
     switch (ndim) {
         case 2: return run_nd<2>(in, pos_out, dia_out, hist_out, hist_cap, origin_out, scal_out);
         case 3: return run_nd<3>(in, pos_out, dia_out, hist_out, hist_cap, origin_out, scal_out);

@@ -17,7 +17,7 @@ class HostEmu:
         self.lib.hostemu_run_packing.restype = C.c_int
 
     def run(self, positions, diameters, box, walls, max_steps=0, neighbor_max=0, reorder=2000,
-            fix_height=False, mu=None, fix_diameter=False):
+            fix_height=False, mu=None, fix_diameter=False, growth_steps=0):
         pos = np.ascontiguousarray(positions, dtype=np.float64)
         N, nd = pos.shape
         D = np.ascontiguousarray(diameters, dtype=np.float64)
@@ -36,7 +36,8 @@ class HostEmu:
             C.c_uint32(neighbor_max), int(bool(fix_height)), C.c_uint64(max_steps),
             C.c_double(0.0 if mu is None else mu), int(mu is not None), int(bool(fix_diameter)),
             C.c_uint64(reorder), po.ctypes.data_as(_dp), do.ctypes.data_as(_dp), ho.ctypes.data_as(_dp),
-            C.c_uint64(cap), oo.ctypes.data_as(C.POINTER(C.c_uint64)), so.ctypes.data_as(_dp))
+            C.c_uint64(cap), oo.ctypes.data_as(C.POINTER(C.c_uint64)), so.ctypes.data_as(_dp),
+            C.c_uint64(growth_steps))
         assert rc == 0
         s = int(so[0])
         names = ("phi_history", "force_history", "energy_history", "max_overlap_history",

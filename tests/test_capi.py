@@ -29,7 +29,7 @@ def test_exports_every_declared_symbol(native):
 
 
 def test_version_and_abi(native):
-    assert native.lib.rcpg_abi_version() == 2
+    assert native.lib.rcpg_abi_version() == 3
     assert b"sm_100a" in native.lib.rcpg_version()
 
 
