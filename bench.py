@@ -1,4 +1,4 @@
-"""Throughput of the packing engine on BASELINE config 2.
+"""Throughput of the packing engine on the 2-D bidisperse N = 1M packing.
 
 Workload (one replica per GPU, independent packings, no collective):
 2-D bidisperse disks, N = 1,000,000, diameters 1.0 : 1.4 at 50:50 number
@@ -163,30 +163,9 @@ def batch_instances(count: int, seed0: int = 0):
     [64, 16384], ndim from {2, 3, 4}, diameters mono (d=1), bidisperse 50:50
     with ratio uniform on [1.1, 3.0], or log-normal with std/mean uniform on
     [0.1, 0.6] truncated to [0.2, 5] x mean; periodic unit boxes at phi 0.10;
-    seeds seed0.. . Positions and diameters from the engine's initializer."""
-    import rcpgenerator_b200 as rb
-    out = []
-    for k in range(count):
-        seed = seed0 + k
-        rng = np.random.default_rng(seed)
-        n = int(round(np.exp(rng.uniform(np.log(64), np.log(16384)))))
-        nd = int(rng.choice([2, 3, 4]))
-        kind = int(rng.integers(3))
-        if kind == 0:
-            dist = {"type": "mono", "d": 1.0}
-        elif kind == 1:
-            dist = {"type": "bidisperse", "d1": 1.0, "d2": float(rng.uniform(1.1, 3.0)), "p": 0.5}
-        else:
-            cv = rng.uniform(0.1, 0.6)
-            s2 = np.log1p(cv * cv)
-            d = rng.lognormal(-0.5 * s2, np.sqrt(s2), size=4 * n)
-            d = d[(d >= 0.2) & (d <= 5.0)][:n]
-            dist = {"type": "custom", "custom": d.tolist()}
-        init = rb.initialize_particles({"phi": 0.10, "N": n, "Ndim": nd, "box": [1.0] * nd,
-                                        "walls": [0] * nd, "dist": dist, "seed": seed})
-        out.append(({"positions": np.asarray(init["positions"]), "diameters": np.asarray(init["diameters"])},
-                    {"box": init["box"], "walls": init["walls"], "neighbor_max": 0, "seed": seed}))
-    return out
+    seeds seed0.. (rcpgenerator_b200.warmstart.draw_packing)."""
+    from rcpgenerator_b200.warmstart import draw_packing
+    return [draw_packing(seed0 + k) for k in range(count)]
 
 
 def _ref_capped(args_):
@@ -237,6 +216,27 @@ def run_batch_workload(args) -> int:
     steps = [r["steps"] for r in res]
     value = len(items) / (t2 - t1) * 3600.0
     single_value = len(single) / (t1 - t0) * 3600.0
+    warm = None
+    if not args.no_warm_start:
+        from rcpgenerator_b200 import warmstart as W
+        if Path(args.warm_start_model).exists():
+            ws = W.WarmStart.load(args.warm_start_model, device=local)
+            t3 = time.perf_counter()
+            wres, phi_pred = ws.run_batch(items, run_opts, concurrency=args.concurrency)
+            t4 = time.perf_counter()
+            pj = np.asarray([r["phi"] for r in res])
+            wj = np.asarray([r["phi"] for r in wres])
+            warm = {"value": len(items) / (t4 - t3) * 3600.0, "unit": BATCH_METRIC,
+                    "vs_plain_engine": len(items) / (t4 - t3) * 3600.0 / single_value,
+                    "vs_batched_plain": (t2 - t1) / (t4 - t3),
+                    "mean_steps": float(np.mean([r["steps"] for r in wres])),
+                    "delta_phi_J_mean": float(wj.mean() - pj.mean()),
+                    "delta_phi_J_abs_mean": float(np.abs(wj - pj).mean()),
+                    "phi_J_pred_mae": float(np.abs(phi_pred - pj).mean()),
+                    "max_overlap": float(max(r["max_min_dist"] for r in wres)),
+                    "model": str(Path(args.warm_start_model).name),
+                    "note": "the same packings with the network's growth-rung lengths (inference inside "
+                            "the timed region); phi_J compared packing by packing with the batched plain run"}
     cpu = None
     if not args.no_cpu_baseline and rank == 0:
         procs = os.cpu_count() or 1
@@ -267,6 +267,7 @@ def run_batch_workload(args) -> int:
         "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": BATCH_METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "note": "the timed region is already end to end (host arrays in, result dicts out)"},
+        "warm_start": warm,
     }
     if rank == 0:
         print(json.dumps(line))
@@ -292,7 +293,7 @@ def run_reference_arm(args):
                    "engine": "reference C++/OpenMP run_packing_observed, portable build",
                    "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"first {s['timed_steps']} steps after step 1 of config 2 "
+                         "sample": f"first {s['timed_steps']} steps after step 1 of the same packing "
                                    f"(observer timestamps), setup excluded"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -309,6 +310,8 @@ def main() -> int:
     ap.add_argument("--cpu-sample-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-warm-start", action="store_true", help="batch workload: skip the warm-started arm")
+    ap.add_argument("--warm-start-model", default=str(REPO / "rcpgenerator_b200" / "warmstart_model.npz"))
     ap.add_argument("--pair-precision", default="mixed", choices=["mixed", "f64"],
                     help="pair arithmetic: mixed = FP32 pair terms while the max overlap >= 1e-5 "
                          "(the workload's stated precision), f64 = FP64 throughout")

@@ -42,6 +42,7 @@ struct DevCtl {
     // D0 in [class_d0[k], class_d0[k+1]) and has its own grid, as wide as the
     // pair cutoff of its largest member (class_d0max[k]); nclass <= 1: one grid
     int nclass;
+    int tile_rows;       // 2-D tiled build: tile height in cells (set by k_build_prepare)
     double class_d0[kMaxClass + 1];
     double class_d0max[kMaxClass];
     int cls_ncell[kMaxClass][kMaxDim];

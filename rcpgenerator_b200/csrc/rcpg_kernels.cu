@@ -112,6 +112,11 @@ __global__ void __launch_bounds__(256) k_adam_refresh(DevArrays a, int do_adam, 
 // ===========================================================================
 // B. pair-list rebuild: grid -> bin -> scan -> scatter -> search
 // ===========================================================================
+// Height of the 2-D tiles of the tiled search (k_build_search_tiled), chosen
+// per build from the mean cell occupancy.
+constexpr int kTileRowsMin = 4, kTileRowsMax = 12, kTileRowsPref = 8;
+constexpr int kTileStage2 = 1024;  // staged particles per 2-D tile (TileShape<2>::stage)
+
 __global__ void k_build_prepare(DevArrays a) {
     DevCtl* ctl = a.ctl;
     if (build_off(ctl)) return;
@@ -170,6 +175,18 @@ __global__ void k_build_prepare(DevArrays a) {
             ctl->cell_scale[d] = ctl->cls_scale[0][d];
         }
         ctl->ncells = cells;
+        // 2-D tiles: kTileRowsPref cells high, lower where the halo's
+        // particles at the mean cell occupancy (with 30 % headroom) would not
+        // fit the staging area
+        if (nd == 2) {
+            const double ppc = static_cast<double>(a.N) / static_cast<double>(cells ? cells : 1u);
+            const double fit = floor(static_cast<double>(kTileStage2) / (18.0 * 1.3 * (ppc > 1e-3 ? ppc : 1e-3))) - 2.0;
+            double r = fit < static_cast<double>(kTileRowsPref) ? fit : static_cast<double>(kTileRowsPref);
+            if (!(r >= kTileRowsMin)) r = kTileRowsMin;
+            ctl->tile_rows = static_cast<int>(r);
+        } else {
+            ctl->tile_rows = 0;
+        }
         // every rebuild re-anchors every particle (x_last is written by k_bin)
         ctl->kappa_min = ctl->build_kappa;
         // graph mode: the tiled build also computes this step's forces
@@ -472,11 +489,13 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
 // neighbour cells from shared memory only. Used when every axis has at least
 // tile + 2 cells (no cell of the halo is loaded twice); otherwise, and for
 // ndim > 3, k_build_search handles the build.
+// 2-D tiles are 16 cells wide and ctl->tile_rows (kTileRowsMin..kTileRowsMax)
+// high; t(1) is the largest height.
 template <int ND> struct TileShape;
 template <> struct TileShape<2> {
-    __host__ __device__ static constexpr int t(int d) { return d == 0 ? 16 : 8; }
-    static constexpr int halo_cells = 18 * 10;
-    static constexpr int stage = 1024;
+    __host__ __device__ static constexpr int t(int d) { return d == 0 ? 16 : kTileRowsMax; }
+    static constexpr int halo_cells = 18 * (kTileRowsMax + 2);
+    static constexpr int stage = kTileStage2;
 };
 template <> struct TileShape<3> {
     __host__ __device__ static constexpr int t(int) { return 4; }
@@ -504,7 +523,7 @@ __device__ __forceinline__ bool tiled_build_ok(const DevCtl* ctl) {
     bool ok = ctl->nclass <= 1;
     RCPG_UNROLL
     for (int d = 0; d < (ND <= 3 ? ND : 3); ++d)
-        ok = ok & (ctl->ncell[d] >= TileShape<(ND <= 3 ? ND : 3)>::t(d) + 2);
+        ok = ok & (ctl->ncell[d] >= (ND == 2 && d == 1 ? ctl->tile_rows : TileShape<(ND <= 3 ? ND : 3)>::t(d)) + 2);
     return ok;
 }
 
@@ -598,15 +617,23 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     __shared__ float hbf[ND];  // half box, FP32 (mixed minimum image)
     if (threadIdx.x < ND) hbf[threadIdx.x] = static_cast<float>(0.5 * ctl->g.box[threadIdx.x]);
     int nc[ND], nt[ND];
-    double cellw[ND];  // origin of a tile's relative coordinates: its first cell's corner
+    // cell width (origin of a tile's relative coordinates: its first cell's
+    // corner) and tile extent per axis (the 2-D height is chosen per build)
+    __shared__ double cellw[ND];
+    __shared__ int s_ts[ND];
     std::uint32_t tiles = 1;
     RCPG_UNROLL
     for (int d = 0; d < ND; ++d) {
         nc[d] = ctl->ncell[d];
-        cellw[d] = ctl->g.box[d] / static_cast<double>(nc[d]);
-        nt[d] = (nc[d] + TS::t(d) - 1) / TS::t(d);
+        const int tsd = (ND == 2 && d == 1) ? ctl->tile_rows : TS::t(d);
+        if (threadIdx.x == 0) {
+            s_ts[d] = tsd;
+            cellw[d] = ctl->g.box[d] / static_cast<double>(nc[d]);
+        }
+        nt[d] = (nc[d] + tsd - 1) / tsd;
         tiles *= static_cast<std::uint32_t>(nt[d]);
     }
+    __syncthreads();  // s_ts, cellw, bx, ibx, hbf
     if (threadIdx.x == 0) s_need = 0u;
     if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) ctl->nsum_blocks = gridDim.x;
     std::uint16_t* mine = s_rows + threadIdx.x;
@@ -622,8 +649,8 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
         for (int d = 0; d < ND; ++d) {
             const int tc = static_cast<int>(rem % static_cast<std::uint32_t>(nt[d]));
             rem /= static_cast<std::uint32_t>(nt[d]);
-            t0[d] = tc * TS::t(d);
-            const int tw = min(TS::t(d), nc[d] - t0[d]);
+            t0[d] = tc * s_ts[d];
+            const int tw = min(s_ts[d], nc[d] - t0[d]);
             hw[d] = tw + 2;
             H *= hw[d];
         }

@@ -192,7 +192,7 @@ class WarmStart:
     deadline]."""
 
     def __init__(self, net: Network, x_mean, x_std, y_mean, y_std, eps: float = 2e-3,
-                 margin: float = 1.0, min_steps: int = 1500, meta: dict | None = None):
+                 margin: float = 1.5, min_steps: int = 1500, meta: dict | None = None):
         self.net = net
         self.x_mean = np.asarray(x_mean, dtype=np.float64)
         self.x_std = np.asarray(x_std, dtype=np.float64)

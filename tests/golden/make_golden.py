@@ -108,7 +108,7 @@ PACK_CASES = [
     ("n60_2d_fix_height_wall", {"positions": _FH_POS.tolist(), "diameters": _FH_D.tolist()},
      {"box": [20.0, 4.0], "walls": [0, 1], "neighbor_max": 0, "seed": 0, "fix_height": True},
      {"max_steps": 1500}),
-    # size ratio 10 (BASELINE config 3's distribution, spherical container), several grid size classes
+    # size ratio 10 (power law d^-3 on [0.1, 1], spherical container), several grid size classes
     ("n600_3d_powerlaw10_sphere_1500", dict(phi=0.2, N=600, Ndim=3, box=[1.0, 1.0, 1.0], walls=[-3, 0, 0],
                                             dist={"type": "powerlaw", "d_min": 0.1, "d_max": 1.0, "exponent": -3.0},
                                             seed=123), None, {"max_steps": 1500}),

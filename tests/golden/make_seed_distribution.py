@@ -1,4 +1,4 @@
-"""Reference phi_J / steps / final max overlap of BASELINE config 1 over seeds
+"""Reference phi_J / steps / final max overlap of the 3-D monodisperse N = 2000 packing over seeds
 0..63 (3-D monodisperse, N = 2000, initial phi 0.08, periodic unit box), one
 OpenMP thread per packing, eight packings at a time. Writes
 tests/golden/cfg1_seeds.npz. Needs the reference build in oracle/_ref

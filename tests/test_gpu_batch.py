@@ -130,7 +130,7 @@ def test_persistent_batch_mixed_ndim_converges(cuda_device, golden):
 
 @pytest.mark.parametrize("precision", ["f64", "mixed"])
 def test_persistent_batch_config1_phiJ_distribution_64_seeds(cuda_device, golden, precision):
-    """BASELINE config 1 over 64 seeds in one persistent launch against the
+    """The 3-D monodisperse N = 2000 packing over 64 seeds in one persistent launch against the
     reference's distribution on the same seeds: |mean phi_J - reference| <= 1e-3,
     mean step count within 5 %, every packing under the reference's gate."""
     import rcpgenerator_b200 as rb

@@ -1,4 +1,4 @@
-"""Graph-mode packings of BASELINE config 1 over 64 seeds against the
+"""Graph-mode packings of the 3-D monodisperse N = 2000 packing (phi0 0.08) over 64 seeds against the
 reference's distribution on the same seeds (tests/golden/cfg1_seeds.npz):
 relaxation to jamming is chaotic, so the graph engine (tree-order FP64
 reductions, CUDA libm in the controller) is matched in distribution:

@@ -9,7 +9,7 @@ every global sum stay FP64. Checked here:
 * the first steps track the FP64 graph engine (FP32 rounding of the forces);
 * the run reports the final state's energy / force error of the FP32 terms
   against FP64 terms on the same rows, and the step of the switch;
-* BASELINE config 1 over 64 seeds matches the reference's phi_J distribution
+* the 3-D monodisperse N = 2000 packing over 64 seeds matches the reference's phi_J distribution
   (|mean phi_J - reference mean| <= 1e-3) and every packing meets the gate.
 """
 

@@ -1,7 +1,7 @@
 """Whole packings on the GPU.
 
 * exact engine: bit-for-bit equal to the reference engine (one OpenMP thread)
-  on the golden packings, including BASELINE config 1 (N=2000 3D, seed 123);
+  on the golden packings, including the 3-D monodisperse N=2000 packing (seed 123);
 * graph engine: converges under the reference's own gate, and its first
   steps agree with the exact engine to 1e-12 relative.
 """
