@@ -770,7 +770,7 @@ struct Pool {
     template <typename T>
     T* get(std::size_t n) {
         void* p = nullptr;
-        const cudaError_t e = cudaMallocAsync(&p, std::max<std::size_t>(n * sizeof(T), 16), st);
+        const cudaError_t e = pool_alloc_async(&p, n * sizeof(T), st);
         if (e != cudaSuccess) {
             cudaGetLastError();
             throw EngineError(-2, std::string("rcpgenerator_b200: batch allocation failed: ") + cudaGetErrorString(e));

@@ -168,8 +168,8 @@ struct Scratch {
     explicit Scratch(cudaStream_t s) : st(s) {}
     void* get(std::size_t bytes) {
         void* p = nullptr;
-        if (cudaMallocAsync(&p, bytes < 16 ? 16 : bytes, st) != cudaSuccess)
-            throw rcpg::EngineError(-2, "rcpgenerator_b200: cudaMallocAsync failed");
+        if (rcpg::pool_alloc_async(&p, bytes, st) != cudaSuccess)
+            throw rcpg::EngineError(-2, "rcpgenerator_b200: device allocation failed");
         ptrs.push_back(p);
         return p;
     }
@@ -308,6 +308,12 @@ int32_t run_batch_impl(const rcpg_packing_input* inputs, uint64_t count, const r
                                      (narrow && rcpg::batch_cost(inputs[k].N, inputs[k].ndim) <= kPersistentBudget));
         (ok ? persistent : on_streams).push_back(k);
     }
+    // the stream workers take the most expensive packings first (longest
+    // processing time first), so that no large packing starts last and runs
+    // alone at the end; results keep their input slots
+    std::stable_sort(on_streams.begin(), on_streams.end(), [&](uint64_t x, uint64_t y) {
+        return rcpg::batch_cost(inputs[x].N, inputs[x].ndim) > rcpg::batch_cost(inputs[y].N, inputs[y].ndim);
+    });
     std::thread pthread;
     if (!persistent.empty()) {
         pthread = std::thread([&]() {
@@ -351,6 +357,7 @@ int32_t run_batch_impl(const rcpg_packing_input* inputs, uint64_t count, const r
             const uint64_t k = on_streams[q];
             try {
                 rcpg::Engine eng(input_of(k), st);
+                eng.set_blocking_sync(true);  // many host threads: sleep while the GPU works
                 eng.run(0, false, 0, rcpg::ObserverFn(), nullptr);
                 const rcpg::EngineResult r = eng.result();
                 results[k] = make_result(r, eng.N(), eng.ndim(), nullptr, false, eng.launches());

@@ -134,6 +134,10 @@ void launch_rebuild_timed(const DevArrays& a, cudaStream_t st, cudaEvent_t e0, c
 void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st);
 void launch_reduce_exact(const DevArrays& a, cudaStream_t st);
 void launch_reduce_fast(const DevArrays& a, cudaStream_t st);
+// out[0] = max |ref[k]|, out[1] = max |cmp[k] - ref[k]| over k < n, as the bit
+// patterns of the non-negative doubles (out zeroed first by the caller).
+void launch_diff_max(const double* ref, const double* cmp, std::uint64_t n, unsigned long long* out,
+                     cudaStream_t st);
 void launch_controller(const DevArrays& a, int open_only, cudaStream_t st);
 void launch_reorder(const DevArrays& a, cudaStream_t st);
 void launch_fix_height(const DevArrays& a, cudaStream_t st);

@@ -21,15 +21,50 @@
 
 namespace rcpg {
 
-// Device memory of an engine comes from the device's stream-ordered pool
-// (cudaMallocAsync / cudaFreeAsync on the engine's stream), so creating and
-// destroying engines never synchronises the device: engines on other streams
-// (a batch) keep running. The pinned control block used to read the device
+// Device memory of an engine comes from this library's stream-ordered pool of
+// the device (cudaMallocFromPoolAsync / cudaFreeAsync on the engine's stream),
+// so creating and destroying engines never synchronises the device: engines
+// on other streams (a batch) keep running. The pool keeps up to kPoolKeep
+// bytes of freed memory reserved for the next engine (the default pool hands
+// it back to the driver at every synchronisation, and the next engine pays a
+// driver allocation again). The pinned control block used to read the device
 // controller is recycled through a process-wide free list for the same reason.
 namespace {
 std::mutex g_pinned_mu;
 std::vector<DevCtl*> g_pinned_free;
+std::mutex g_pool_mu;
+std::vector<cudaMemPool_t> g_pools;  // by device ordinal, created on first use
+constexpr std::uint64_t kPoolKeep = std::uint64_t{16} << 30;
 }  // namespace
+
+cudaError_t pool_alloc_async(void** p, std::size_t bytes, cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (static_cast<int>(g_pools.size()) <= dev) g_pools.resize(dev + 1, nullptr);
+        if (!g_pools[dev]) {
+            cudaMemPoolProps props;
+            std::memset(&props, 0, sizeof(props));
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&g_pools[dev], &props);
+            if (e != cudaSuccess) {
+                g_pools[dev] = nullptr;
+                return e;
+            }
+            std::uint64_t keep = kPoolKeep;
+            e = cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+            if (e != cudaSuccess) return e;
+        }
+        pool = g_pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes < 16 ? 16 : bytes, pool, st);
+}
 
 DevCtl* pinned_ctl_acquire() {
     {
@@ -116,7 +151,7 @@ void Engine::alloc_device() {
     P_ = pos_stride(nd);
     auto dalloc = [&](std::size_t bytes) -> void* {
         void* p = nullptr;
-        check(cudaMallocAsync(&p, bytes < 16 ? 16 : bytes, st_), "cudaMallocAsync");
+        check(pool_alloc_async(&p, bytes, st_), "cudaMallocFromPoolAsync");
         allocs_.push_back(p);
         return p;
     };
@@ -224,11 +259,11 @@ void Engine::ensure_row_capacity(std::uint32_t need) {
     a_.nbr = nullptr;
     a_.pterm = nullptr;
     void* p = nullptr;
-    check(cudaMallocAsync(&p, static_cast<std::size_t>(S) * N_ * 4, st_), "cudaMallocAsync(nbr)");
+    check(pool_alloc_async(&p, static_cast<std::size_t>(S) * N_ * 4, st_), "cudaMallocFromPoolAsync(nbr)");
     allocs_.push_back(p);
     a_.nbr = static_cast<std::uint32_t*>(p);
     if (exact_) {
-        check(cudaMallocAsync(&p, static_cast<std::size_t>(S) * N_ * sizeof(PairTerms), st_), "cudaMallocAsync(pterm)");
+        check(pool_alloc_async(&p, static_cast<std::size_t>(S) * N_ * sizeof(PairTerms), st_), "cudaMallocFromPoolAsync(pterm)");
         allocs_.push_back(p);
         a_.pterm = static_cast<PairTerms*>(p);
     }
@@ -253,8 +288,22 @@ void Engine::push_ctl() {
 
 void Engine::pull_ctl() {
     check(cudaMemcpyAsync(hctl_pinned_, a_.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, st_), "pull ctl");
-    check(cudaStreamSynchronize(st_), "sync");
+    if (sync_ev_) {
+        check(cudaEventRecord(sync_ev_, st_), "event record");
+        check(cudaEventSynchronize(sync_ev_), "sync");
+    } else {
+        check(cudaStreamSynchronize(st_), "sync");
+    }
     hctl_ = *hctl_pinned_;
+}
+
+void Engine::set_blocking_sync(bool on) {
+    if (on && !sync_ev_) {
+        check(cudaEventCreateWithFlags(&sync_ev_, cudaEventBlockingSync | cudaEventDisableTiming), "event");
+    } else if (!on && sync_ev_) {
+        cudaEventDestroy(sync_ev_);
+        sync_ev_ = nullptr;
+    }
 }
 
 // Parameters of the kernels of the step that begin_step() just opened
@@ -384,6 +433,7 @@ Engine::Engine(const EngineInput& in, cudaStream_t stream) {
 
 Engine::~Engine() {
     cudaSetDevice(device_);
+    if (sync_ev_) cudaEventDestroy(sync_ev_);
     free_device();
     if (own_stream_ && st_) cudaStreamDestroy(st_);
 }
@@ -398,7 +448,7 @@ void Engine::profile_build_kernel(std::uint32_t reps, double* avg_ms, double* al
     const DevCtl saved = hctl_;
     const std::size_t flush_bytes = std::size_t{256} << 20;
     void* flush = nullptr;
-    check(cudaMallocAsync(&flush, flush_bytes, st_), "cudaMallocAsync(flush)");
+    check(pool_alloc_async(&flush, flush_bytes, st_), "cudaMallocFromPoolAsync(flush)");
     cudaEvent_t e0, e1;
     check(cudaEventCreate(&e0), "event");
     check(cudaEventCreate(&e1), "event");
@@ -447,7 +497,7 @@ void Engine::profile_pair_kernel(std::uint32_t reps, double* avg_ms, double* alg
     // launch's lines (L2 is 126 MB), then the launch alone is timed
     const std::size_t flush_bytes = std::size_t{256} << 20;
     void* flush = nullptr;
-    check(cudaMallocAsync(&flush, flush_bytes, st_), "cudaMallocAsync(flush)");
+    check(pool_alloc_async(&flush, flush_bytes, st_), "cudaMallocFromPoolAsync(flush)");
     cudaEvent_t e0, e1;
     check(cudaEventCreate(&e0), "event");
     check(cudaEventCreate(&e1), "event");
@@ -904,7 +954,12 @@ void Engine::pair_precision_error(double* energy_rel, double* force_rel) {
     const DevCtl saved = hctl_;
     const std::uint64_t n = N_ * static_cast<std::uint64_t>(ndim_);
     check(cudaMemcpyAsync(a_.vec_tmp, a_.F, n * 8, cudaMemcpyDeviceToDevice, st_), "save F");
-    std::vector<double> F[2];
+    // the FP64 forces and the two maxima stay on the device
+    void* scratch = nullptr;
+    check(pool_alloc_async(&scratch, n * 8 + 16, st_), "cudaMallocFromPoolAsync(precision check)");
+    double* F64 = static_cast<double*>(scratch);
+    unsigned long long* mx = reinterpret_cast<unsigned long long*>(F64 + n);
+    check(cudaMemsetAsync(mx, 0, 16, st_), "memset");
     double U[2] = {0.0, 0.0};
     for (int prec = 0; prec < 2; ++prec) {  // 0: FP64, 1: FP32 pair terms
         hctl_ = saved;
@@ -916,19 +971,25 @@ void Engine::pair_precision_error(double* energy_rel, double* force_rel) {
         launch_forces(a_, 0, st_);
         launch_reduce_fast(a_, st_);
         launches_ += 2;
-        F[prec].resize(n);
-        check(cudaMemcpyAsync(F[prec].data(), a_.F, n * 8, cudaMemcpyDeviceToHost, st_), "D2H F");
+        if (prec == 0) {
+            check(cudaMemcpyAsync(F64, a_.F, n * 8, cudaMemcpyDeviceToDevice, st_), "copy F");
+        } else {
+            launch_diff_max(F64, a_.F, n, mx, st_);
+            ++launches_;
+        }
         pull_ctl();
         U[prec] = hctl_.sums.pair_U;
     }
-    double fmax = 0.0, dmax = 0.0;
-    for (std::uint64_t k = 0; k < n; ++k) {
-        fmax = std::max(fmax, std::fabs(F[0][k]));
-        dmax = std::max(dmax, std::fabs(F[1][k] - F[0][k]));
-    }
+    unsigned long long bits[2] = {0ull, 0ull};
+    check(cudaMemcpyAsync(bits, mx, 16, cudaMemcpyDeviceToHost, st_), "D2H max");
+    check(cudaStreamSynchronize(st_), "sync");
+    double fmax, dmax;
+    std::memcpy(&fmax, &bits[0], 8);
+    std::memcpy(&dmax, &bits[1], 8);
     *energy_rel = U[0] != 0.0 ? std::fabs(U[1] - U[0]) / std::fabs(U[0]) : std::fabs(U[1]);
     *force_rel = fmax > 0.0 ? dmax / fmax : dmax;
     check(cudaMemcpyAsync(a_.F, a_.vec_tmp, n * 8, cudaMemcpyDeviceToDevice, st_), "restore F");
+    check(cudaFreeAsync(scratch, st_), "cudaFreeAsync");
     hctl_ = saved;
     push_ctl();
 }

@@ -52,6 +52,9 @@ using ObserverFn = std::function<void(const Observation&, const std::vector<doub
 
 struct DevCtl;
 // pinned host copies of the control block, recycled across engines
+// Stream-ordered device allocation from this library's pool of the current
+// device (freed memory stays reserved for the next engine; free with cudaFreeAsync).
+cudaError_t pool_alloc_async(void** p, std::size_t bytes, cudaStream_t st);
 DevCtl* pinned_ctl_acquire();
 void pinned_ctl_release(DevCtl* p);
 
@@ -101,6 +104,9 @@ class Engine {
     // FP64 pair terms on the same rows; relative difference of the pair
     // energy sum and max |F32 - F64| / max |F64|. Leaves the state unchanged.
     void pair_precision_error(double* energy_rel, double* force_rel);
+    // Waits for the device by sleeping on a blocking event instead of spinning
+    // (for many engines driven by more host threads than cores: a batch).
+    void set_blocking_sync(bool on);
 
    private:
     void setup_host(const EngineInput& in);
@@ -165,6 +171,7 @@ class Engine {
     std::uint64_t graph_nodes_per_step_ = 0;
     std::uint32_t* pinned_ = nullptr;
     DevCtl* hctl_pinned_ = nullptr;
+    cudaEvent_t sync_ev_ = nullptr;  // blocking-sync event (set_blocking_sync)
 };
 
 }  // namespace rcpg

@@ -1726,6 +1726,46 @@ void launch_reduce_exact(const DevArrays& a, cudaStream_t st) {
     RCPG_DISPATCH_ND(a.ndim, (k_reduce_exact<ND><<<1, 1, 0, st>>>(a)));
 }
 
+// max |ref| and max |cmp - ref| (mixed-precision error report): a
+// non-negative double's bit pattern orders like its value, so the block
+// maxima combine with an integer atomicMax
+__global__ void __launch_bounds__(256) k_diff_max(const double* __restrict__ ref, const double* __restrict__ cmp,
+                                                  std::uint64_t n, unsigned long long* out) {
+    double m0 = 0.0, m1 = 0.0;
+    for (std::uint64_t k = blockIdx.x * 256ull + threadIdx.x; k < n; k += static_cast<std::uint64_t>(gridDim.x) * 256ull) {
+        const double r = ref[k];
+        m0 = fmax(m0, fabs(r));
+        m1 = fmax(m1, fabs(cmp[k] - r));
+    }
+    RCPG_UNROLL
+    for (int o = 16; o > 0; o >>= 1) {
+        m0 = fmax(m0, __shfl_down_sync(0xffffffffu, m0, o));
+        m1 = fmax(m1, __shfl_down_sync(0xffffffffu, m1, o));
+    }
+    __shared__ double s0[8], s1[8];
+    if ((threadIdx.x & 31) == 0) {
+        s0[threadIdx.x >> 5] = m0;
+        s1[threadIdx.x >> 5] = m1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; ++w) {
+            m0 = fmax(m0, s0[w]);
+            m1 = fmax(m1, s1[w]);
+        }
+        atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(m0)));
+        atomicMax(out + 1, static_cast<unsigned long long>(__double_as_longlong(m1)));
+    }
+}
+
+void launch_diff_max(const double* ref, const double* cmp, std::uint64_t n, unsigned long long* out,
+                     cudaStream_t st) {
+    std::uint64_t blocks = (n + 255) / 256;
+    if (blocks > 1184) blocks = 1184;
+    if (blocks < 1) blocks = 1;
+    k_diff_max<<<static_cast<unsigned>(blocks), 256, 0, st>>>(ref, cmp, n, out);
+}
+
 void launch_reduce_fast(const DevArrays& a, cudaStream_t st) {
     k_reduce_fast<<<1, kCtlThreads, 0, st>>>(a);
 }

@@ -1,7 +1,8 @@
 // Learned warm start: a small MLP (BF16 weights and activations, FP32
 // accumulation, FP32 master weights) mapping size-distribution descriptors to
 // a predicted phi_J and a growth schedule. Hand-written training and inference
-// kernels: a strided tiled GEMM, GELU, mean squared error, Adam.
+// kernels: a strided tensor-core GEMM (mma.sync BF16 -> FP32), GELU, mean
+// squared error, Adam.
 //
 // Parameters of an L-layer MLP with widths w[0..L] are packed in one FP32
 // array: layer l holds W_l [w[l+1] x w[l]] row-major, then b_l [w[l+1]]. The
@@ -19,30 +20,84 @@
 
 namespace {
 
-constexpr int kTile = 16;
+// Tensor-core GEMM: C[m, n] = sum_k A[m*sam + k*sak] * B[k*sbk + n*sbn] (+ bias[n]).
+// A 64x64 tile of C per block of 4 warps (2x2), each warp 32x32 as 2x4
+// mma.sync.m16n8k16 BF16 tiles with FP32 accumulators. Any operand strides:
+// every K step of 16 stages the A (m, k) and B (n, k) slices in shared memory,
+// zero-filled outside the matrices, with rows padded to 24 elements (12
+// words) so that the fragment loads of a warp fall in distinct banks.
+constexpr int kBM = 64, kBN = 64, kBK = 16, kPad = 24, kGemmThreads = 128;
 
-// C[m, n] = sum_k A[m*sam + k*sak] * B[k*sbk + n*sbn] (+ bias[n]); operands
-// BF16, accumulation FP32 in the fixed order k = 0, 1, ...
-__global__ void __launch_bounds__(kTile* kTile)
+__device__ __forceinline__ std::uint32_t lds_pair(const __nv_bfloat16* p) {
+    return *reinterpret_cast<const std::uint32_t*>(p);
+}
+
+__global__ void __launch_bounds__(kGemmThreads)
     k_gemm_bf16(int M, int N, int K, const __nv_bfloat16* __restrict__ A, long long sam, long long sak,
                 const __nv_bfloat16* __restrict__ B, long long sbk, long long sbn, float* __restrict__ C,
                 long long ldc, const float* __restrict__ bias) {
-    __shared__ float As[kTile][kTile + 1];
-    __shared__ float Bs[kTile][kTile + 1];
-    const int tx = threadIdx.x % kTile, ty = threadIdx.x / kTile;
-    const int m = blockIdx.y * kTile + ty, n = blockIdx.x * kTile + tx;
-    float acc = 0.0f;
-    for (int k0 = 0; k0 < K; k0 += kTile) {
-        const int ka = k0 + tx, kb = k0 + ty;
-        const int ma = blockIdx.y * kTile + ty, nb = blockIdx.x * kTile + tx;
-        As[ty][tx] = (ma < M && ka < K) ? __bfloat162float(A[ma * sam + ka * sak]) : 0.0f;
-        Bs[ty][tx] = (kb < K && nb < N) ? __bfloat162float(B[kb * sbk + nb * sbn]) : 0.0f;
-        __syncthreads();
+    __shared__ __align__(16) __nv_bfloat16 As[kBM][kPad];
+    __shared__ __align__(16) __nv_bfloat16 Bs[kBN][kPad];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+    float acc[2][4][4];
 #pragma unroll
-        for (int k = 0; k < kTile; ++k) acc = fmaf(As[ty][k], Bs[k][tx], acc);
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0f;
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+    for (int k0 = 0; k0 < K; k0 += kBK) {
+        // stage: 64x16 elements of each operand, 8 per thread
+#pragma unroll
+        for (int r = 0; r < (kBM * kBK) / kGemmThreads; ++r) {
+            const int e = tid + r * kGemmThreads;
+            const int row = e / kBK, kk = e % kBK;
+            const int m = m0 + row, n = n0 + row, k = k0 + kk;
+            As[row][kk] = (m < M && k < K) ? A[m * sam + k * sak] : zero;
+            Bs[row][kk] = (n < N && k < K) ? B[k * sbk + n * sbn] : zero;
+        }
+        __syncthreads();
+        std::uint32_t af[2][4], bf[4][2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int r0 = wm + i * 16 + g;
+            af[i][0] = lds_pair(&As[r0][2 * t]);
+            af[i][1] = lds_pair(&As[r0 + 8][2 * t]);
+            af[i][2] = lds_pair(&As[r0][2 * t + 8]);
+            af[i][3] = lds_pair(&As[r0 + 8][2 * t + 8]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int c0 = wn + j * 8 + g;
+            bf[j][0] = lds_pair(&Bs[c0][2 * t]);
+            bf[j][1] = lds_pair(&Bs[c0][2 * t + 8]);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                asm volatile(
+                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+                    "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+                    : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+                    : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bf[j][0]), "r"(bf[j][1]));
         __syncthreads();
     }
-    if (m < M && n < N) C[m * ldc + n] = acc + (bias ? bias[n] : 0.0f);
+    // epilogue: c0, c1 at (g, 2t..2t+1), c2, c3 at (g+8, 2t..2t+1) of each 16x8 tile
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int m = m0 + wm + i * 16 + g + (r >= 2 ? 8 : 0);
+                const int n = n0 + wn + j * 8 + 2 * t + (r & 1);
+                if (m < M && n < N) C[m * ldc + n] = acc[i][j][r] + (bias ? bias[n] : 0.0f);
+            }
 }
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
@@ -106,8 +161,8 @@ __global__ void k_adam(int n, float* __restrict__ w, float* __restrict__ m, floa
 
 void gemm(cudaStream_t st, int M, int N, int K, const __nv_bfloat16* A, long long sam, long long sak,
           const __nv_bfloat16* B, long long sbk, long long sbn, float* C, long long ldc, const float* bias) {
-    dim3 grid((N + kTile - 1) / kTile, (M + kTile - 1) / kTile);
-    k_gemm_bf16<<<grid, kTile * kTile, 0, st>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, bias);
+    dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
+    k_gemm_bf16<<<grid, kGemmThreads, 0, st>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, bias);
 }
 
 unsigned blocks(long long n) { return static_cast<unsigned>((n + 255) / 256); }

@@ -8,12 +8,36 @@
 #include <limits>
 #include <numeric>
 #include <stdexcept>
+#include <thread>
 
 namespace rcpg {
 
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;
+
+// fn(i) for i in [0, n) on up to 16 host threads (large n only). Used for
+// per-particle terms that the caller then sums in index order, so results do
+// not depend on the thread count.
+template <typename Fn>
+void parallel_for(std::size_t n, Fn fn) {
+    unsigned T = std::thread::hardware_concurrency();
+    T = T < 1 ? 1 : (T > 16 ? 16 : T);
+    if (n < (std::size_t{1} << 16) || T == 1) {
+        for (std::size_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const std::size_t chunk = (n + T - 1) / T;
+    for (unsigned t = 0; t < T; ++t) {
+        const std::size_t lo = t * chunk, hi = std::min(n, lo + chunk);
+        if (lo >= hi) break;
+        pool.emplace_back([lo, hi, &fn]() {
+            for (std::size_t i = lo; i < hi; ++i) fn(i);
+        });
+    }
+    for (auto& th : pool) th.join();
+}
 
 }  // namespace
 
@@ -27,8 +51,15 @@ std::vector<double> scale_diameters_nd(const std::vector<double>& D, double phi_
                                        bool fix_height, double* factor_out) {
     double V_box = 1.0;
     for (double L : box) V_box *= L;
+    // sphere_volume(Di * 0.5, ndim) per particle, its constant factors
+    // evaluated once (same operations in the same order), summed in order
+    const double c_pi = std::pow(kPi, ndim / 2.0), c_gamma = std::tgamma(ndim / 2.0 + 1.0);
+    std::vector<double> vol(D.size());
+    parallel_for(D.size(), [&](std::size_t i) {
+        vol[i] = c_pi * std::pow(D[i] * 0.5, static_cast<double>(ndim)) / c_gamma;
+    });
     double sumVol = 0.0;
-    for (double Di : D) sumVol += sphere_volume(Di * 0.5, ndim);
+    for (double v : vol) sumVol += v;
     const double factor = fix_height ? std::pow(phi_target * V_box / sumVol, 1.0 / double(ndim - 1))
                                      : std::pow(phi_target * V_box / sumVol, 1.0 / double(ndim));
     std::vector<double> out = D;
@@ -48,12 +79,12 @@ std::vector<std::uint32_t> pair_caps(const std::vector<double>& D, int ndim,
     if (dmin <= 0.0) dmin = 1.0;
     const double scaling = static_cast<double>(ndim) / 3.0;
     const double omega = 1.0 + static_cast<double>(ndim) / 6.0;
-    for (std::size_t i = 0; i < N; ++i) {
+    parallel_for(N, [&](std::size_t i) {
         const double cap_d = scaling * (50.0 * std::pow(D[i] / dmin, omega) + static_cast<double>(neighbor_max));
         std::uint32_t cap = static_cast<std::uint32_t>(std::ceil(cap_d));
         if (static_cast<std::uint64_t>(cap) > N) cap = static_cast<std::uint32_t>(N);
         caps[i] = cap;
-    }
+    });
     return caps;
 }
 
@@ -76,6 +107,7 @@ RunSetup prepare_run(const EngineInput& in) {
 
     // refresh-trigger scale from the caller's diameters (ENG:4401-4430)
     double trigger_scale;
+    double med_in;  // median of the caller's diameters (rank N/2)
     {
         double dmx = 0.0, dmn = std::numeric_limits<double>::max();
         for (double dv : D) {
@@ -85,6 +117,7 @@ RunSetup prepare_run(const EngineInput& in) {
         std::vector<double> Ds = D;
         std::nth_element(Ds.begin(), Ds.begin() + Ds.size() / 2, Ds.end());
         const double med = Ds[Ds.size() / 2];
+        med_in = med;
         const double t_shell = std::min(std::max(med * 1.02, dmn * 2.25), dmx) * 0.5;
         const double rho = t_shell / dmn;
         trigger_scale = std::min(1.28 * rho, 1.9);
@@ -115,18 +148,20 @@ RunSetup prepare_run(const EngineInput& in) {
     else if (nd == 4) phi = 0.15;
     else if (nd == 5) phi = 0.10;
     else if (nd > 5) phi = 0.10 / std::pow(2, (nd - 4));
+    double factor = 1.0;  // diameter scale of the start (1 with fix_diameter)
     if (!in.fix_diameter) {
-        double factor = 1.0;
         std::vector<double> Ds = scale_diameters_nd(D, phi * phi_modifier, box, nd, in.fix_height, &factor);
         if (in.fix_height) {
             box[nd - 1] = box[nd - 1] * factor;
             for (std::size_t i = 0; i < N; ++i) x[i * nd + (nd - 1)] = x[i * nd + (nd - 1)] * factor;
         }
-        D = Ds;
+        D = std::move(Ds);
     }
     const double coeff = std::pow(kPi, nd / 2.0) / std::tgamma(nd / 2.0 + 1.0);
+    std::vector<double> terms(N);
+    parallel_for(N, [&](std::size_t i) { terms[i] = coeff * std::pow(D[i] / 2.0, static_cast<double>(nd)); });
     double current_volume = 0.0;
-    for (std::size_t i = 0; i < N; ++i) current_volume += coeff * std::pow(D[i] / 2.0, static_cast<double>(nd));
+    for (double v : terms) current_volume += v;
     double box_volume = std::accumulate(box.begin(), box.end(), 1.0, std::multiplies<double>());
     phi = current_volume / box_volume / phi_modifier;
     const double Dmin = *std::min_element(D.begin(), D.end());
@@ -174,9 +209,9 @@ RunSetup prepare_run(const EngineInput& in) {
         S += rN;
         if (D0_[i] > D0max) D0max = D0_[i];
     }
-    std::vector<double> Dm = D0_;
-    std::nth_element(Dm.begin(), Dm.begin() + N / 2, Dm.end());
-    const double D0med = Dm[N / 2];
+    // the median of D0 = D * factor: a positive scale keeps every rank, and
+    // the element at rank N/2 was scaled by the same rounded multiplication
+    const double D0med = in.fix_diameter ? med_in : med_in * factor;
 
     Controller& c = out.c;
     std::memset(&c, 0, sizeof(c));

@@ -1,8 +1,12 @@
 """The warm-start network's CUDA kernels (csrc/rcpg_mlp.cu, through the C ABI)
 against the CPU oracle oracle/mlp_oracle.py, which rounds to BF16 exactly
 where the kernels store BF16 and computes in FP64 otherwise. The remaining
-differences are FP32 accumulation order and the rare BF16 rounding that order
-flips, hence relative tolerances of about 1e-4 on norms."""
+differences come from the tensor cores' FP32 accumulation (their summation
+order and internal alignment, about 1e-6 relative on a pre-activation) and
+from the BF16 roundings those differences flip (2^-8 relative each, on about
+one stored value in a thousand), which compound over the three hidden
+layers: relative tolerances of 1e-3 on the output and 5e-3 on each layer's
+gradient norm."""
 
 from __future__ import annotations
 
@@ -49,7 +53,34 @@ def test_forward_matches_oracle(cuda_device, B):
     Y = net.forward(X)
     Yo, _, _ = mo.forward(net.params(), WIDTHS, X, bf16=True)
     assert Y.shape == (B, WIDTHS[-1])
-    assert np.linalg.norm(Y - Yo) <= 1e-4 * np.linalg.norm(Yo)
+    assert np.linalg.norm(Y - Yo) <= 1e-3 * np.linalg.norm(Yo)
+
+
+@pytest.mark.parametrize("K,O,B", [(11, 17, 5), (256, 256, 70), (100, 3, 129)])
+def test_tensor_core_gemm_exact_on_small_integers(cuda_device, K, O, B):
+    """A one-layer network (no activation) on small integers: every product
+    and partial sum is exact in BF16 / FP32, so the forward GEMM, the weight
+    gradient GEMM and the bias gradient must match NumPy exactly; this pins
+    the fragment layout of the tensor-core tiles and the tile edges."""
+    from rcpgenerator_b200.warmstart import Network
+    rng = np.random.default_rng(K * 1000 + O + B)
+    W = rng.integers(-3, 4, size=(O, K)).astype(np.float64)
+    X = rng.integers(-3, 4, size=(B, K)).astype(np.float32)
+    net = Network(widths=(K, O), params=np.concatenate([W.ravel(), np.zeros(O)]))
+    Y = net.forward(X)
+    np.testing.assert_array_equal(Y, X.astype(np.float64) @ W.T)
+    # dL/dz = 2 (Y - T) / (B O) with (Y - T) small integers and B O a power of two
+    Bp, Op = 32, 16
+    W2 = rng.integers(-3, 4, size=(Op, K)).astype(np.float64)
+    X2 = rng.integers(-3, 4, size=(Bp, K)).astype(np.float32)
+    d = rng.integers(-3, 4, size=(Bp, Op)).astype(np.float64)
+    T2 = (X2.astype(np.float64) @ W2.T - d).astype(np.float32)
+    net2 = Network(widths=(K, Op), params=np.concatenate([W2.ravel(), np.zeros(Op)]))
+    net2.train_step(X2, T2, 0.0, update=False)
+    g = net2.grad.cpu().numpy().astype(np.float64)
+    dz = 2.0 * d / (Bp * Op)
+    np.testing.assert_array_equal(g[:Op * K].reshape(Op, K), dz.T @ X2.astype(np.float64))
+    np.testing.assert_array_equal(g[Op * K:], dz.sum(axis=0))
 
 
 @pytest.mark.parametrize("widths,B", [(WIDTHS, 64), ((5, 19, 33, 3), 45), ((11, 256, 17), 300)])
@@ -59,9 +90,9 @@ def test_gradient_matches_oracle(cuda_device, widths, B):
     loss = float(net.train_step(X, T, 0.0, w, update=False))
     g = net.grad.cpu().numpy().astype(np.float64)
     lo, go = mo.loss_and_grad(net.params(), widths, X, T, w, bf16=True)
-    assert abs(loss - lo) <= 1e-5 * lo
+    assert abs(loss - lo) <= 1e-4 * lo
     for gb, ob in zip(_blocks(g, widths), _blocks(go, widths)):
-        assert np.linalg.norm(gb - ob) <= 1e-3 * np.linalg.norm(ob) + 1e-12
+        assert np.linalg.norm(gb - ob) <= 5e-3 * np.linalg.norm(ob) + 1e-12
 
 
 def test_adam_step_matches_oracle(cuda_device):
@@ -79,7 +110,7 @@ def test_adam_step_matches_oracle(cuda_device):
         assert np.abs(net.params() - p).max() <= 1e-6 * np.abs(p).max()
         # and its gradient from the oracle's
         gk = net.grad.cpu().numpy().astype(np.float64)
-        assert np.linalg.norm(gk - g) <= 1e-3 * np.linalg.norm(g)
+        assert np.linalg.norm(gk - g) <= 5e-3 * np.linalg.norm(g)
         p = net.params()
     # the BF16 copy is the rounded master copy
     w16 = net.w16.float().cpu().numpy().astype(np.float64)
