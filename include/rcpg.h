@@ -307,6 +307,21 @@ int32_t rcpg_initialize_particles(double phi, uint64_t N, int32_t ndim, const do
                                   double* box_out, int8_t* walls_out, double* scale_factor_out,
                                   double* phi_modifier_out, char* err, size_t errlen);
 
+/* ---- analysis ------------------------------------------------------------- */
+
+/* overlap_report of the reference's analysis package (rcptools/overlap.py:7-113):
+ * candidates are the pairs i < j within 2 * max(D)/2 (minimum image on every
+ * axis when box != NULL, as the reference does whatever the walls); a candidate
+ * overlaps when (r_i + r_j) - |pos_i - pos_j| > 0. Host arrays in and out:
+ * *n_candidate_out, *n_overlap_out; for the first min(n_overlap, capacity)
+ * overlapping pairs in ascending (i, j): pairs_out[2m] = {i, j},
+ * frac_sum_out[m] = overlap / (r_i + r_j), frac_min_out[m] = overlap / min(r_i, r_j).
+ * RCPG_ENOSPC when n_overlap > capacity (the counts are still set). */
+int32_t rcpg_overlap_report(uint64_t N, int32_t ndim, const double* positions, const double* diameters,
+                            const double* box, uint64_t* n_candidate_out, uint64_t* n_overlap_out,
+                            uint64_t capacity, uint32_t* pairs_out, double* frac_sum_out,
+                            double* frac_min_out, int32_t device, char* err, size_t errlen);
+
 /* ---- learned warm start (no counterpart in the reference) ----------------
  *
  * A fully connected network with layer widths widths[0..layers]: hidden

@@ -47,6 +47,7 @@ EXPORTED_SYMBOLS = (
     "rcpg_refresh_check",
     "rcpg_scale_diameters_nd",
     "rcpg_initialize_particles",
+    "rcpg_overlap_report",
     "rcpg_mlp_param_count",
     "rcpg_mlp_workspace_bytes",
     "rcpg_mlp_forward",
@@ -245,6 +246,11 @@ def _load() -> C.CDLL:
             C.c_int32,
             [C.c_double, C.c_uint64, C.c_int32, _dp, C.c_int32, _i8p, C.c_int32, C.c_int32,
              C.POINTER(Distribution), C.c_uint64, _dp, _dp, _dp, _i8p, _dp, _dp, cp, sz],
+        ),
+        "rcpg_overlap_report": (
+            C.c_int32,
+            [C.c_uint64, C.c_int32, _dp, _dp, _dp, _u64p, _u64p, C.c_uint64, _u32p, _dp, _dp, C.c_int32,
+             cp, sz],
         ),
         "rcpg_mlp_param_count": (C.c_uint64, [_i32p, C.c_int32]),
         "rcpg_mlp_workspace_bytes": (C.c_uint64, [_i32p, C.c_int32, C.c_int32]),

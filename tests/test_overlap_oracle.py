@@ -1,0 +1,43 @@
+"""The overlap-report oracle (oracle/overlap_oracle.py) against the reference's
+overlap_report on the final states of the golden packings
+(tests/golden/overlap_report.npz, made by tests/golden/make_overlap_golden.py),
+and phi_corrected / engine_max_overlap of the jobs client on the CPU."""
+
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
+import overlap_oracle as oo  # noqa: E402
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def _cases():
+    z = np.load(GOLD / "overlap_report.npz")
+    return sorted({k.split("/")[0] for k in z.files})
+
+
+@pytest.mark.parametrize("case", _cases())
+def test_oracle_matches_reference_overlap_report(case):
+    g = np.load(GOLD / "overlap_report.npz")
+    p = np.load(GOLD / "packs.npz")
+    P, S, M, ncand = oo.overlap_pairs(p[f"{case}/positions"], p[f"{case}/diameters"], p[f"{case}/box"])
+    np.testing.assert_array_equal(P, g[f"{case}/pairs"])
+    assert (len(P), ncand) == tuple(g[f"{case}/counts"])
+    np.testing.assert_allclose(S, g[f"{case}/fractions_sum"], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(M, g[f"{case}/fractions_min"], rtol=1e-12, atol=1e-15)
+
+
+def test_phi_corrected_and_engine_max_overlap():
+    from rcpgenerator_b200 import jobs
+    assert jobs.phi_corrected(0.64, 1e-3, 3) == pytest.approx(0.64 * 0.999 ** 3, rel=1e-15)
+
+    class P:
+        max_min_dist = 4.5e-4
+    assert jobs.engine_max_overlap(P()) == 4.5e-4
+    assert jobs.engine_max_overlap(object()) == 0.0
