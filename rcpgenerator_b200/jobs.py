@@ -246,7 +246,9 @@ def _prepare_job(job):
     """(seed, D, Packing or None, row or None) of one job: the shuffle and the
     pre-screen of run_packing_job (jobs.py:268-300), then the packing."""
     seed = int(job["seed"])
-    D = np.asarray(job["diameters"], dtype=float)
+    # a copy: the caller's job keeps its diameters (the reference's workers
+    # shuffle a pickled copy)
+    D = np.array(job["diameters"], dtype=float)
     np.random.default_rng(seed).shuffle(D)
     ndim = int(job["Ndim"])
     ps = job.get("prescreen", {}) or {}

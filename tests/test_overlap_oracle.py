@@ -41,3 +41,16 @@ def test_phi_corrected_and_engine_max_overlap():
         max_min_dist = 4.5e-4
     assert jobs.engine_max_overlap(P()) == 4.5e-4
     assert jobs.engine_max_overlap(object()) == 0.0
+
+
+def test_job_preparation_leaves_the_job_unchanged():
+    """The seeded shuffle of run_packing_job works on a copy: the caller's
+    job dict (and a second run of it) sees the original diameter order."""
+    from rcpgenerator_b200 import jobs
+    d = np.linspace(0.8, 1.2, 64)
+    job = {"diameters": d.copy(), "seed": 4, "Ndim": 2, "phi_init": 0.5, "initializer_phi": 0.11}
+    s1, D1, p1, r1 = jobs._prepare_job(job)
+    np.testing.assert_array_equal(job["diameters"], d)
+    s2, D2, p2, r2 = jobs._prepare_job(job)
+    np.testing.assert_array_equal(D1, D2)
+    assert r1 is None and np.allclose(sorted(p1.diameters), sorted(p2.diameters))
