@@ -74,7 +74,7 @@ struct DevArrays {
     std::uint64_t N;
     int ndim;
     int P;                  // pos stride
-    double* pos;            // [N*P] x_0..x_{d-1}, D0
+    double* pos;            // [N*P] x_0..x_{d-1}, D0 (32-byte aligned records for the force kernel)
     double* pos_tmp;        // [N*P] reorder gather target
     double* spos;           // [N*P] positions in cell order (build scratch; may alias pos_tmp)
     double* F;              // [N*ndim]

@@ -27,6 +27,27 @@ __device__ __forceinline__ void load_pos(const double* __restrict__ pos, std::ui
     }
 }
 
+// load_pos from global memory: with ld256 (P == 4, 32-byte aligned records,
+// data not written by the running kernel; the caller checks the alignment)
+// the record is one 256-bit read-only load instead of two 128-bit loads.
+template <int ND>
+__device__ __forceinline__ void load_pos_g(const double* __restrict__ pos, std::uint64_t i, double* x,
+                                           double& D0, int ld256) {
+    if constexpr (pos_stride(ND) == 4) {
+        if (ld256) {
+            double w[4];
+            asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+                : "=d"(w[0]), "=d"(w[1]), "=d"(w[2]), "=d"(w[3])
+                : "l"(pos + i * 4));
+#pragma unroll
+            for (int d = 0; d < ND; ++d) x[d] = w[d];
+            D0 = w[ND];
+            return;
+        }
+    }
+    load_pos<ND>(pos, i, x, D0);
+}
+
 template <int ND>
 __device__ __forceinline__ void store_pos(double* __restrict__ pos, std::uint64_t i,
                                           const double* x, double D0) {

@@ -1080,7 +1080,7 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
          t += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
         const std::uint64_t i = a.work ? a.work[t] : t;
         double xi[ND], D0i;
-        load_pos<ND>(a.pos, i, xi, D0i);
+        load_pos_g<ND>(a.pos, i, xi, D0i, 1);
         const double Di = xmul(D0i, kap);
         double fi[ND];
         const std::uint32_t n = min(a.nbr_cnt[t], a.S);
@@ -1113,7 +1113,7 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
                     jj[u] = (k0 + u < n) ? __ldg(a.nbr + static_cast<std::uint64_t>(k0 + u) * N + t) : 0u;
                 RCPG_UNROLL
                 for (std::uint32_t u = 0; u < kChunk; ++u)
-                    if (k0 + u < n && jj[u] < N) load_pos<ND>(a.pos, jj[u], xj[u], D0j[u]);
+                    if (k0 + u < n && jj[u] < N) load_pos_g<ND>(a.pos, jj[u], xj[u], D0j[u], 1);
                 RCPG_UNROLL
                 for (std::uint32_t u = 0; u < kChunk; ++u) {
                     if (k0 + u >= n) break;
@@ -1714,6 +1714,9 @@ void launch_rebuild_timed(const DevArrays& a, cudaStream_t st, cudaEvent_t e0, c
 }
 
 void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st) {
+    // k_forces reads a 4-double particle record (ndim <= 3) with one 256-bit load
+    if (a.P == 4 && (reinterpret_cast<std::uintptr_t>(a.pos) & 31u) != 0)
+        throw std::invalid_argument("rcpgenerator_b200: particle records must be 32-byte aligned");
     if (exact_terms) {
         RCPG_DISPATCH_ND(a.ndim, (forces_nd<ND, true, false>(a, st)));
     } else {
