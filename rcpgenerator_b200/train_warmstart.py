@@ -39,8 +39,16 @@ def main(argv=None) -> dict:
     ap.add_argument("--eval-n", type=int, default=100_000)
     ap.add_argument("--eval-concurrency", type=int, default=8)
     ap.add_argument("--eval-margins", default="", help="extra comma-separated margins to evaluate")
+    ap.add_argument("--eval-only", action="store_true", help="evaluate the model file --out without training")
     a = ap.parse_args(argv)
     opts = {"pair_precision": a.pair_precision}
+    if a.eval_only:
+        ws = W.WarmStart.load(a.out)
+        items = [W.draw_evaluation_packing(s, a.eval_n) for s in range(a.eval_count)]
+        out = {"model": str(a.out), "eval": W.evaluate(ws, items, opts, a.eval_concurrency)}
+        out["eval"]["N"] = a.eval_n
+        print(json.dumps(out))
+        return out
     t0 = time.perf_counter()
     if a.data:
         z = np.load(a.data)
