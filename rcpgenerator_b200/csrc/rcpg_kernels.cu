@@ -325,12 +325,16 @@ __global__ void __launch_bounds__(256) k_build_cell_sort(DevArrays a) {
 
 // Warp search (every build the tiled search does not take: ndim > 3, small
 // packings, grids narrower than a tile). One warp per row slot t (particle
-// work[t]); its lanes share the 3^ndim neighbour cells, test every member
-// against the reference's shell predicate, and collect the partners in shared
-// memory; the row is then sorted ascending by a bitonic sort in the warp, so
-// it does not depend on the order in which the lanes found its entries.
+// work[t]). The neighbour cells are taken 32 at a time: each lane reads one
+// cell's member range, a warp scan numbers the chunk's candidates, and the
+// lanes test consecutive candidates (each finds its cell by a binary search
+// over the lanes' ranges), so every lane has a candidate in every round
+// whatever the cell occupancy. Accepted partners take row slots in candidate
+// order (ballot + popc): the row is in a fixed scan order. Rows that must be
+// sorted (sorted_rows: exact mode) are then sorted ascending by a bitonic
+// sort in the warp.
 constexpr int kWarpSearchWarps = 4;    // warps per block
-constexpr int kWarpRowSmem = 256;      // row entries sorted in shared memory
+constexpr int kWarpRowSmem = 256;      // row entries held (and sorted) in shared memory
 
 template <int ND>
 __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArrays a) {
@@ -339,7 +343,6 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
     if (build_off(ctl) | use_tiled<ND>(ctl, N)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->forces_done = 0u;
     __shared__ std::uint32_t buf[kWarpSearchWarps][kWarpRowSmem];
-    __shared__ std::uint32_t cnt[kWarpSearchWarps];
     __shared__ std::uint32_t block_need;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (threadIdx.x == 0) block_need = 0u;
@@ -361,9 +364,7 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
         double xi[ND], D0i;
         load_pos<ND>(a.spos, t, xi, D0i);
         const double Di = xmul(D0i, kap);
-        if (lane == 0) cnt[w] = 0u;
-        __syncwarp();
-        std::uint32_t n_half = 0;
+        std::uint32_t n = 0, n_half = 0;  // n: warp-uniform row length so far
         // every grid: cells within the largest cutoff of particle i and a member
         // of the class (one cell for its own and smaller classes, more for
         // classes of smaller particles than i, whose cells are narrower)
@@ -394,38 +395,74 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
                 total_combo *= nn[d];
             }
             const std::uint32_t base = ctl->cls_base[kc];
-            for (int combo = lane; combo < total_combo; combo += 32) {
-                std::uint32_t cell = base, mul = 1;
-                int r = combo;
-                RCPG_UNROLL
-                for (int d = 0; d < ND; ++d) {
-                    const int kk = r % nn[d];
-                    r /= nn[d];
-                    int c = lo[d] + kk;
-                    if (c < 0) c += nc[d];
-                    else if (c >= nc[d]) c -= nc[d];
-                    cell += static_cast<std::uint32_t>(c) * mul;
-                    mul *= static_cast<std::uint32_t>(nc[d]);
+            for (int cb = 0; cb < total_combo; cb += 32) {
+                // this lane's cell of the chunk and its member range
+                const int combo = cb + lane;
+                std::uint32_t q0 = 0, cntc = 0;
+                if (combo < total_combo) {
+                    std::uint32_t cell = base, mul = 1;
+                    int r = combo;
+                    RCPG_UNROLL
+                    for (int d = 0; d < ND; ++d) {
+                        const int kk = r % nn[d];
+                        r /= nn[d];
+                        int c = lo[d] + kk;
+                        if (c < 0) c += nc[d];
+                        else if (c >= nc[d]) c -= nc[d];
+                        cell += static_cast<std::uint32_t>(c) * mul;
+                        mul *= static_cast<std::uint32_t>(nc[d]);
+                    }
+                    q0 = a.cell_start[cell];
+                    cntc = a.cell_start[cell + 1] - q0;
                 }
-                const std::uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
-                for (std::uint32_t q = q0; q < q1; ++q) {
-                    const std::uint32_t j = a.work[q];
-                    if (j == i) continue;
-                    double xj[ND], D0j;
-                    load_pos<ND>(a.spos, q, xj, D0j);
-                    const double Dj = xmul(D0j, kap);
-                    const bool ok = (ND <= 3 || j > i) ? in_shell<ND>(xi, xj, Di, Dj, bx, ibx, t_shell)
-                                                       : in_shell<ND>(xi, xj, Dj, Di, bx, ibx, t_shell);
-                    if (!ok) continue;
-                    const std::uint32_t slot = atomicAdd(&cnt[w], 1u);
-                    if (slot < static_cast<std::uint32_t>(kWarpRowSmem)) row[slot] = j;
-                    else if (slot < S) a.nbr[static_cast<std::uint64_t>(slot) * N + t] = j;
-                    if (j > i) ++n_half;
+                // inclusive scan of the member counts over the lanes
+                std::uint32_t incl = cntc;
+                RCPG_UNROLL
+                for (int o = 1; o < 32; o <<= 1) {
+                    const std::uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const std::uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+                for (std::uint32_t k0 = 0; k0 < tot; k0 += 32) {
+                    const std::uint32_t k = k0 + lane;
+                    bool ok = false;
+                    std::uint32_t j = 0;
+                    // owner lane of candidate k: the first lane whose inclusive
+                    // count exceeds k (5-step search over the lanes)
+                    int s_lo = 0;
+                    RCPG_UNROLL
+                    for (int step = 16; step > 0; step >>= 1) {
+                        const std::uint32_t v = __shfl_sync(0xffffffffu, incl, s_lo + step - 1);
+                        if (v <= k) s_lo += step;
+                    }
+                    const int own = s_lo < 31 ? s_lo : 31;
+                    const std::uint32_t own_q0 = __shfl_sync(0xffffffffu, q0, own);
+                    const std::uint32_t own_incl = __shfl_sync(0xffffffffu, incl, own);
+                    const std::uint32_t own_cnt = __shfl_sync(0xffffffffu, cntc, own);
+                    if (k < tot) {
+                        const std::uint32_t q = own_q0 + (k - (own_incl - own_cnt));
+                        j = a.work[q];
+                        if (j != i) {
+                            double xj[ND], D0j;
+                            load_pos<ND>(a.spos, q, xj, D0j);
+                            const double Dj = xmul(D0j, kap);
+                            ok = (ND <= 3 || j > i) ? in_shell<ND>(xi, xj, Di, Dj, bx, ibx, t_shell)
+                                                    : in_shell<ND>(xi, xj, Dj, Di, bx, ibx, t_shell);
+                        }
+                    }
+                    // row slots in candidate order
+                    const unsigned mask = __ballot_sync(0xffffffffu, ok);
+                    if (ok) {
+                        const std::uint32_t slot = n + __popc(mask & ((1u << lane) - 1u));
+                        if (slot < static_cast<std::uint32_t>(kWarpRowSmem)) row[slot] = j;
+                        else if (slot < S) a.nbr[static_cast<std::uint64_t>(slot) * N + t] = j;
+                        if (j > i) ++n_half;
+                    }
+                    n += static_cast<std::uint32_t>(__popc(mask));
                 }
             }
         }
         __syncwarp();
-        const std::uint32_t n = cnt[w];
         RCPG_UNROLL
         for (int o = 16; o > 0; o >>= 1) n_half += __shfl_xor_sync(0xffffffffu, n_half, o);
         if (lane == 0) {
@@ -438,7 +475,11 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
             a.nbr_cnt[t] = n > S ? 0u : n;  // overflow: empty row, rebuilt after the capacity grows
         }
         if (n > S) continue;
-        if (n <= static_cast<std::uint32_t>(kWarpRowSmem)) {
+        if (!a.sorted_rows) {
+            // scan-order row: the shared part goes out as it is
+            const std::uint32_t ns = n < static_cast<std::uint32_t>(kWarpRowSmem) ? n : kWarpRowSmem;
+            for (std::uint32_t e = lane; e < ns; e += 32) a.nbr[static_cast<std::uint64_t>(e) * N + t] = row[e];
+        } else if (n <= static_cast<std::uint32_t>(kWarpRowSmem)) {
             // bitonic sort of the row padded to a power of two
             std::uint32_t p2 = 1;
             while (p2 < n) p2 <<= 1;
