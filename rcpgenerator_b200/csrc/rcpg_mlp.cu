@@ -268,6 +268,8 @@ int32_t rcpg_mlp_train_step(const int32_t* widths, int32_t layers, int32_t batch
                             char* err, size_t errlen) {
     if (!widths || layers <= 0 || batch <= 0 || !w_fp32 || !w_bf16 || !grad || !X || !T || !workspace)
         return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: bad arguments to rcpg_mlp_train_step");
+    if (adam_m && adam_v && lr > 0.0f && step < 1)
+        return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: the Adam step counter starts at 1");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     Work wk;
     if (!carve(workspace, workspace_bytes, widths, layers, batch, wk))
