@@ -177,6 +177,14 @@ void rcpg_result_free(rcpg_result* r);
 int32_t rcpg_run_batch(const rcpg_packing_input* inputs, uint64_t count, const rcpg_run_options* opt,
                        int32_t concurrency, rcpg_result** results, int32_t* status, char* err,
                        size_t errlen);
+/* Autotuned launch shape of the persistent batch kernel for packings of
+ * `ndim` (pair_precision as in rcpg_run_options): the same synthetic batch is
+ * timed at 1 and 2 resident blocks per SM (steps_per_s[2], packing-steps per
+ * second) and the faster is kept for the process (*blocks_per_sm). Runs the
+ * tuning on first use; rcpg_run_batch uses it when every packing goes to the
+ * persistent kernel. No counterpart in the reference. */
+int32_t rcpg_batch_tuning(int32_t ndim, int32_t device, int32_t pair_precision, int32_t* blocks_per_sm,
+                          double* steps_per_s, char* err, size_t errlen);
 /* rcpg_run_batch with a growth-rung length per packing (growth_steps[k],
  * 0 = the reference's deadline), overriding opt->growth_steps: the batch form
  * of a learned warm start. No counterpart in the reference. */

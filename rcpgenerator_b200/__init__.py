@@ -8,6 +8,7 @@ hand-written sm_100a CUDA kernels behind a C ABI (include/rcpg.h).
 
 from ._api import (
     PackingEngine,
+    batch_tuning,
     get_num_threads,
     initialize_particles,
     run_packing,
@@ -20,6 +21,7 @@ from ._wrapper import Packing
 __all__ = [
     "Packing",
     "PackingEngine",
+    "batch_tuning",
     "get_num_threads",
     "initialize_particles",
     "run_packing",

@@ -335,6 +335,19 @@ def run_packing_batch(items: list, options: dict | None = None, concurrency: int
                 N.lib.rcpg_result_free(r)
 
 
+def batch_tuning(ndim: int, device: int = 0, pair_precision: str = "f64") -> dict:
+    """The persistent batch kernel's autotuned launch shape for packings of
+    `ndim` (tuned on first use): blocks per SM and the packing-steps per second
+    measured at 1 and 2 blocks per SM."""
+    b = C.c_int32(0)
+    r = (C.c_double * 2)()
+    err = N.errbuf()
+    rc = N.lib.rcpg_batch_tuning(int(ndim), int(device), 1 if pair_precision == "mixed" else 0, C.byref(b), r,
+                                 err, len(err))
+    N.raise_for(rc, err)
+    return {"blocks_per_sm": int(b.value), "steps_per_s": [float(r[0]), float(r[1])]}
+
+
 class PackingEngine:
     """One packing advanced in slices of steps (rcpg_engine_* of the C ABI).
 

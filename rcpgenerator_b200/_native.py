@@ -30,6 +30,7 @@ EXPORTED_SYMBOLS = (
     "rcpg_result_free",
     "rcpg_run_batch",
     "rcpg_run_batch_growth",
+    "rcpg_batch_tuning",
     "rcpg_engine_create",
     "rcpg_engine_advance",
     "rcpg_engine_steps",
@@ -191,6 +192,9 @@ def _load() -> C.CDLL:
              OBSERVER, vp, C.POINTER(C.POINTER(Result)), cp, sz],
         ),
         "rcpg_result_free": (None, [C.POINTER(Result)]),
+        "rcpg_batch_tuning": (
+            C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), _dp, cp, sz]
+        ),
         "rcpg_run_batch_growth": (
             C.c_int32,
             [C.POINTER(PackingInput), C.c_uint64, C.POINTER(RunOptions), _u64p, C.c_int32,

@@ -15,6 +15,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -987,6 +991,55 @@ std::vector<std::uint32_t> run_group(const std::vector<EngineInput>& ins, const 
 
 }  // namespace
 
+namespace {
+constexpr std::uint64_t kTunePackingN = 256;
+constexpr std::uint64_t kTuneSteps = 200;
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, BatchTuning> g_tuned;
+}  // namespace
+
+BatchTuning tune_batch(int ndim, int device, bool mixed) {
+    const auto key = std::make_tuple(device, ndim, mixed ? 1 : 0);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) return it->second;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    std::vector<EngineInput> ins(static_cast<std::size_t>(2 * sms));
+    std::uint64_t rng = 0x9E3779B97F4A7C15ull;
+    for (std::size_t k = 0; k < ins.size(); ++k) {
+        EngineInput& e = ins[k];
+        e.N = kTunePackingN;
+        e.ndim = ndim;
+        e.positions.resize(kTunePackingN * ndim);
+        for (double& v : e.positions) {  // xorshift uniforms in [0, 1)
+            rng ^= rng << 13;
+            rng ^= rng >> 7;
+            rng ^= rng << 17;
+            v = static_cast<double>(rng >> 11) * (1.0 / 9007199254740992.0);
+        }
+        e.diameters.assign(kTunePackingN, 1.0);
+        e.max_steps = kTuneSteps;
+        e.device = device;
+        e.pair_precision = mixed ? 1 : 0;
+    }
+    BatchTuning t;
+    for (int b = 1; b <= 2; ++b) {
+        const auto t0 = std::chrono::steady_clock::now();
+        const std::vector<BatchOutcome> r = run_batch_persistent(ins, 2048u, b);
+        const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::uint64_t steps = 0;
+        for (const BatchOutcome& o : r) steps += o.code == 0 ? o.result.steps : 0;
+        t.steps_per_s[b - 1] = s > 0.0 ? static_cast<double>(steps) / s : 0.0;
+    }
+    t.blocks_per_sm = t.steps_per_s[1] > t.steps_per_s[0] ? 2 : 1;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = t;
+    return t;
+}
+
 std::vector<BatchOutcome> run_batch_persistent(const std::vector<EngineInput>& ins, std::uint32_t chunk,
                                                int blocks_per_sm) {
     std::vector<BatchOutcome> out(ins.size());
@@ -1020,7 +1073,9 @@ std::vector<BatchOutcome> run_batch_persistent(const std::vector<EngineInput>& i
                 for (std::size_t k : pending)
                     if (su[k].ndim == nd) grp.push_back(k);
                 if (grp.empty()) continue;
-                const std::vector<std::uint32_t> st_k = run_group(ins, su, grp, mult, chunk, blocks_per_sm, st, out);
+                const int bps = blocks_per_sm > 0 ? blocks_per_sm
+                                                  : tune_batch(nd, ins[0].device, ins[0].pair_precision == 1).blocks_per_sm;
+                const std::vector<std::uint32_t> st_k = run_group(ins, su, grp, mult, chunk, bps, st, out);
                 for (std::size_t q = 0; q < grp.size(); ++q) {
                     const std::size_t k = grp[q];
                     if (st_k[q] == 2u) continue;

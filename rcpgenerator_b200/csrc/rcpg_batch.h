@@ -54,11 +54,25 @@ struct BatchOutcome {
 };
 
 // Runs every packing to completion in persistent launches of at most `chunk`
-// steps per packing, with at most `blocks_per_sm` resident blocks per SM. All
-// share the run options of `ins[k]` (graph engine; packings that can reach a
-// target-phi lock are reported as unsupported).
+// steps per packing, with at most `blocks_per_sm` resident blocks per SM
+// (0: the autotuned value of each ndim, tune_batch). All share the run
+// options of `ins[k]` (graph engine; packings that can reach a target-phi
+// lock are reported as unsupported).
 std::vector<BatchOutcome> run_batch_persistent(const std::vector<EngineInput>& ins, std::uint32_t chunk,
                                                int blocks_per_sm);
+
+// Launch-shape autotuner of the persistent batch kernel for one (device,
+// ndim, pair precision): the same synthetic batch -- two packings per SM of
+// kTunePackingN particles, uniform positions, mono diameters, capped at
+// kTuneSteps steps -- runs at 1 and at 2 resident blocks per SM, and the
+// faster (packing-steps per second) is kept for the process. A result does
+// not depend on the launch shape (each packing runs in one block of fixed
+// size), so the choice only moves time.
+struct BatchTuning {
+    int blocks_per_sm = 1;
+    double steps_per_s[2] = {0.0, 0.0};  // at 1 and 2 blocks per SM
+};
+BatchTuning tune_batch(int ndim, int device, bool mixed);
 
 // Work of one build step of a packing in the persistent kernel, in candidate
 // tests (N x 3^ndim x members per cell): the batch sends the packings above a

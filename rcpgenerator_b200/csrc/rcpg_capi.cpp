@@ -322,7 +322,7 @@ int32_t run_batch_impl(const rcpg_packing_input* inputs, uint64_t count, const r
                 ins.reserve(persistent.size());
                 for (uint64_t k : persistent) ins.push_back(input_of(k));
                 const std::vector<rcpg::BatchOutcome> res =
-                    rcpg::run_batch_persistent(ins, 2048u, on_streams.empty() ? 2 : 1);
+                    rcpg::run_batch_persistent(ins, 2048u, on_streams.empty() ? 0 : 1);
                 for (std::size_t q = 0; q < persistent.size(); ++q) {
                     const uint64_t k = persistent[q];
                     const rcpg::BatchOutcome& b = res[q];
@@ -390,6 +390,25 @@ int32_t rcpg_run_batch_growth(const rcpg_packing_input* inputs, uint64_t count, 
                               const uint64_t* growth_steps, int32_t concurrency, rcpg_result** results,
                               int32_t* status, char* err, size_t errlen) {
     return run_batch_impl(inputs, count, opt, growth_steps, concurrency, results, status, err, errlen);
+}
+
+int32_t rcpg_batch_tuning(int32_t ndim, int32_t device, int32_t pair_precision, int32_t* blocks_per_sm,
+                          double* steps_per_s, char* err, size_t errlen) {
+    if (ndim < 2 || ndim > rcpg::kMaxDim)
+        return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: Ndim must be in [2, 8]");
+    if (!have_device(err, errlen)) return RCPG_ECUDA;
+    try {
+        cuda_ok(cudaSetDevice(device), "cudaSetDevice");
+        const rcpg::BatchTuning t = rcpg::tune_batch(ndim, device, pair_precision == 1);
+        if (blocks_per_sm) *blocks_per_sm = t.blocks_per_sm;
+        if (steps_per_s) {
+            steps_per_s[0] = t.steps_per_s[0];
+            steps_per_s[1] = t.steps_per_s[1];
+        }
+        return RCPG_OK;
+    } catch (const std::exception& e) {
+        return fail(err, errlen, classify(e), e.what());
+    }
 }
 
 void rcpg_result_free(rcpg_result* r) {

@@ -142,3 +142,12 @@ def test_persistent_batch_config1_phiJ_distribution_64_seeds(cuda_device, golden
     assert abs(phis.mean() - g["phi"].mean()) <= 1e-3
     assert abs(steps.mean() - g["steps"].mean()) <= 0.05 * g["steps"].mean()
     assert (np.asarray([r["max_min_dist"] for r in out]) < 5e-4).all()
+
+
+def test_batch_autotuner_picks_the_faster_measured_shape(cuda_device):
+    import rcpgenerator_b200 as rb
+    t = rb.batch_tuning(3, pair_precision="mixed")
+    assert t["blocks_per_sm"] in (1, 2)
+    assert min(t["steps_per_s"]) > 0.0
+    assert t["steps_per_s"][t["blocks_per_sm"] - 1] == max(t["steps_per_s"])
+    assert rb.batch_tuning(3, pair_precision="mixed") == t  # kept for the process
