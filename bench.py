@@ -277,6 +277,32 @@ def run_batch_workload(args) -> int:
     return 0
 
 
+def run_one_packing(args) -> int:
+    """ADAM steps/s of one packing of the batched workload's generator (seed
+    --seed), graph engine: 300 untimed steps, then --steps timed (host wall
+    clock around PackingEngine.advance, which ends in a device sync). For
+    profiling the engines that run a batch's large packings."""
+    import rcpgenerator_b200 as rb
+    from rcpgenerator_b200.warmstart import draw_packing
+    rank, _, local = dist_env()
+    inp, cfg = draw_packing(args.seed)
+    cfg.update({"pair_precision": args.pair_precision, "device": local})
+    eng = rb.PackingEngine(inp, cfg, {})
+    eng.advance(300)
+    steps = max(args.steps, 1) * 10
+    t0 = time.perf_counter()
+    eng.advance(steps)
+    dt = time.perf_counter() - t0
+    done = eng.steps - 300
+    n, nd = inp["positions"].shape
+    if rank == 0:
+        print(json.dumps({"metric": "ADAM steps/s", "value": done / dt, "unit": "ADAM steps/s",
+                          "steps": done, "config": {"workload": f"batch_generator_seed{args.seed}_{nd}d_N{n}",
+                                                    "pair_precision": args.pair_precision}}))
+    eng.close()
+    return 0
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -319,8 +345,10 @@ def main() -> int:
                     help="pair arithmetic: mixed = FP32 pair terms while the max overlap >= 1e-5 "
                          "(the workload's stated precision), f64 = FP64 throughout")
     ap.add_argument("--n", type=int, default=WORKLOAD["N"], help="particles (smaller cases for profiling)")
-    ap.add_argument("--workload", default="single", choices=["single", "batch"],
-                    help="single: ADAM steps/s of one N=1M packing; batch: packings/hour of many small ones")
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "one"],
+                    help="single: ADAM steps/s of one N=1M packing; batch: packings/hour of many small ones; "
+                         "one: ADAM steps/s of packing --seed of the batch generator (profiling)")
+    ap.add_argument("--seed", type=int, default=4, help="one: generator seed (4: 4-D, N = 11,948)")
     ap.add_argument("--batch-count", type=int, default=128)
     ap.add_argument("--batch-single", type=int, default=8, help="packings timed one at a time")
     ap.add_argument("--concurrency", type=int, default=0,
@@ -332,6 +360,8 @@ def main() -> int:
         return run_reference_arm(args)
     if args.workload == "batch":
         return run_batch_workload(args)
+    if args.workload == "one":
+        return run_one_packing(args)
 
     import torch
     import torch.distributed as dist
