@@ -31,9 +31,10 @@ def overlap_pairs(pos, D, box=None, chunk=512):
     for i0 in range(0, N, chunk):
         i1 = min(N, i0 + chunk)
         delta = pos[i0:i1, None, :] - pos[None, :, :]
-        if L is not None:
-            delta = delta - np.round(delta / L) * L
-        dist = np.sqrt(np.sum(delta * delta, axis=2))
+        with np.errstate(divide="ignore", invalid="ignore"):  # a zero box side gives NaN, as in the reference
+            if L is not None:
+                delta = delta - np.round(delta / L) * L
+            dist = np.sqrt(np.sum(delta * delta, axis=2))
         ii, jj = np.meshgrid(np.arange(i0, i1), np.arange(N), indexing="ij")
         upper = jj > ii
         cand = upper & (dist <= rq)

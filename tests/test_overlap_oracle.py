@@ -54,3 +54,27 @@ def test_job_preparation_leaves_the_job_unchanged():
     s2, D2, p2, r2 = jobs._prepare_job(job)
     np.testing.assert_array_equal(D1, D2)
     assert r1 is None and np.allclose(sorted(p1.diameters), sorted(p2.diameters))
+
+
+def test_prescreen_and_safe_phi():
+    """The job loop's geometric pre-screen (jobs.py:137-143) and the sanity
+    checked phi of a state (rcptools/_helpers.py:30-77)."""
+    from rcpgenerator_b200 import jobs
+    d = np.ones(40)
+    d[0] = 60.0
+    rej, dmax, L = jobs._prescreen_reject(d, 2, 0.85, 2.5)
+    V = np.pi / 4 * (39 + 3600)
+    assert rej and dmax == 60.0 and L == pytest.approx(np.sqrt(V / 0.85))
+    assert not jobs._prescreen_reject(np.ones(40), 2, 0.85, 2.5)[0]
+
+    class S:
+        positions = np.array([[0.1, 0.2], [0.5, 0.9]])
+        diameters = np.array([0.2, 0.2])
+        box = np.array([1.0, 1.0])
+        walls = [0, 0]
+    assert jobs._safe_phi(S()) == pytest.approx(2 * np.pi * 0.01)
+    S.positions = np.array([[0.1, 0.2], [0.5, 1.1]])  # outside the box
+    assert jobs._safe_phi(S()) == 0.0
+    S.positions = np.array([[0.1, 0.2], [0.5, 0.5]])
+    S.walls = [-2, -1]  # disk container: phi relative to its area
+    assert jobs._safe_phi(S()) == pytest.approx(2 * np.pi * 0.01 / (np.pi / 4))
