@@ -229,8 +229,11 @@ extern "C" int32_t rcpg_overlap_report(uint64_t N, int32_t ndim, const double* p
             for (int d = 0; d < ndim; ++d) {
                 double v = positions[i * ndim + d] - g.lo[d];
                 if (box) v -= std::floor(v / box[d]) * box[d];
-                long long k = static_cast<long long>(std::floor(v / g.width[d]));
-                k = std::min<long long>(std::max<long long>(k, 0), g.ncell[d] - 1);
+                // cell index, clamped (a NaN from a zero box side goes to cell 0)
+                const double q = std::floor(v / g.width[d]);
+                long long k = 0;
+                if (q >= static_cast<double>(g.ncell[d] - 1)) k = g.ncell[d] - 1;
+                else if (q > 0.0) k = static_cast<long long>(q);
                 c += static_cast<std::uint32_t>(k) * mul;
                 mul *= static_cast<std::uint32_t>(g.ncell[d]);
             }
