@@ -78,3 +78,18 @@ def test_prescreen_and_safe_phi():
     S.positions = np.array([[0.1, 0.2], [0.5, 0.5]])
     S.walls = [-2, -1]  # disk container: phi relative to its area
     assert jobs._safe_phi(S()) == pytest.approx(2 * np.pi * 0.01 / (np.pi / 4))
+
+
+def test_custom_packing_preparation():
+    """run_one_custom_packing's preparation (jobs.py:34-134): a dilute mono
+    initialisation, then the caller's diameters (non-finite dropped, floored
+    at 1e-12) scaled so that the realised phi is phi_init."""
+    from rcpgenerator_b200 import jobs
+    d = np.array([1.0, 2.0, np.nan, 1.5, np.inf] + [1.0] * 60)
+    p = jobs.prepare_custom_packing(d, seed=5, Ndim=3, phi_init=0.3, initializer_phi=0.05)
+    D = np.asarray(p.diameters)
+    assert len(D) == 63 and p.N == 63
+    vol = np.sum(np.pi / 6 * D ** 3) / np.prod(p.box)
+    assert vol == pytest.approx(0.3, rel=1e-12)
+    np.testing.assert_allclose(D / D[0], np.array([1.0, 2.0, 1.5] + [1.0] * 60), rtol=1e-14)
+    assert p.needs_pack and not p.needs_initialize and np.asarray(p.positions).shape == (63, 3)
