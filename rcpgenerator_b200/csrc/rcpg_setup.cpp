@@ -54,16 +54,16 @@ std::vector<double> scale_diameters_nd(const std::vector<double>& D, double phi_
     // sphere_volume(Di * 0.5, ndim) per particle, its constant factors
     // evaluated once (same operations in the same order), summed in order
     const double c_pi = std::pow(kPi, ndim / 2.0), c_gamma = std::tgamma(ndim / 2.0 + 1.0);
-    std::vector<double> vol(D.size());
+    // the volumes go through the output buffer, which then takes the scaled diameters
+    std::vector<double> out(D.size());
     parallel_for(D.size(), [&](std::size_t i) {
-        vol[i] = c_pi * std::pow(D[i] * 0.5, static_cast<double>(ndim)) / c_gamma;
+        out[i] = c_pi * std::pow(D[i] * 0.5, static_cast<double>(ndim)) / c_gamma;
     });
     double sumVol = 0.0;
-    for (double v : vol) sumVol += v;
+    for (double v : out) sumVol += v;
     const double factor = fix_height ? std::pow(phi_target * V_box / sumVol, 1.0 / double(ndim - 1))
                                      : std::pow(phi_target * V_box / sumVol, 1.0 / double(ndim));
-    std::vector<double> out = D;
-    for (double& v : out) v *= factor;
+    parallel_for(D.size(), [&](std::size_t i) { out[i] = D[i] * factor; });
     if (factor_out) *factor_out = factor;
     return out;
 }
@@ -198,8 +198,8 @@ RunSetup prepare_run(const EngineInput& in) {
     if (nd == 4) alpha = alpha_max = 0.0035;
     if (nd >= 5) alpha = alpha_max = 0.0025;
 
-    // D0 statistics (ENG:4800-4838)
-    out.D0 = D;
+    // D0 statistics (ENG:4800-4838); D is not used after this point
+    out.D0 = std::move(D);
     const std::vector<double>& D0_ = out.D0;
     double D0min = D0_[0], S = 0.0, D0max = 0.0;
     for (std::size_t i = 0; i < N; ++i) {

@@ -57,3 +57,26 @@ def test_scale_diameters_host(native):
     vol = (np.pi / 4 * out ** 2).sum()
     assert abs(vol - 0.5) < 1e-12
     assert np.allclose(out, D * f, rtol=0, atol=0)
+
+
+def test_scale_diameters_host_large_is_the_sequential_result(native):
+    """Above 65,536 particles the per-particle volumes are computed on several
+    host threads; they are summed in index order, so the result equals the
+    one-thread restatement bit for bit."""
+    import math
+    rng = np.random.default_rng(9)
+    n, nd = 100_000, 3
+    D = rng.uniform(0.5, 1.5, n)
+    out = np.zeros(n)
+    dp = C.POINTER(C.c_double)
+    box = np.array([1.0, 1.3, 0.9])
+    f = native.lib.rcpg_scale_diameters_nd(D.ctypes.data_as(dp), n, 0.33, box.ctypes.data_as(dp), nd, 0,
+                                           out.ctypes.data_as(dp))
+    c_pi, c_gamma = math.pow(math.pi, nd / 2.0), math.gamma(nd / 2.0 + 1.0)
+    s = 0.0
+    for d in D.tolist():
+        s += c_pi * math.pow(d * 0.5, float(nd)) / c_gamma
+    v_box = 1.0 * 1.3 * 0.9
+    factor = math.pow(0.33 * v_box / s, 1.0 / nd)
+    assert f == factor
+    np.testing.assert_array_equal(out, D * factor)
