@@ -223,16 +223,23 @@ int32_t fail(char* err, std::size_t errlen, int32_t code, const char* msg) {
     return code;
 }
 
+bool widths_ok(const int32_t* w, int L) {
+    if (!w || L <= 0) return false;
+    for (int l = 0; l <= L; ++l)
+        if (w[l] <= 0 || w[l] > (1 << 20)) return false;
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
 
 uint64_t rcpg_mlp_param_count(const int32_t* widths, int32_t layers) {
-    return widths && layers > 0 ? param_count(widths, layers) : 0;
+    return widths_ok(widths, layers) ? param_count(widths, layers) : 0;
 }
 
 uint64_t rcpg_mlp_workspace_bytes(const int32_t* widths, int32_t layers, int32_t batch) {
-    if (!widths || layers <= 0 || batch <= 0) return 0;
+    if (!widths_ok(widths, layers) || batch <= 0) return 0;
     int wmax = 0;
     std::size_t b = 0;
     for (int l = 0; l <= layers; ++l) {
@@ -247,7 +254,7 @@ uint64_t rcpg_mlp_workspace_bytes(const int32_t* widths, int32_t layers, int32_t
 int32_t rcpg_mlp_forward(const int32_t* widths, int32_t layers, int32_t batch, const void* w_bf16,
                          const float* w_fp32, const float* X, float* Y, void* workspace,
                          uint64_t workspace_bytes, void* stream, char* err, size_t errlen) {
-    if (!widths || layers <= 0 || batch <= 0 || !w_bf16 || !w_fp32 || !X || !Y || !workspace)
+    if (!widths_ok(widths, layers) || batch <= 0 || !w_bf16 || !w_fp32 || !X || !Y || !workspace)
         return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: bad arguments to rcpg_mlp_forward");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     Work wk;
@@ -266,7 +273,7 @@ int32_t rcpg_mlp_train_step(const int32_t* widths, int32_t layers, int32_t batch
                             const float* T, const float* out_weight, float lr, int32_t step,
                             float* loss_terms, void* workspace, uint64_t workspace_bytes, void* stream,
                             char* err, size_t errlen) {
-    if (!widths || layers <= 0 || batch <= 0 || !w_fp32 || !w_bf16 || !grad || !X || !T || !workspace)
+    if (!widths_ok(widths, layers) || batch <= 0 || !w_fp32 || !w_bf16 || !grad || !X || !T || !workspace)
         return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: bad arguments to rcpg_mlp_train_step");
     if (adam_m && adam_v && lr > 0.0f && step < 1)
         return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: the Adam step counter starts at 1");

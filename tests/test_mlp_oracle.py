@@ -79,3 +79,18 @@ def test_bf16_emulation_is_close_to_fp64():
     _, g64 = mo.loss_and_grad(p, WIDTHS, X, T, w)
     _, g16 = mo.loss_and_grad(p, WIDTHS, X, T, w, bf16=True)
     assert np.linalg.norm(g16 - g64) / np.linalg.norm(g64) < 3e-2
+
+
+def test_mlp_abi_sizes_on_the_host():
+    """Parameter count and workspace size of the C ABI (host functions) agree
+    with the oracle's layout; invalid widths give 0."""
+    import ctypes as C
+    from rcpgenerator_b200 import _native as N
+    w = (C.c_int32 * 5)(11, 256, 256, 256, 17)
+    assert N.lib.rcpg_mlp_param_count(w, 4) == mo.param_count((11, 256, 256, 256, 17)) == 139025
+    ws = N.lib.rcpg_mlp_workspace_bytes(w, 4, 256)
+    # activations (BF16) + pre-activations (FP32) + gradient scratch + loss terms
+    need = 256 * (2 * (11 + 3 * 256 + 17) + 4 * (3 * 256 + 17) + 8 * 256 + 4 * 17)
+    assert need <= ws <= need + 256 * 16
+    assert N.lib.rcpg_mlp_param_count((C.c_int32 * 3)(4, 0, 2), 2) == 0
+    assert N.lib.rcpg_mlp_workspace_bytes(w, 4, 0) == 0
