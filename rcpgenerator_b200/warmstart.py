@@ -6,7 +6,7 @@ shortens the growth rung of the reference's schedule (mu_flag = 1, the first
 6000 + 9 sqrt(N ndim) steps, rcp_generator.cpp:5834-5931) to the step at which
 the predicted curve has reached phi_J. The rest of the run -- mu decay,
 oscillation, and the unchanged overlap / force convergence gate -- is the
-plain method's, so every warm-started packing is still judged by the engine's
+plain method's, so every warm-started packing still ends by the engine's
 own criterion; the time saved is in the rung, whose length also sets the
 oscillation period that follows it.
 
