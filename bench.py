@@ -124,48 +124,45 @@ def make_input(rank: int):
     return pos, dia, init
 
 
-def reference_sample(pos, dia, box, walls, steps: int, threads: int):
+def reference_sample(pos, dia, box, walls, warmup: int, steps: int, threads: int):
     """The reference engine (oracle/_ref, compiled from the reference sources)
-    on the same input, timed per step through its own observer callback."""
-    ref_dir = REPO / "oracle" / "_ref"
-    if not any(ref_dir.glob("_rcpgenerator*.so")):
+    on the same input, run to step warmup + steps and timed by its own
+    observer callback from the end of step `warmup` (>= 1) to the end of step
+    warmup + steps: the same window as the GPU arm's."""
+    ref = reference_module()
+    if ref is None:
         return None, "reference build oracle/_ref missing"
-    sys.path.insert(0, str(ref_dir))
-    for k in list(os.environ):
-        if k.startswith("RCP_"):
-            del os.environ[k]
-    import _rcpgenerator as ref
     ref.set_num_threads(threads)
-    stamps = []
+    stamps = {}
 
     def cb(update):
-        stamps.append((int(update["step"]), time.perf_counter()))
+        stamps[int(update["step"])] = time.perf_counter()
 
+    w = max(1, warmup)
     t0 = time.perf_counter()
     ref.run_packing_observed({"positions": pos.tolist(), "diameters": dia.tolist()},
                              {"box": box, "walls": walls, "neighbor_max": 0, "seed": 0},
-                             1, False, 0, cb, {"max_steps": steps + 1})
+                             1, False, 0, cb, {"max_steps": w + steps})
     t1 = time.perf_counter()
-    st = [t for s, t in stamps if 1 <= s <= steps + 1]
-    if len(st) < 2:
+    if w not in stamps or w + steps not in stamps:
         return None, "reference produced no step timings"
-    per = (st[-1] - st[0]) / (len(st) - 1)
-    return {"steps_per_s": 1.0 / per, "timed_steps": len(st) - 1, "setup_s": stamps[0][1] - t0
-            if stamps else None, "wall_s": t1 - t0}, None
+    per = (stamps[w + steps] - stamps[w]) / steps
+    return {"steps_per_s": 1.0 / per, "timed_steps": steps, "first": w + 1, "last": w + steps,
+            "wall_s": t1 - t0}, None
 
 
 # ---- batched workload: many independent small packings (packings/hour) ----
 BATCH_METRIC = "packings/hour"
 
 
-def batch_instances(count: int, seed0: int = 0):
+def batch_instances(seeds):
     """Independent packings drawn like the batched workload: N log-uniform on
     [64, 16384], ndim from {2, 3, 4}, diameters mono (d=1), bidisperse 50:50
     with ratio uniform on [1.1, 3.0], or log-normal with std/mean uniform on
     [0.1, 0.6] truncated to [0.2, 5] x mean; periodic unit boxes at phi 0.10;
-    seeds seed0.. (rcpgenerator_b200.warmstart.draw_packing)."""
+    one packing per seed (rcpgenerator_b200.warmstart.draw_packing)."""
     from rcpgenerator_b200.warmstart import draw_packing
-    return [draw_packing(seed0 + k) for k in range(count)]
+    return [draw_packing(int(s)) for s in seeds]
 
 
 def _ref_capped(args_):
@@ -201,7 +198,11 @@ def reference_batch_rate(items, cap: int, procs: int):
 def run_batch_workload(args) -> int:
     import rcpgenerator_b200 as rb
     rank, world, local = dist_env()
-    items = batch_instances(args.batch_count, seed0=rank * args.batch_count)
+    # a stratified sample of the generator's seeds 0..4095 (every stride-th),
+    # the ranks taking interleaved seeds
+    stride = args.batch_stride or max(1, 4096 // max(1, args.batch_count * world))
+    seeds = [(k * world + rank) * stride for k in range(args.batch_count)]
+    items = batch_instances(seeds)
     run_opts = {"pair_precision": args.pair_precision, "device": local}
     for _, c in items:
         c.update({"pair_precision": args.pair_precision, "device": local})
@@ -258,6 +259,7 @@ def run_batch_workload(args) -> int:
         "dtype": "f64 state, f32 pair terms" if args.pair_precision == "mixed" else "f64",
         "data": "synthetic",
         "config": {"workload": f"batch{len(items)}_N64-16384_ndim234_phi0.10", "packings": len(items),
+                   "seeds": f"{seeds[0]}, {seeds[1] if len(seeds) > 1 else ''}, ... every {stride * world}-th of 0..4095",
                    "concurrency": args.concurrency,
                    "engine": {0: "persistent batch kernel for the small packings + engines on 32 streams"}.get(
                        args.concurrency, "persistent batch kernel" if args.concurrency < 0 else "graph engines on streams"),
@@ -303,13 +305,48 @@ def run_one_packing(args) -> int:
     return 0
 
 
+def bench_config(n: int, warmup: int, steps: int) -> dict:
+    """The workload as both arms name it (identical dict in both lines)."""
+    return {"workload": workload_name(n), "N": n, "Ndim": 2,
+            "dist": "bidisperse 1.0:1.4 at 50:50", "init_phi": 0.30, "box": "periodic unit square",
+            "seed": WORKLOAD["seed"], "window": f"ADAM steps {warmup + 1}..{warmup + steps} of pack() from "
+                                                 f"the start (early phase, a rebuild every step)",
+            "l2": "inputs larger than L2 (~150 MB touched per step)"}
+
+
+def reference_module():
+    """The reference engine compiled from its own sources (oracle/_ref), with a
+    clean RCP_* environment; None when it was not built."""
+    ref_dir = REPO / "oracle" / "_ref"
+    if not any(ref_dir.glob("_rcpgenerator*.so")):
+        return None
+    if str(ref_dir) not in sys.path:
+        sys.path.insert(0, str(ref_dir))
+    for k in list(os.environ):
+        if k.startswith("RCP_"):
+            del os.environ[k]
+    import _rcpgenerator as ref
+    return ref
+
+
 def run_reference_arm(args):
+    """The reference's own CPU engine on the same workload: its own
+    initializer (same seed, the input this project's initializer reproduces
+    bit for bit) and its run_packing_observed, timed per step by its own
+    observer on all host threads. Nothing of this project is imported."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    pos, dia, init = make_input(0)
+    ref = reference_module()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
+        return 0
+    cfg = dict(WORKLOAD)
+    init = ref.initialize_particles(cfg)
+    pos = np.asarray(init["positions"], dtype=np.float64)
+    dia = np.asarray(init["diameters"], dtype=np.float64)
     threads = os.cpu_count() or 1
-    s, why = reference_sample(pos, dia, init["box"], init["walls"], args.warmup + args.steps, threads)
+    s, why = reference_sample(pos, dia, init["box"], init["walls"], args.warmup, args.steps, threads)
     if s is None:
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return 0
@@ -318,15 +355,221 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(WORKLOAD["N"]), "N": WORKLOAD["N"], "Ndim": 2,
-                   "engine": "reference C++/OpenMP run_packing_observed, portable build",
-                   "l2": "inputs larger than L2"},
+        "config": bench_config(WORKLOAD["N"], args.warmup, args.steps),
+        "engine": "reference C++/OpenMP run_packing_observed (oracle/_ref, portable build), "
+                  "input from its own initialize_particles",
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"first {s['timed_steps']} steps after step 1 of the same packing "
-                                   f"(observer timestamps), setup excluded"},
+                         "sample": f"steps {s['first']}..{s['last']} of the packing (observer timestamps), "
+                                   f"setup excluded"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+    return 0
+
+
+def growth_deadline(n: int, nd: int) -> int:
+    """Last step of the growth rung (mu_flag = 1) on the reference's schedule:
+    6000 + 9 sqrt(N d), at least 1500 (ENG:4713-4737)."""
+    return max(1500, int(6000 + 9 * (n * nd) ** 0.5))
+
+
+def timed_window(eng, stream, steps: int, clocks=None):
+    """K steps of an engine timed with CUDA events on its stream."""
+    import torch
+    torch.cuda.synchronize()
+    l0, s0 = eng.kernel_launches, eng.steps
+    if clocks is not None:
+        clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    eng.advance(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks is not None else None
+    return e0.elapsed_time(e1), eng.steps - s0, eng.kernel_launches - l0, clk
+
+
+def late_phase(rb, pos, dia, init, precision, local, steps):
+    """ADAM steps/s after the growth rung: the engine is advanced untimed past
+    the rung's last step, then `steps` steps are timed (the phase where most
+    steps skip the rebuild and the pair kernel dominates)."""
+    import torch
+    stream = torch.cuda.Stream()
+    eng = rb.PackingEngine({"positions": pos, "diameters": dia},
+                           {"box": init["box"], "walls": init["walls"], "device": local,
+                            "pair_precision": precision}, {}, stream=stream.cuda_stream)
+    n, nd = pos.shape
+    start = growth_deadline(n, nd) + 200
+    eng.advance(start)
+    b0 = eng.result(as_arrays=True)["engine_stats"]["pair_builds"]
+    ms, done, launches, _ = timed_window(eng, stream, steps)
+    res = eng.result(as_arrays=True)
+    prof = eng.profile_pair_kernel(reps=20)
+    eng.close()
+    return {"value": done / (ms / 1e3), "unit": UNIT, "steps": done, "ms_per_step": ms / max(done, 1),
+            "window": f"steps {start + 1}..{start + done}", "pair_builds_in_window":
+            int(res["engine_stats"]["pair_builds"] - b0),
+            "fp64_switch_step": int(res["engine_stats"]["fp64_switch_step"]),
+            "max_overlap_at_end": float(res["max_overlap_history"][-1]) if len(res["max_overlap_history"]) else None,
+            "gpu_launches": int(launches)}, prof
+
+
+def roofline_of(prof, peak, peak_kind, kernel, traffic_per_byte):
+    achieved = prof["alg_bytes"] / (prof["avg_ms"] / 1e3) / 1e9
+    out = {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "peak_kind": peak_kind,
+           "traffic": prof["alg_bytes"] * traffic_per_byte,
+           "traffic_note": "ncu DRAM bytes per algorithmic byte of a smaller capture (profiles/), scaled",
+           "alg_bytes_per_launch": prof["alg_bytes"], "avg_launch_ms": prof["avg_ms"]}
+    if "mean_row" in prof:
+        out["mean_row"] = prof["mean_row"]
+    return out
+
+
+def batch_summary(args, local):
+    """packings/hour of the batched workload on a sample of its generator
+    (seeds 0..count-1): the batch engine plain and warm-started, the same
+    engine one packing at a time, and the reference estimate."""
+    ns = argparse.Namespace(**vars(args))
+    ns.batch_count = args.bench_batch
+    buf = []
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()) as out:
+        run_batch_workload(ns)
+    for line in out.getvalue().splitlines():
+        if line.startswith("{"):
+            buf.append(json.loads(line))
+    if not buf:
+        return None
+    b = buf[-1]
+    return {"metric": BATCH_METRIC, "value": b["value"], "unit": BATCH_METRIC,
+            "packings": b["config"]["packings"], "workload": b["config"]["workload"],
+            "engine": b["config"]["engine"], "mean_steps": b["config"]["mean_steps"],
+            "pair_precision": b["config"]["pair_precision"], "timing": b["config"]["timing"],
+            "plain_engine": b["plain_engine"], "warm_start": b["warm_start"],
+            "cpu_baseline": b["cpu_baseline"]}
+
+
+def run_single(args) -> int:
+    """The default line: ADAM steps/s of the N = 1M packing."""
+    import torch
+    import torch.distributed as dist
+    import rcpgenerator_b200 as rb
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    pos, dia, init = make_input(rank)
+    n, nd = pos.shape
+    run_cfg = {"box": init["box"], "walls": init["walls"], "device": local,
+               "pair_precision": args.pair_precision}
+
+    def early(precision, clocks=None):
+        stream = torch.cuda.Stream()
+        cfg = dict(run_cfg, pair_precision=precision)
+        eng = rb.PackingEngine({"positions": pos, "diameters": dia}, cfg, {}, stream=stream.cuda_stream)
+        eng.advance(args.warmup)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        return eng, timed_window(eng, stream, args.steps, clocks)
+
+    # the headline window: early phase, the workload's stated (mixed) precision
+    clocks = ClockSampler(local)
+    eng, (ms, done_steps, launches, clk) = early(args.pair_precision, clocks)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    bprof = eng.profile_build_kernel(reps=10)
+    res = eng.result(as_arrays=True)
+    eng.close()
+    # the same window in FP64 pair arithmetic
+    other = "f64" if args.pair_precision == "mixed" else "mixed"
+    eng2, (ms2, done2, _, _) = early(other)
+    eng2.close()
+    late = {}
+    prof = None
+    if not args.no_late:
+        for prec in (args.pair_precision, other):
+            late[prec], p = late_phase(rb, pos, dia, init, prec, local, args.late_steps)
+            if prec == args.pair_precision:
+                prof = p
+
+    # end to end through the public API: host buffers in, results out
+    torch.cuda.synchronize()
+    e2e_steps, t_e2e = 0, 0.0
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        r2 = rb.run_packing_observed({"positions": pos, "diameters": dia}, run_cfg,
+                                     0, False, 0, None, {"max_steps": args.steps}, as_arrays=True)["result"]
+        t_e2e = time.perf_counter() - t0
+        e2e_steps = int(r2["steps"])
+
+    batch = None
+    if not args.no_batch and rank == 0:
+        batch = batch_summary(args, local)
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+    value = world * done_steps / (ms / 1e3)
+    peak, peak_kind = hbm_peak()
+    cpu = None
+    if not args.no_cpu_baseline:
+        s, why = reference_sample(pos, dia, init["box"], init["walls"], 1, args.cpu_sample_steps,
+                                  os.cpu_count() or 1)
+        if s is not None:
+            cpu = {"value": s["steps_per_s"], "unit": UNIT, "cores": os.cpu_count(),
+                   "kind": "reference",
+                   "sample": f"steps {s['first']}..{s['last']} of the same packing on the reference "
+                             f"engine (oracle/_ref), all host threads"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": why}
+    dtype = {"mixed": "f64 state, f32 pair terms", "f64": "f64"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done_steps,
+        "warmup": args.warmup, "ms_per_step": ms / max(done_steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype[args.pair_precision],
+        "data": "synthetic",
+        "config": bench_config(n, args.warmup, args.steps),
+        "engine": {"mode": "graph (CUDA-graph step loop, controller on the GPU)",
+                   "pair_precision": args.pair_precision,
+                   "fp64_switch_step": int(res["engine_stats"]["fp64_switch_step"]),
+                   "parallelism": f"replicas{world}",
+                   "pair_builds": int(res["engine_stats"]["pair_builds"]),
+                   "row_capacity": int(res["engine_stats"]["row_capacity"])},
+        # the same window with the other pair precision (FP64 is the reference's precision)
+        "other_precision": {"pair_precision": other, "dtype": dtype[other],
+                            "value": done2 / (ms2 / 1e3), "unit": UNIT, "ms_per_step": ms2 / max(done2, 1)},
+        "late_phase": late or None,
+        # the step's dominant kernel in this window: every step rebuilds its
+        # rows, and the tiled build computes that step's forces in the same pass
+        "roofline": roofline_of(bprof, peak, peak_kind, "k_build_search_tiled (neighbour build + fused forces)",
+                                BUILD_TRAFFIC_PER_ALG_BYTE),
+        # the pair kernel of the steps without a rebuild (the reference's 81 % kernel),
+        # on the state after the growth rung
+        "roofline_pair_kernel": (roofline_of(prof, peak, peak_kind, "k_forces (pair energy/gradient, full rows)",
+                                             FORCES_TRAFFIC_PER_ALG_BYTE) if prof else None),
+        "cpu_baseline": cpu,
+        "e2e": None if args.no_e2e else {"value": e2e_steps / t_e2e, "unit": UNIT,
+                "h2d_bytes_per_step": int((n * (nd + 1) * 8) / max(e2e_steps, 1)),
+                "d2h_bytes_per_step": int((n * (nd + 2) * 8 + e2e_steps * 6 * 8) / max(e2e_steps, 1)),
+                "note": "run_packing_observed(max_steps=K) from host NumPy arrays: setup, K steps, results"},
+        "batch": batch,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
     return 0
 
 
@@ -339,6 +582,10 @@ def main() -> int:
     ap.add_argument("--cpu-sample-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-late", action="store_true", help="skip the late-phase windows")
+    ap.add_argument("--late-steps", type=int, default=2000)
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-workload sub-object")
+    ap.add_argument("--bench-batch", type=int, default=512, help="packings in the default line's batch sample")
     ap.add_argument("--no-warm-start", action="store_true", help="batch workload: skip the warm-started arm")
     ap.add_argument("--warm-start-model", default=str(REPO / "rcpgenerator_b200" / "warmstart_model.npz"))
     ap.add_argument("--pair-precision", default="mixed", choices=["mixed", "f64"],
@@ -350,6 +597,9 @@ def main() -> int:
                          "one: ADAM steps/s of packing --seed of the batch generator (profiling)")
     ap.add_argument("--seed", type=int, default=4, help="one: generator seed (4: 4-D, N = 11,948)")
     ap.add_argument("--batch-count", type=int, default=128)
+    ap.add_argument("--batch-stride", type=int, default=0,
+                    help="batch: generator seeds k * stride (0: 4096 // count, a stratified sample of "
+                         "seeds 0..4095)")
     ap.add_argument("--batch-single", type=int, default=8, help="packings timed one at a time")
     ap.add_argument("--concurrency", type=int, default=0,
                     help="-1: persistent batch kernel; 0: persistent for small packings + 32 streams; k: k streams")
@@ -362,123 +612,7 @@ def main() -> int:
         return run_batch_workload(args)
     if args.workload == "one":
         return run_one_packing(args)
-
-    import torch
-    import torch.distributed as dist
-    import rcpgenerator_b200 as rb
-
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    pos, dia, init = make_input(rank)
-    stream = torch.cuda.Stream()
-    run_cfg = {"box": init["box"], "walls": init["walls"], "device": local,
-               "pair_precision": args.pair_precision}
-    eng = rb.PackingEngine({"positions": pos, "diameters": dia}, run_cfg, {}, stream=stream.cuda_stream)
-    eng.advance(args.warmup)
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    l0 = eng.kernel_launches
-    s0 = eng.steps
-    clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    eng.advance(args.steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    done_steps = eng.steps - s0
-    launches = eng.kernel_launches - l0
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        if dist.is_initialized():
-            dist.barrier()
-    prof = eng.profile_pair_kernel(reps=max(10, min(args.steps, 100)))
-    bprof = eng.profile_build_kernel(reps=10)
-    res = eng.result(as_arrays=True)
-    eng.close()
-
-    # end to end through the public API: host buffers in, results out
-    torch.cuda.synchronize()
-    e2e_steps, t_e2e = 0, 0.0
-    if not args.no_e2e:
-        t0 = time.perf_counter()
-        r2 = rb.run_packing_observed({"positions": pos, "diameters": dia}, run_cfg,
-                                     0, False, 0, None, {"max_steps": args.steps}, as_arrays=True)["result"]
-        t_e2e = time.perf_counter() - t0
-        e2e_steps = int(r2["steps"])
-
-    if rank != 0:
-        if world > 1:
-            dist.destroy_process_group()
-        return 0
-    value = world * done_steps / (ms / 1e3)
-    peak, peak_kind = hbm_peak()
-    achieved = prof["alg_bytes"] / (prof["avg_ms"] / 1e3) / 1e9
-    b_achieved = bprof["alg_bytes"] / (bprof["avg_ms"] / 1e3) / 1e9
-    cpu = None
-    if not args.no_cpu_baseline:
-        s, why = reference_sample(pos, dia, init["box"], init["walls"], args.cpu_sample_steps,
-                                  os.cpu_count() or 1)
-        if s is not None:
-            cpu = {"value": s["steps_per_s"], "unit": UNIT, "cores": os.cpu_count(),
-                   "kind": "reference",
-                   "sample": f"{s['timed_steps']} steps (2..{s['timed_steps'] + 1}) of the same "
-                             f"packing on the reference engine, all host threads"}
-        else:
-            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                   "sample": why}
-    n, nd = pos.shape
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done_steps,
-        "warmup": args.warmup, "ms_per_step": ms / max(done_steps, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 state, f32 pair terms" if args.pair_precision == "mixed" else "f64",
-        "data": "synthetic",
-        "config": {"workload": workload_name(n), "N": n, "Ndim": nd,
-                   "engine": "graph", "pair_precision": args.pair_precision,
-                   "fp64_switch_step": int(res["engine_stats"]["fp64_switch_step"]),
-                   "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (~150 MB touched per step)",
-                   "pair_builds": int(res["engine_stats"]["pair_builds"]),
-                   "row_capacity": int(res["engine_stats"]["row_capacity"])},
-        # the step's dominant kernel: every step of this phase rebuilds its rows,
-        # and the tiled build computes that step's forces in the same pass
-        "roofline": {"bound": "hbm", "kernel": "k_build_search_tiled (neighbour build + fused forces)",
-                     "achieved": b_achieved, "peak": peak, "unit": "GB/s", "frac": b_achieved / peak,
-                     "peak_kind": peak_kind,
-                     "traffic": bprof["alg_bytes"] * BUILD_TRAFFIC_PER_ALG_BYTE,
-                     "traffic_note": "ncu DRAM bytes per algorithmic byte at N=300k (profiles/), scaled",
-                     "alg_bytes_per_launch": bprof["alg_bytes"], "avg_launch_ms": bprof["avg_ms"]},
-        # the pair kernel of the steps without a rebuild (the reference's 81 % kernel)
-        "roofline_pair_kernel": {"bound": "hbm", "kernel": "k_forces (pair energy/gradient, full rows)",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind,
-                     "traffic": prof["alg_bytes"] * FORCES_TRAFFIC_PER_ALG_BYTE,
-                     "traffic_note": "ncu DRAM bytes per algorithmic byte at N=300k (profiles/), scaled",
-                     "alg_bytes_per_launch": prof["alg_bytes"], "avg_launch_ms": prof["avg_ms"],
-                     "mean_row": prof["mean_row"]},
-        "cpu_baseline": cpu,
-        "e2e": None if args.no_e2e else {"value": e2e_steps / t_e2e, "unit": UNIT,
-                "h2d_bytes_per_step": int((n * (nd + 1) * 8) / max(e2e_steps, 1)),
-                "d2h_bytes_per_step": int((n * (nd + 2) * 8 + e2e_steps * 6 * 8) / max(e2e_steps, 1)),
-                "note": "run_packing_observed(max_steps=K) from host NumPy arrays: setup, K steps, results"},
-        "gpu_launches": int(launches),
-        "clocks": clk,
-    }
-    print(json.dumps(line))
-    if world > 1:
-        dist.destroy_process_group()
-    return 0
+    return run_single(args)
 
 
 if __name__ == "__main__":

@@ -250,13 +250,36 @@ int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const dou
  * cell grid, P = 4 for ndim <= 3, i.e. roughly 20,000 particles in 3-D at
  * row_capacity 64 -- is rejected with RCPG_ENOSPC before any work. The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress)
- * and should be made before any stream capture. All calls share the array and
- * it keeps the previous call's contents (the build clears what must start at
- * zero); calls whose GPU work overlaps in time race and must be serialised. */
+ * and should be made before any stream capture. Every call waits for `stream`
+ * to finish, because it reads the longest row back to the host to report it.
+ * All calls share the array and it keeps the previous call's contents (the
+ * build clears what must start at zero); calls whose GPU work overlaps in time
+ * race and must be serialised. */
 int32_t rcpg_pairs_full_noalloc(uint64_t N, int32_t ndim, const double* x_dev, const double* D_dev,
                                 const double* box, const int8_t* walls, double t_shell,
                                 uint32_t row_capacity, uint32_t* nbr_dev, uint32_t* cnt_dev,
                                 uint32_t* row_need_out, void* stream, char* err, size_t errlen);
+
+/* One neighbour build of the graph engine on a given state, with that state's
+ * forces: get_pairs_kdtree (ENG:2758-3526) with every particle refreshed, then
+ * get_forces_nd_3 (rcp_generator.hpp:218-243) + compute_mean_force
+ * (:150-155), the way a rebuild step of the graph engine does them. Rows hold
+ * the same partners as rcpg_pairs_full but in the build's scan order (mixed
+ * precision: a superset, see below), returned in particle order like
+ * rcpg_pairs_full; F_dev [N*ndim] and scalars[7] as rcpg_forces with tree-order
+ * sums. Where the build computes the forces in the same pass (the tiled
+ * search: ndim <= 3, N >= 20,000, one size class) *fused_out = 1, else the
+ * pair kernel computes them on the new rows and *fused_out = 0.
+ * pair_precision 1 = the graph engine's mixed precision (FP32 pair terms on
+ * FP64 differences; the row test is widened by 1e-5 relative, so rows hold
+ * every pair of the FP64 shell and a few just outside it), 0 = FP64.
+ * Diagnostic entry point for parity tests; no counterpart in the reference. */
+int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, const double* D_dev,
+                               const double* box, const int8_t* walls, double t_shell, double mu,
+                               int32_t pair_precision, uint32_t row_capacity, uint32_t* nbr_dev,
+                               uint32_t* cnt_dev, uint32_t* row_need_out, double* F_dev,
+                               double* scalars, int32_t* fused_out, void* stream, char* err,
+                               size_t errlen);
 
 /* get_forces_nd_3 (rcp_generator.hpp:218-243) on rows from rcpg_pairs_full
  * (any superset of the overlapping pairs gives the same result), followed by

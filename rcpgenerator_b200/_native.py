@@ -42,6 +42,7 @@ EXPORTED_SYMBOLS = (
     "rcpg_t_shell",
     "rcpg_pairs_full",
     "rcpg_pairs_full_noalloc",
+    "rcpg_pairs_forces_scan",
     "rcpg_forces",
     "rcpg_mean_force",
     "rcpg_adam_step",
@@ -228,6 +229,11 @@ def _load() -> C.CDLL:
             C.c_int32,
             [C.c_uint64, C.c_int32, vp, vp, _dp, _i8p, C.c_double, C.c_uint32, vp, vp, _u32p, vp,
              cp, sz],
+        ),
+        "rcpg_pairs_forces_scan": (
+            C.c_int32,
+            [C.c_uint64, C.c_int32, vp, vp, _dp, _i8p, C.c_double, C.c_double, C.c_int32, C.c_uint32,
+             vp, vp, _u32p, vp, _dp, _i32p, vp, cp, sz],
         ),
         "rcpg_forces": (
             C.c_int32,

@@ -573,6 +573,100 @@ int32_t rcpg_pairs_full(uint64_t N, int32_t ndim, const double* x_dev, const dou
     }
 }
 
+int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, const double* D_dev,
+                               const double* box, const int8_t* walls, double t_shell, double mu,
+                               int32_t pair_precision, uint32_t row_capacity, uint32_t* nbr_dev,
+                               uint32_t* cnt_dev, uint32_t* row_need_out, double* F_dev,
+                               double* scalars, int32_t* fused_out, void* stream, char* err,
+                               size_t errlen) {
+    if (N == 0 || ndim < 2 || ndim > rcpg::kMaxDim || !x_dev || !D_dev || !nbr_dev || !cnt_dev ||
+        !F_dev || row_capacity == 0 || pair_precision < 0 || pair_precision > 1)
+        return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: bad arguments to rcpg_pairs_forces_scan");
+    if (!have_device(err, errlen)) return RCPG_ECUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    try {
+        const int P = rcpg::pos_stride(ndim);
+        std::vector<double> D(N);
+        cuda_ok(cudaMemcpyAsync(D.data(), D_dev, N * 8, cudaMemcpyDeviceToHost, st), "D2H D");
+        cuda_ok(cudaStreamSynchronize(st), "sync");
+        const double Dmax = *std::max_element(D.begin(), D.end());
+        Scratch sc(st);
+        DevArrays a{};
+        a.N = N;
+        a.ndim = ndim;
+        a.P = P;
+        a.pos = static_cast<double*>(sc.get(N * P * 8));
+        a.spos = static_cast<double*>(sc.get(N * P * 8));
+        a.x_last = static_cast<double*>(sc.get(N * ndim * 8));
+        a.F = F_dev;
+        a.nbr = static_cast<std::uint32_t*>(sc.get(static_cast<std::size_t>(row_capacity) * N * 4));
+        a.nbr_cnt = static_cast<std::uint32_t*>(sc.get(N * 4));
+        a.S = row_capacity;
+        a.sorted_rows = 0;  // the graph engine's scan order
+        a.mixed = pair_precision;
+        a.caps = static_cast<std::uint32_t*>(sc.get(N * 4));
+        a.cell_of = static_cast<std::uint32_t*>(sc.get(N * 4));
+        a.cell_rank = static_cast<std::uint32_t*>(sc.get(N * 4));
+        a.cell_list = static_cast<std::uint32_t*>(sc.get(N * 4));
+        a.work = static_cast<std::uint32_t*>(sc.get(N * 4));
+        {
+            const double cutoff = (Dmax + t_shell) * (1.0 + 1e-6);
+            double cells = 1.0;
+            for (int d = 0; d < ndim; ++d) cells *= std::max(1.0, std::floor((box ? box[d] : 1.0) / cutoff));
+            double cap = std::min(cells + 64.0, 8.0 * static_cast<double>(N) + 1024.0);
+            a.C_alloc = static_cast<std::uint32_t>(std::min(cap, 2.0e9));
+        }
+        a.cell_count = static_cast<std::uint32_t*>(sc.get((a.C_alloc + 1ull) * 4));
+        a.cell_start = static_cast<std::uint32_t*>(sc.get((a.C_alloc + 1ull) * 4));
+        a.scan_tmp = static_cast<std::uint32_t*>(sc.get(2 * 4096 * 4 + 64));
+        a.block_sums = static_cast<rcpg::ForceSums*>(
+            sc.get(std::max<std::size_t>(rcpg::force_blocks(N), 4096) * sizeof(rcpg::ForceSums)));
+        a.ctl = static_cast<DevCtl*>(sc.get(sizeof(DevCtl)));
+        DevCtl h;
+        std::memset(&h, 0, sizeof(h));
+        geometry_from(h, ndim, box, walls);
+        h.build_kappa = 1.0;
+        h.build_t_shell = t_shell;
+        h.build_Dmax = Dmax;
+        h.force_kappa = 1.0;
+        h.force_mu = mu;
+        h.rebuild_flag = 1u;
+        h.fuse_forces = 1u;
+        h.pair_fp32 = static_cast<std::uint32_t>(pair_precision);
+        cuda_ok(cudaMemcpyAsync(a.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st), "H2D ctl");
+        cuda_ok(cudaMemsetAsync(a.caps, 0xFF, N * 4, st), "memset caps");
+        rcpg::launch_pack(N, ndim, x_dev, D_dev, a.pos, st);
+        rcpg::launch_rebuild(a, st);
+        // the forces of the build, or (builds that do not fuse them) of the pair kernel
+        DevCtl after;
+        cuda_ok(cudaMemcpyAsync(&after, a.ctl, sizeof(after), cudaMemcpyDeviceToHost, st), "D2H ctl");
+        cuda_ok(cudaStreamSynchronize(st), "sync");
+        rcpg::launch_forces(a, 0, st);
+        rcpg::launch_reduce_fast(a, st);
+        rcpg::launch_rows_to_particle_order(N, a.work, a.nbr, a.nbr_cnt, nbr_dev, cnt_dev, st);
+        cuda_ok(cudaMemcpyAsync(&h, a.ctl, sizeof(h), cudaMemcpyDeviceToHost, st), "D2H ctl");
+        cuda_ok(cudaStreamSynchronize(st), "sync");
+        cuda_ok(cudaGetLastError(), "kernel launch");
+        if (row_need_out) *row_need_out = h.row_need;
+        if (fused_out) *fused_out = static_cast<int32_t>(after.forces_done);
+        if (h.row_need > row_capacity)
+            return fail(err, errlen, RCPG_ENOSPC, "rcpgenerator_b200: a neighbour row exceeds row_capacity");
+        const rcpg::StepScalars s = rcpg::finalize_sums(h.sums, mu, ndim);
+        if (scalars) {
+            scalars[0] = s.U;
+            scalars[1] = s.max_overlap;
+            scalars[2] = s.Lc;
+            scalars[3] = s.Fmean;
+            scalars[4] = s.dkappa;
+            scalars[5] = s.mean_force;
+            scalars[6] = s.count;
+        }
+        return RCPG_OK;
+    } catch (const std::exception& e) {
+        return fail(err, errlen, classify(e), e.what());
+    }
+}
+
 int32_t rcpg_forces(uint64_t N, int32_t ndim, const double* x_dev, const double* D_dev,
                     const double* box, const int8_t* walls, const uint32_t* nbr_dev,
                     const uint32_t* cnt_dev, uint32_t row_capacity, double mu,

@@ -25,12 +25,15 @@
 #include <mutex>
 #include <string>
 
+#include <stdexcept>
+
 #include "../../include/rcpg.h"
 #include "rcpg_device.h"
+#include "rcpg_noalloc_plan.h"
 
 namespace {
 
-constexpr std::size_t kNoAllocScratchBytes = std::size_t{8} << 20;
+using rcpg::kNoAllocScratchBytes;
 constexpr int kMaxDevices = 64;
 
 // The scratch array. Host code must not use its name as a pointer: on the
@@ -84,24 +87,6 @@ int32_t scratch_address(void** out, char* err, std::size_t errlen) {
     return RCPG_OK;
 }
 
-struct Carver {
-    unsigned char* base;
-    std::size_t used = 0;
-    std::size_t cap;
-    bool ok = true;
-    template <typename T>
-    T* take(std::size_t count) {
-        const std::size_t off = (used + 255) & ~std::size_t{255};
-        const std::size_t bytes = count * sizeof(T);
-        if (off + bytes > cap) {
-            ok = false;
-            return nullptr;
-        }
-        used = off + bytes;
-        return reinterpret_cast<T*>(base + off);
-    }
-};
-
 }  // namespace
 
 extern "C" int32_t rcpg_pairs_full_noalloc(uint64_t N, int32_t ndim, const double* x_dev,
@@ -119,49 +104,37 @@ extern "C" int32_t rcpg_pairs_full_noalloc(uint64_t N, int32_t ndim, const doubl
     const int32_t rc = scratch_address(&base, err, errlen);
     if (rc != RCPG_OK) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int P = rcpg::pos_stride(ndim);
-    Carver cv{static_cast<unsigned char*>(base), 0, kNoAllocScratchBytes};
-    rcpg::DevArrays a{};
-    a.N = N;
-    a.ndim = ndim;
-    a.P = P;
-    a.ctl = cv.take<rcpg::DevCtl>(1);
-    a.pos = cv.take<double>(N * P);
-    a.spos = cv.take<double>(N * P);
-    a.x_last = cv.take<double>(N * ndim);
-    a.caps = cv.take<std::uint32_t>(N);
-    a.cell_of = cv.take<std::uint32_t>(N);
-    a.cell_rank = cv.take<std::uint32_t>(N);
-    a.cell_list = cv.take<std::uint32_t>(N);
-    a.work = cv.take<std::uint32_t>(N);
-    a.nbr_cnt = cv.take<std::uint32_t>(N);
-    a.nbr = cv.take<std::uint32_t>(static_cast<std::size_t>(row_capacity) * N);
-    a.scan_tmp = cv.take<std::uint32_t>(2 * 4096 + 16);
-    a.S = row_capacity;
-    a.sorted_rows = 1;  // the reference's row order
-    if (!cv.ok) {
+    const rcpg::NoAllocPlan plan = rcpg::plan_noalloc(N, ndim, row_capacity, sizeof(rcpg::DevCtl));
+    if (!plan.ok) {
         set_err(err, errlen,
                 "rcpgenerator_b200: rcpg_pairs_full_noalloc needs more than its fixed 8 MiB "
                 "device scratch for this N / ndim / row_capacity (use rcpg_pairs_full)");
         return RCPG_ENOSPC;
     }
-    // whatever is left holds the cell grid (two arrays of C_alloc + 1 counters);
-    // the build coarsens its grid to fit
-    const std::size_t left = (kNoAllocScratchBytes - ((cv.used + 255) & ~std::size_t{255})) / 8;
-    if (left < 64) {
-        set_err(err, errlen, "rcpgenerator_b200: rcpg_pairs_full_noalloc scratch exhausted");
-        return RCPG_ENOSPC;
-    }
-    std::size_t calloc_n = left - 2;
-    const std::size_t cap_cells = static_cast<std::size_t>(8) * N + 1024;
-    if (calloc_n > cap_cells) calloc_n = cap_cells;
-    a.C_alloc = static_cast<std::uint32_t>(calloc_n);
-    a.cell_count = cv.take<std::uint32_t>(calloc_n + 1);
-    a.cell_start = cv.take<std::uint32_t>(calloc_n + 1);
-    if (!cv.ok) {
-        set_err(err, errlen, "rcpgenerator_b200: rcpg_pairs_full_noalloc scratch exhausted");
-        return RCPG_ENOSPC;
-    }
+    unsigned char* b = static_cast<unsigned char*>(base);
+    rcpg::DevArrays a{};
+    a.N = N;
+    a.ndim = ndim;
+    a.P = rcpg::pos_stride(ndim);
+    a.ctl = reinterpret_cast<rcpg::DevCtl*>(b + plan.ctl);
+    a.pos = reinterpret_cast<double*>(b + plan.pos);
+    a.spos = reinterpret_cast<double*>(b + plan.spos);
+    a.x_last = reinterpret_cast<double*>(b + plan.x_last);
+    a.caps = reinterpret_cast<std::uint32_t*>(b + plan.caps);
+    a.cell_of = reinterpret_cast<std::uint32_t*>(b + plan.cell_of);
+    a.cell_rank = reinterpret_cast<std::uint32_t*>(b + plan.cell_rank);
+    a.cell_list = reinterpret_cast<std::uint32_t*>(b + plan.cell_list);
+    a.work = reinterpret_cast<std::uint32_t*>(b + plan.work);
+    a.nbr_cnt = reinterpret_cast<std::uint32_t*>(b + plan.nbr_cnt);
+    a.nbr = reinterpret_cast<std::uint32_t*>(b + plan.nbr);
+    a.scan_tmp = reinterpret_cast<std::uint32_t*>(b + plan.scan_tmp);
+    a.S = row_capacity;
+    a.sorted_rows = 1;  // the reference's row order
+    // the rest of the array holds the cell grid; the build coarsens its grid
+    // to these many cells
+    a.C_alloc = plan.cell_capacity;
+    a.cell_count = reinterpret_cast<std::uint32_t*>(b + plan.cell_count);
+    a.cell_start = reinterpret_cast<std::uint32_t*>(b + plan.cell_start);
     rcpg::DevCtl h;
     std::memset(&h, 0, sizeof(h));
     rcpg::Geometry& g = h.g;
@@ -183,10 +156,21 @@ extern "C" int32_t rcpg_pairs_full_noalloc(uint64_t N, int32_t ndim, const doubl
         set_err(err, errlen, std::string("rcpgenerator_b200: ") + cudaGetErrorString(e));
         return RCPG_ECUDA;
     }
-    k_noalloc_dmax<<<1, 1024, 0, st>>>(N, D_dev, a.ctl);
-    rcpg::launch_pack(N, ndim, x_dev, D_dev, a.pos, st);
-    rcpg::launch_rebuild(a, st);
-    rcpg::launch_rows_to_particle_order(N, a.work, a.nbr, a.nbr_cnt, nbr_dev, cnt_dev, st);
+    try {
+        k_noalloc_dmax<<<1, 1024, 0, st>>>(N, D_dev, a.ctl);
+        rcpg::launch_pack(N, ndim, x_dev, D_dev, a.pos, st);
+        rcpg::launch_rebuild(a, st);
+        rcpg::launch_rows_to_particle_order(N, a.work, a.nbr, a.nbr_cnt, nbr_dev, cnt_dev, st);
+    } catch (const std::length_error& ex) {
+        set_err(err, errlen, std::string("rcpgenerator_b200: ") + ex.what());
+        return RCPG_ENOSPC;
+    } catch (const std::invalid_argument& ex) {
+        set_err(err, errlen, std::string("rcpgenerator_b200: ") + ex.what());
+        return RCPG_EINVAL;
+    } catch (const std::exception& ex) {
+        set_err(err, errlen, std::string("rcpgenerator_b200: ") + ex.what());
+        return RCPG_ERUNTIME;
+    }
     std::uint32_t need = 0;
     e = cudaMemcpyAsync(&need, &a.ctl->row_need, sizeof(need), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -13,7 +13,7 @@ inputs, what the reference's own code returns:
                      thread): steps, phi, positions, diameters, origins, and
                      SHA-256 digests of every history
 
-Usage:  python tests/golden/make_golden.py
+Usage:  python tests/golden/make_golden.py /path/to/RCPGenerator
 """
 
 from __future__ import annotations
@@ -122,10 +122,11 @@ def digest(a) -> str:
     return hashlib.sha256(np.ascontiguousarray(np.asarray(a)).tobytes()).hexdigest()
 
 
-def main() -> None:
+def main(ref_root: str) -> None:
     env = dict(os.environ)
     env.pop("OMP_NUM_THREADS", None)
-    subprocess.run(["make", "-C", str(REPO / "oracle"), "PY=" + sys.executable], check=True, env=env)
+    subprocess.run(["make", "-C", str(REPO / "oracle"), "PY=" + sys.executable,
+                    "REF_ROOT=" + str(Path(ref_root) / "python_code" / "python")], check=True, env=env)
     sys.path.insert(0, str(REF_DIR))
     for k in list(os.environ):
         if k.startswith("RCP_"):
@@ -233,4 +234,6 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py /path/to/RCPGenerator")
+    main(sys.argv[1])

@@ -50,4 +50,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_overlap_golden.py /path/to/RCPGenerator")
+    main(sys.argv[1])

@@ -10,6 +10,8 @@
 #include <vector>
 
 #include "rcpg_core.h"
+#include "rcpg_device.h"
+#include "rcpg_noalloc_plan.h"
 #include "rcpg_schedule.h"
 #include "rcpg_setup.h"
 
@@ -291,4 +293,22 @@ extern "C" int hostemu_run_packing(std::uint64_t N, int ndim, const double* posi
         case 4: return run_nd<4>(in, pos_out, dia_out, hist_out, hist_cap, origin_out, scal_out);
         default: return -22;
     }
+}
+
+// Layout of the allocation-free build's fixed scratch array (the product's
+// own sizing, rcpg_noalloc_plan.h) for a CPU test: out[0..13] = byte offsets
+// of ctl, pos, spos, x_last, caps, cell_of, cell_rank, cell_list, work,
+// nbr_cnt, nbr, scan_tmp, cell_count, cell_start; out[14] = cell capacity,
+// out[15] = bytes used, out[16] = array size. Returns 1 when the plan fits.
+extern "C" int hostemu_noalloc_plan(std::uint64_t N, int ndim, std::uint32_t row_capacity,
+                                    std::uint64_t* out) {
+    const NoAllocPlan p = plan_noalloc(N, ndim, row_capacity, sizeof(DevCtl));
+    const std::size_t offs[14] = {p.ctl, p.pos, p.spos, p.x_last, p.caps, p.cell_of, p.cell_rank,
+                                  p.cell_list, p.work, p.nbr_cnt, p.nbr, p.scan_tmp, p.cell_count,
+                                  p.cell_start};
+    for (int k = 0; k < 14; ++k) out[k] = offs[k];
+    out[14] = p.cell_capacity;
+    out[15] = p.used;
+    out[16] = kNoAllocScratchBytes;
+    return p.ok ? 1 : 0;
 }

@@ -92,3 +92,33 @@ def test_noalloc_rejects_oversized_working_set(cuda_device, native):
             None, err, len(err))
     assert rc == N.RCPG_ENOSPC
     assert b"8 MiB" in err.value
+
+
+@pytest.mark.parametrize("case,cap", [("large_bi2d_n30k", 16), ("large_bi3d_sphere_n20k", 64)])
+def test_noalloc_tiled_sizes_equal_allocating_build(cuda_device, native, golden, case, cap):
+    """Sizes at which the build takes its tiled search (N >= 20,000, ndim <= 3)
+    and still fit the fixed array."""
+    fn = _setup(native)
+    g = golden(f"{case}.npz")
+    D = g["D"]
+    t = native.lib.rcpg_t_shell(np.ascontiguousarray(D).ctypes.data_as(C.POINTER(C.c_double)), D.size)
+    ref = _build(native.lib.rcpg_pairs_full, g["x"], D, g["box"], g["walls"], t, cap)
+    for _ in range(2):
+        got = _build(fn, g["x"], D, g["box"], g["walls"], t, cap)
+        assert got[2] == ref[2]
+        assert np.array_equal(got[0], ref[0]) and got[1] == ref[1]
+
+
+def test_noalloc_coarsened_grid_near_the_limit(cuda_device, native):
+    """A 3-D working set that leaves little room for the cell grid: the build
+    coarsens the grid to what is left and still returns the allocating build's
+    rows."""
+    fn = _setup(native)
+    rng = np.random.default_rng(2024)
+    n = 22_600
+    x = rng.random((n, 3))
+    D = np.full(n, 0.01)
+    t = native.lib.rcpg_t_shell(np.ascontiguousarray(D).ctypes.data_as(C.POINTER(C.c_double)), D.size)
+    ref = _build(native.lib.rcpg_pairs_full, x, D, [1.0, 1.0, 1.0], [0, 0, 0], t, 64)
+    got = _build(fn, x, D, [1.0, 1.0, 1.0], [0, 0, 0], t, 64)
+    assert np.array_equal(got[0], ref[0]) and got[1] == ref[1]
