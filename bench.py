@@ -573,6 +573,54 @@ def run_single(args) -> int:
     return 0
 
 
+JAM_CONFIGS = {
+    # the N = 1M 2-D bidisperse packing of the default line
+    2: dict(phi=0.30, N=1_000_000, Ndim=2, box=[1.0, 1.0], walls=[0, 0],
+            dist={"type": "bidisperse", "d1": 1.0, "d2": 1.4, "p": 0.5}, seed=123),
+    # 3-D power law d^-3 on [0.1, 1] (size ratio 10) in a spherical container, N = 2M
+    3: dict(phi=0.20, N=2_000_000, Ndim=3, box=[1.0, 1.0, 1.0], walls=[-3, 0, 0],
+            dist={"type": "powerlaw", "d_min": 0.1, "d_max": 1.0, "exponent": -3.0}, seed=123),
+}
+
+
+def run_jam(args) -> int:
+    """One packing run to the reference's convergence gate (pack()) in mixed
+    and in FP64 pair precision: phi_J, steps, final max overlap, wall time and
+    the mixed run's differences from the FP64 run."""
+    import rcpgenerator_b200 as rb
+    rank, _, local = dist_env()
+    cfg = dict(JAM_CONFIGS[args.jam_config])
+    if args.n != WORKLOAD["N"]:
+        cfg["N"] = args.n
+    t0 = time.perf_counter()
+    init = rb.initialize_particles(cfg)
+    t_init = time.perf_counter() - t0
+    inp = {"positions": np.ascontiguousarray(init["positions"]),
+           "diameters": np.ascontiguousarray(init["diameters"])}
+    out = {"workload": f"config{args.jam_config}", "N": cfg["N"], "Ndim": cfg["Ndim"], "dist": cfg["dist"]["type"],
+           "walls": cfg["walls"], "init_phi": cfg["phi"], "initializer_s": t_init}
+    runs = {}
+    for prec in ("mixed", "f64"):
+        t0 = time.perf_counter()
+        r = rb.run_packing_observed(inp, {"box": init["box"], "walls": init["walls"], "device": local,
+                                          "pair_precision": prec}, 0, False, 0, None, {}, as_arrays=True)["result"]
+        dt = time.perf_counter() - t0
+        st = r["engine_stats"]
+        runs[prec] = r
+        out[prec] = {"phi_J": float(r["phi"]), "steps": int(r["steps"]), "max_overlap": float(r["max_min_dist"]),
+                     "force_magnitude": float(r["force_magnitude"]), "wall_s": dt, "steps_per_s": r["steps"] / dt,
+                     "pair_builds": int(st["pair_builds"]), "fp64_switch_step": int(st["fp64_switch_step"]),
+                     "pair_energy_rel_error": float(st["pair_energy_rel_error"]),
+                     "pair_force_rel_error": float(st["pair_force_rel_error"])}
+    a, b = runs["mixed"], runs["f64"]
+    out["mixed_vs_f64"] = {"delta_phi_J": float(a["phi"] - b["phi"]),
+                           "delta_steps": int(a["steps"] - b["steps"]),
+                           "delta_final_energy": float(a["energy_history"][-1] - b["energy_history"][-1])}
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -592,9 +640,11 @@ def main() -> int:
                     help="pair arithmetic: mixed = FP32 pair terms while the max overlap >= 1e-5 "
                          "(the workload's stated precision), f64 = FP64 throughout")
     ap.add_argument("--n", type=int, default=WORKLOAD["N"], help="particles (smaller cases for profiling)")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "one"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "one", "jam"],
                     help="single: ADAM steps/s of one N=1M packing; batch: packings/hour of many small ones; "
-                         "one: ADAM steps/s of packing --seed of the batch generator (profiling)")
+                         "one: ADAM steps/s of packing --seed of the batch generator (profiling); "
+                         "jam: one packing of --jam-config run to convergence in mixed and FP64 precision")
+    ap.add_argument("--jam-config", type=int, default=2, choices=[2, 3])
     ap.add_argument("--seed", type=int, default=4, help="one: generator seed (4: 4-D, N = 11,948)")
     ap.add_argument("--batch-count", type=int, default=128)
     ap.add_argument("--batch-stride", type=int, default=0,
@@ -612,6 +662,8 @@ def main() -> int:
         return run_batch_workload(args)
     if args.workload == "one":
         return run_one_packing(args)
+    if args.workload == "jam":
+        return run_jam(args)
     return run_single(args)
 
 

@@ -579,8 +579,8 @@ int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, co
                                uint32_t* cnt_dev, uint32_t* row_need_out, double* F_dev,
                                double* scalars, int32_t* fused_out, void* stream, char* err,
                                size_t errlen) {
-    if (N == 0 || ndim < 2 || ndim > rcpg::kMaxDim || !x_dev || !D_dev || !nbr_dev || !cnt_dev ||
-        !F_dev || row_capacity == 0 || pair_precision < 0 || pair_precision > 1)
+    if (N == 0 || N > 0xFFFFFFFFull || ndim < 2 || ndim > rcpg::kMaxDim || !x_dev || !D_dev || !nbr_dev ||
+        !cnt_dev || !F_dev || row_capacity == 0 || pair_precision < 0 || pair_precision > 1)
         return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: bad arguments to rcpg_pairs_forces_scan");
     if (!have_device(err, errlen)) return RCPG_ECUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -595,20 +595,34 @@ int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, co
         a.N = N;
         a.ndim = ndim;
         a.P = P;
-        a.pos = static_cast<double*>(sc.get(N * P * 8));
-        a.spos = static_cast<double*>(sc.get(N * P * 8));
-        a.x_last = static_cast<double*>(sc.get(N * ndim * 8));
-        a.F = F_dev;
-        a.nbr = static_cast<std::uint32_t*>(sc.get(static_cast<std::size_t>(row_capacity) * N * 4));
-        a.nbr_cnt = static_cast<std::uint32_t*>(sc.get(N * 4));
+        // the graph engine's layout: cell-order storage in two buffer sets
+        a.permute = 1;
+        auto dbl = [&](std::size_t n) { return static_cast<double*>(sc.get(n * 8)); };
+        auto u32 = [&](std::size_t n) { return static_cast<std::uint32_t*>(sc.get(n * 4)); };
+        auto u64 = [&](std::size_t n) { return static_cast<std::uint64_t*>(sc.get(n * 8)); };
+        a.pos = dbl(N * P);
+        a.pos_alt = dbl(N * P);
+        a.m = dbl(N * ndim);
+        a.m_alt = dbl(N * ndim);
+        a.v = dbl(N * ndim);
+        a.v_alt = dbl(N * ndim);
+        a.origin = u64(N);
+        a.origin_alt = u64(N);
+        a.caps = u32(N);
+        a.caps_alt = u32(N);
+        a.ref_rank = u32(N);
+        a.ref_rank_alt = u32(N);
+        a.x_last = dbl(N * ndim);
+        a.F = dbl(N * ndim);
+        a.nbr = u32(static_cast<std::size_t>(row_capacity) * N);
+        a.nbr_cnt = u32(N);
         a.S = row_capacity;
         a.sorted_rows = 0;  // the graph engine's scan order
         a.mixed = pair_precision;
-        a.caps = static_cast<std::uint32_t*>(sc.get(N * 4));
-        a.cell_of = static_cast<std::uint32_t*>(sc.get(N * 4));
-        a.cell_rank = static_cast<std::uint32_t*>(sc.get(N * 4));
-        a.cell_list = static_cast<std::uint32_t*>(sc.get(N * 4));
-        a.work = static_cast<std::uint32_t*>(sc.get(N * 4));
+        a.cell_of = u32(N);
+        a.cell_rank = u32(N);
+        a.cell_list = u32(N);
+        a.work = u32(N);
         {
             const double cutoff = (Dmax + t_shell) * (1.0 + 1e-6);
             double cells = 1.0;
@@ -616,9 +630,9 @@ int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, co
             double cap = std::min(cells + 64.0, 8.0 * static_cast<double>(N) + 1024.0);
             a.C_alloc = static_cast<std::uint32_t>(std::min(cap, 2.0e9));
         }
-        a.cell_count = static_cast<std::uint32_t*>(sc.get((a.C_alloc + 1ull) * 4));
-        a.cell_start = static_cast<std::uint32_t*>(sc.get((a.C_alloc + 1ull) * 4));
-        a.scan_tmp = static_cast<std::uint32_t*>(sc.get(2 * 4096 * 4 + 64));
+        a.cell_count = u32(a.C_alloc + 1ull);
+        a.cell_start = u32(a.C_alloc + 1ull);
+        a.scan_tmp = u32(2 * 4096 + 16);
         a.block_sums = static_cast<rcpg::ForceSums*>(
             sc.get(std::max<std::size_t>(rcpg::force_blocks(N), 4096) * sizeof(rcpg::ForceSums)));
         a.ctl = static_cast<DevCtl*>(sc.get(sizeof(DevCtl)));
@@ -633,8 +647,15 @@ int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, co
         h.rebuild_flag = 1u;
         h.fuse_forces = 1u;
         h.pair_fp32 = static_cast<std::uint32_t>(pair_precision);
+        std::vector<std::uint64_t> ident(N);
+        for (std::uint64_t i = 0; i < N; ++i) ident[i] = i;
+        std::vector<std::uint32_t> ident32(ident.begin(), ident.end());
         cuda_ok(cudaMemcpyAsync(a.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st), "H2D ctl");
+        cuda_ok(cudaMemcpyAsync(a.origin, ident.data(), N * 8, cudaMemcpyHostToDevice, st), "H2D origin");
+        cuda_ok(cudaMemcpyAsync(a.ref_rank, ident32.data(), N * 4, cudaMemcpyHostToDevice, st), "H2D rank");
         cuda_ok(cudaMemsetAsync(a.caps, 0xFF, N * 4, st), "memset caps");
+        cuda_ok(cudaMemsetAsync(a.m, 0, N * ndim * 8, st), "memset m");
+        cuda_ok(cudaMemsetAsync(a.v, 0, N * ndim * 8, st), "memset v");
         rcpg::launch_pack(N, ndim, x_dev, D_dev, a.pos, st);
         rcpg::launch_rebuild(a, st);
         // the forces of the build, or (builds that do not fuse them) of the pair kernel
@@ -643,7 +664,8 @@ int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, co
         cuda_ok(cudaStreamSynchronize(st), "sync");
         rcpg::launch_forces(a, 0, st);
         rcpg::launch_reduce_fast(a, st);
-        rcpg::launch_rows_to_particle_order(N, a.work, a.nbr, a.nbr_cnt, nbr_dev, cnt_dev, st);
+        // rows, counts and forces back in the caller's particle order
+        rcpg::launch_cell_order_to_particle_order(a, nbr_dev, cnt_dev, F_dev, st);
         cuda_ok(cudaMemcpyAsync(&h, a.ctl, sizeof(h), cudaMemcpyDeviceToHost, st), "D2H ctl");
         cuda_ok(cudaStreamSynchronize(st), "sync");
         cuda_ok(cudaGetLastError(), "kernel launch");

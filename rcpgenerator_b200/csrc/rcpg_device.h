@@ -68,8 +68,26 @@ struct DevCtl {
     std::uint32_t pad0;
     double mixed_switch;
     std::uint64_t fp64_switch_step;  // step whose max overlap fell below mixed_switch (0: none)
+    // cell-order storage (graph mode): which of the two buffer sets holds the
+    // particle state, flipped by each build's permutation; blocks of the
+    // permutation kernel that have finished (the last one flips)
+    std::uint32_t buf;
+    std::uint32_t permute_done;
+    std::uint64_t pair_kernel_runs;  // launches of the pair kernel that computed forces
 };
 
+// In graph mode every pair-list build stores the particles in cell order
+// ("cell-order storage"): the build permutes the per-particle state (pos, m,
+// v, origin, caps, ref_rank) into the second buffer set (*_alt) in the order of
+// the cell grid -- cells in grid order, each cell's members in their previous
+// order -- and flips DevCtl::buf, so the search and the pair kernel read each
+// particle's neighbours from a few contiguous ranges. Rows then hold partner
+// indices of that order and F is in that order too. ref_rank[i] is the
+// particle's index in the reference's own order (input order permuted by its
+// spatial reorders), used to return results in that order. Kernels call
+// bind_buffers() first, which points pos/m/v/origin/caps/ref_rank at the
+// current set; without *_alt (exact mode, the stand-alone C ABI kernels) the
+// arrays never move.
 struct DevArrays {
     std::uint64_t N;
     int ndim;
@@ -116,7 +134,35 @@ struct DevArrays {
     std::uint32_t* sort_hist;  // [256 * nblocks]
     DevCtl* ctl;
     Histories hist;            // device histories (graph mode)
+    // cell-order storage (graph mode; nullptr otherwise): the second buffer
+    // set and the reference-order rank of each particle
+    int permute;               // 1: every build permutes into cell order
+    double* pos_alt;
+    double* m_alt;
+    double* v_alt;
+    std::uint64_t* origin_alt;
+    std::uint32_t* caps_alt;
+    std::uint32_t* ref_rank;
+    std::uint32_t* ref_rank_alt;
+    // Captured step graphs with conditional nodes (graph mode): the handle of
+    // the step's pair-kernel switch (0 = FP64 kernel, 1 = mixed kernel,
+    // 2 = none), set by the step gate and by the build's last kernel; 0 when
+    // the kernels are launched outside such a graph.
+    unsigned long long cond_forces;
 };
+
+// The arrays of the buffer set `buf` (host twin of bind_buffers).
+RCPG_HD DevArrays bound_arrays(DevArrays a, std::uint32_t buf) {
+    if (a.permute && buf) {
+        a.pos = a.pos_alt;
+        a.m = a.m_alt;
+        a.v = a.v_alt;
+        a.origin = a.origin_alt;
+        a.caps = a.caps_alt;
+        a.ref_rank = a.ref_rank_alt;
+    }
+    return a;
+}
 
 constexpr int kForceBlock = 256;
 
@@ -132,6 +178,13 @@ void launch_rebuild(const DevArrays& a, cudaStream_t st);
 // (the tiled build and the warp search; the one that has nothing to do returns)
 void launch_rebuild_timed(const DevArrays& a, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1);
 void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st);
+// One variant of the pair kernel (mixed = 0: FP64 pair terms, 1: FP32 pair
+// terms), the body of a step graph's pair-kernel switch.
+void launch_forces_variant(const DevArrays& a, int mixed, cudaStream_t st);
+// The step gate of a captured step graph: opens the build (cond_build = 1
+// when the step rebuilds its rows) and sets the pair-kernel switch for a step
+// without a build.
+void launch_step_gate(const DevArrays& a, unsigned long long cond_build, cudaStream_t st);
 void launch_reduce_exact(const DevArrays& a, cudaStream_t st);
 void launch_reduce_fast(const DevArrays& a, cudaStream_t st);
 // out[0] = max |ref[k]|, out[1] = max |cmp[k] - ref[k]| over k < n, as the bit
@@ -141,8 +194,6 @@ void launch_diff_max(const double* ref, const double* cmp, std::uint64_t n, unsi
 void launch_controller(const DevArrays& a, int open_only, cudaStream_t st);
 void launch_reorder(const DevArrays& a, cudaStream_t st);
 void launch_fix_height(const DevArrays& a, cudaStream_t st);
-// Half-row counts of the current full rows (j > i entries) into out[N].
-void launch_half_counts(const DevArrays& a, std::uint32_t* out, cudaStream_t st);
 
 void launch_pack(std::uint64_t N, int ndim, const double* x, const double* D, double* pos,
                  cudaStream_t st);
@@ -151,6 +202,10 @@ void launch_refresh_arrays(std::uint64_t N, int ndim, const double* x, double* x
                            const double* D, double* D_last, double* theta, double theta_new,
                            std::uint8_t* refresh, unsigned long long* count, cudaStream_t st);
 void launch_mean_force_blocks(const DevArrays& a, cudaStream_t st);
+// Cell-order storage -> the input's particle order (origin holds each
+// particle's input index): rows (partners mapped too), counts and forces.
+void launch_cell_order_to_particle_order(const DevArrays& a, std::uint32_t* nbr_out, std::uint32_t* cnt_out,
+                                         double* F_out, cudaStream_t st);
 void launch_rows_to_particle_order(std::uint64_t N, const std::uint32_t* work, const std::uint32_t* src,
                                    const std::uint32_t* src_cnt, std::uint32_t* dst,
                                    std::uint32_t* dst_cnt, cudaStream_t st);

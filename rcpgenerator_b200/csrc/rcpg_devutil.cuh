@@ -12,6 +12,19 @@
 namespace rcpg {
 namespace {
 
+// Points the per-particle arrays of `a` at the buffer set that holds the
+// particle state now (cell-order storage, graph mode); no-op otherwise.
+__device__ __forceinline__ void bind_buffers(DevArrays& a) {
+    if (a.permute && a.ctl->buf) {
+        a.pos = a.pos_alt;
+        a.m = a.m_alt;
+        a.v = a.v_alt;
+        a.origin = a.origin_alt;
+        a.caps = a.caps_alt;
+        a.ref_rank = a.ref_rank_alt;
+    }
+}
+
 template <int ND>
 __device__ __forceinline__ void load_pos(const double* __restrict__ pos, std::uint64_t i,
                                          double* x, double& D0) {

@@ -158,9 +158,10 @@ void Engine::alloc_device() {
     a_.N = N;
     a_.ndim = nd;
     a_.P = P_;
+    // graph mode stores the particles in cell order (every build permutes them
+    // into the second buffer set); exact mode keeps the reference's order
+    a_.permute = exact_ ? 0 : 1;
     a_.pos = static_cast<double*>(dalloc(N * P_ * sizeof(double)));
-    a_.pos_tmp = static_cast<double*>(dalloc(N * P_ * sizeof(double)));
-    a_.spos = a_.pos_tmp;  // the build's sorted copy; the reorder uses it only before a build
     a_.F = static_cast<double*>(dalloc(N * nd * sizeof(double)));
     a_.m = static_cast<double*>(dalloc(N * nd * sizeof(double)));
     a_.v = static_cast<double*>(dalloc(N * nd * sizeof(double)));
@@ -169,7 +170,20 @@ void Engine::alloc_device() {
     a_.nbr_cnt = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.caps = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.origin = static_cast<std::uint64_t*>(dalloc(N * 8));
-    a_.u64_tmp = static_cast<std::uint64_t*>(dalloc(N * 8));
+    if (a_.permute) {
+        a_.pos_alt = static_cast<double*>(dalloc(N * P_ * sizeof(double)));
+        a_.m_alt = static_cast<double*>(dalloc(N * nd * sizeof(double)));
+        a_.v_alt = static_cast<double*>(dalloc(N * nd * sizeof(double)));
+        a_.origin_alt = static_cast<std::uint64_t*>(dalloc(N * 8));
+        a_.caps_alt = static_cast<std::uint32_t*>(dalloc(N * 4));
+        a_.ref_rank = static_cast<std::uint32_t*>(dalloc(N * 4));
+        a_.ref_rank_alt = static_cast<std::uint32_t*>(dalloc(N * 4));
+    } else {
+        // the reorder's gather targets and the sorted position copy of the build
+        a_.pos_tmp = static_cast<double*>(dalloc(N * P_ * sizeof(double)));
+        a_.spos = a_.pos_tmp;  // the reorder uses it only before a build
+        a_.u64_tmp = static_cast<std::uint64_t*>(dalloc(N * 8));
+    }
     a_.cell_of = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.cell_rank = static_cast<std::uint32_t*>(dalloc(N * 4));
     a_.cell_list = static_cast<std::uint32_t*>(dalloc(N * 4));
@@ -344,6 +358,12 @@ void Engine::upload_initial() {
     check(cudaMemcpyAsync(a_.pos, pos.data(), pos.size() * 8, cudaMemcpyHostToDevice, st_), "H2D pos");
     check(cudaMemcpyAsync(a_.origin, origin.data(), N * 8, cudaMemcpyHostToDevice, st_), "H2D origin");
     check(cudaMemcpyAsync(a_.caps, caps_.data(), N * 4, cudaMemcpyHostToDevice, st_), "H2D caps");
+    std::vector<std::uint32_t> rank;
+    if (a_.permute) {
+        rank.resize(N);
+        std::iota(rank.begin(), rank.end(), 0u);
+        check(cudaMemcpyAsync(a_.ref_rank, rank.data(), N * 4, cudaMemcpyHostToDevice, st_), "H2D rank");
+    }
     check(cudaMemsetAsync(a_.m, 0, N * nd * 8, st_), "memset m");
     check(cudaMemsetAsync(a_.v, 0, N * nd * 8, st_), "memset v");
     check(cudaMemsetAsync(a_.F, 0, N * nd * 8, st_), "memset F");
@@ -435,6 +455,7 @@ Engine::~Engine() {
     cudaSetDevice(device_);
     if (sync_ev_) cudaEventDestroy(sync_ev_);
     free_device();
+    if (body_st_) cudaStreamDestroy(body_st_);
     if (own_stream_ && st_) cudaStreamDestroy(st_);
 }
 
@@ -454,7 +475,12 @@ void Engine::profile_build_kernel(std::uint32_t reps, double* avg_ms, double* al
     check(cudaEventCreate(&e1), "event");
     double total_ms = 0.0;
     for (std::uint32_t k = 0; k <= reps; ++k) {  // launch 0 warms up
+        // each build of cell-order storage moves the particles to the other
+        // buffer set: keep the set the previous build left current
+        if (k > 0) pull_ctl();
+        const std::uint32_t cur = hctl_.buf;
         hctl_ = saved;
+        hctl_.buf = cur;
         hctl_.stopped = 0u;
         hctl_.halted = 0u;
         hctl_.rebuild_flag = 1u;
@@ -481,7 +507,10 @@ void Engine::profile_build_kernel(std::uint32_t reps, double* avg_ms, double* al
     const double per = 8.0 * P_ + 12.0 + (exact_ ? 0.0 : 8.0 * ndim_);
     *avg_ms = reps ? total_ms / reps : 0.0;
     *alg_bytes = static_cast<double>(N_) * per + 4.0 * total;
+    pull_ctl();
+    const std::uint32_t cur = hctl_.buf;
     hctl_ = saved;
+    hctl_.buf = cur;
     push_ctl();
 }
 
@@ -713,14 +742,76 @@ void Engine::destroy_graph() {
     graph_ = nullptr;
 }
 
+// Kernels of one neighbour build (launch_rebuild): prepare, bin, the scan
+// (one kernel, or three for more than 4096 tiles of cells), scatter, cell
+// sort, the permutation of cell-order storage, the cell-order search
+// (ndim <= 3, N >= 20,000) and the warp search.
+std::uint64_t Engine::kernels_per_build() const {
+    const std::uint64_t cells = static_cast<std::uint64_t>(a_.C_alloc) + 1;
+    const std::uint64_t scans = cells <= 4096 ? 1 : 3;
+    std::uint64_t k = 4 + scans + (a_.permute ? 1 : 0) + 1;
+    if (ndim_ <= 3 && N_ >= 20000 && (a_.permute || a_.sorted_rows)) ++k;
+    return k;
+}
+
+template <typename Body>
+void Engine::add_conditional(int type, unsigned long long handle, unsigned size, Body body) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    std::size_t nd = 0;
+    check(cudaStreamGetCaptureInfo(st_, &status, nullptr, &g, &deps, &nd), "capture info");
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = handle;
+    p.conditional.type = static_cast<cudaGraphConditionalNodeType>(type);
+    p.conditional.size = size;
+    cudaGraphNode_t node = nullptr;
+    check(cudaGraphAddNode(&node, g, deps, nd, &p), "add conditional node");
+    for (unsigned b = 0; b < size; ++b) {
+        check(cudaStreamBeginCaptureToGraph(body_st_, p.conditional.phGraph_out[b], nullptr, nullptr, 0,
+                                            cudaStreamCaptureModeThreadLocal),
+              "capture conditional body");
+        body(body_st_, b);
+        cudaGraph_t out = nullptr;
+        check(cudaStreamEndCapture(body_st_, &out), "end conditional body");
+    }
+    check(cudaStreamUpdateCaptureDependencies(st_, &node, 1, cudaStreamSetCaptureDependencies),
+          "capture dependencies");
+}
+
+void Engine::capture_step() {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g = nullptr;
+    check(cudaStreamGetCaptureInfo(st_, &status, nullptr, &g, nullptr, nullptr), "capture info");
+    cudaGraphConditionalHandle build = 0, forces = 0;
+    check(cudaGraphConditionalHandleCreate(&build, g, 0, cudaGraphCondAssignDefault), "conditional handle");
+    check(cudaGraphConditionalHandleCreate(&forces, g, 2, cudaGraphCondAssignDefault), "conditional handle");
+    DevArrays ag = a_;
+    ag.cond_forces = forces;
+    launch_step_gate(ag, build, st_);
+    add_conditional(cudaGraphCondTypeIf, build, 1, [&](cudaStream_t s, unsigned) { launch_rebuild(ag, s); });
+    add_conditional(cudaGraphCondTypeSwitch, forces, mixed_ ? 2u : 1u,
+                    [&](cudaStream_t s, unsigned variant) { launch_forces_variant(ag, static_cast<int>(variant), s); });
+    launch_controller(ag, 0, st_);
+    launch_adam_refresh(ag, 1, 1, st_);
+}
+
+// The step loop as one CUDA graph of graph_steps_ steps. Each step opens with
+// a one-thread gate kernel; the build and the pair kernel sit in conditional
+// nodes that the gate and the build set on the device, so a step without a
+// rebuild launches four kernels (gate, pair kernel, controller, ADAM).
 void Engine::capture_graph() {
     destroy_graph();
+    if (!body_st_) check(cudaStreamCreateWithFlags(&body_st_, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal), "begin capture");
-    for (int k = 0; k < graph_steps_; ++k) {
-        launch_rebuild(a_, st_);
-        launch_forces(a_, 0, st_);
-        launch_controller(a_, 0, st_);
-        launch_adam_refresh(a_, 1, 1, st_);
+    try {
+        for (int k = 0; k < graph_steps_; ++k) capture_step();
+    } catch (...) {
+        cudaGraph_t partial = nullptr;
+        cudaStreamEndCapture(st_, &partial);
+        if (partial) cudaGraphDestroy(partial);
+        cudaGetLastError();
+        throw;
     }
     check(cudaStreamEndCapture(st_, &graph_), "end capture");
     check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
@@ -786,20 +877,29 @@ bool Engine::advance_graph(std::uint64_t max_new_steps) {
         if (max_new_steps && done_steps >= max_new_steps) break;
         const std::uint64_t want = max_new_steps ? max_new_steps - done_steps : ~0ull;
         if (!graph_exec_) capture_graph();
+        const std::uint64_t b0 = hctl_.nbuilds, f0 = hctl_.pair_kernel_runs;
+        bool replay = false;
         if (want >= static_cast<std::uint64_t>(graph_steps_)) {
             check(cudaGraphLaunch(graph_exec_, st_), "graph launch");
-            launches_ += graph_nodes_per_step_ * graph_steps_;
+            replay = true;
         } else {
             for (std::uint64_t k = 0; k < want; ++k) {
                 launch_rebuild(a_, st_);
                 launch_forces(a_, 0, st_);
                 launch_controller(a_, 0, st_);
                 launch_adam_refresh(a_, 1, 1, st_);
-                launches_ += graph_nodes_per_step_;
+                launches_ += kernels_per_build() + (mixed_ ? 4 : 3);
             }
         }
         pull_ctl();
         c = hctl_.c;
+        if (replay) {
+            // kernels the replay ran: gate, controller and ADAM of each of its
+            // steps (they return at once after a stop), and the builds and pair
+            // kernels its conditional nodes opened
+            launches_ += 3 * static_cast<std::uint64_t>(graph_steps_) +
+                         (hctl_.nbuilds - b0) * kernels_per_build() + (hctl_.pair_kernel_runs - f0);
+        }
         if (hctl_.halted) {
             if (hctl_.cap_error) {
                 throw EngineError(-ENOSPC, std::string("rcpgenerator: particle ") +
@@ -844,7 +944,7 @@ void Engine::handle_overflow_and_resume() {
     launch_forces(a_, 0, st_);
     launch_controller(a_, 0, st_);
     launch_adam_refresh(a_, 1, 1, st_);
-    launches_ += graph_nodes_per_step_;
+    launches_ += kernels_per_build() + (mixed_ ? 4 : 3);
 }
 
 bool Engine::advance(std::uint64_t max_new_steps) {
@@ -894,6 +994,35 @@ void Engine::download_histories() {
     }
 }
 
+void Engine::download_particles(std::vector<double>& pos, std::vector<std::uint64_t>* origin) {
+    const std::uint64_t N = N_;
+    pos.resize(N * P_);
+    if (origin) origin->resize(N);
+    if (!a_.permute) {
+        check(cudaMemcpyAsync(pos.data(), a_.pos, pos.size() * 8, cudaMemcpyDeviceToHost, st_), "D2H pos");
+        if (origin)
+            check(cudaMemcpyAsync(origin->data(), a_.origin, N * 8, cudaMemcpyDeviceToHost, st_), "D2H origin");
+        check(cudaStreamSynchronize(st_), "sync");
+        return;
+    }
+    // cell-order storage: the current buffer set, then particle q goes to its
+    // reference index ref_rank[q]
+    pull_ctl();
+    const DevArrays cur = bound_arrays(a_, hctl_.buf);
+    std::vector<double> cell(N * P_);
+    std::vector<std::uint64_t> org(origin ? N : 0);
+    std::vector<std::uint32_t> rank(N);
+    check(cudaMemcpyAsync(cell.data(), cur.pos, cell.size() * 8, cudaMemcpyDeviceToHost, st_), "D2H pos");
+    check(cudaMemcpyAsync(rank.data(), cur.ref_rank, N * 4, cudaMemcpyDeviceToHost, st_), "D2H rank");
+    if (origin) check(cudaMemcpyAsync(org.data(), cur.origin, N * 8, cudaMemcpyDeviceToHost, st_), "D2H origin");
+    check(cudaStreamSynchronize(st_), "sync");
+    for (std::uint64_t q = 0; q < N; ++q) {
+        const std::uint64_t r = rank[q];
+        for (int k = 0; k < P_; ++k) pos[r * P_ + k] = cell[q * P_ + k];
+        if (origin) (*origin)[r] = org[q];
+    }
+}
+
 EngineResult Engine::result() {
     if (exact_ && adam_pending_) {
         hctl_.adam_go = 1u;
@@ -912,11 +1041,8 @@ EngineResult Engine::result() {
     const std::uint64_t N = N_;
     const int nd = ndim_;
     EngineResult r;
-    std::vector<double> pos(N * P_);
-    r.particle_origin.resize(N);
-    check(cudaMemcpyAsync(pos.data(), a_.pos, pos.size() * 8, cudaMemcpyDeviceToHost, st_), "D2H pos");
-    check(cudaMemcpyAsync(r.particle_origin.data(), a_.origin, N * 8, cudaMemcpyDeviceToHost, st_), "D2H origin");
-    check(cudaStreamSynchronize(st_), "sync");
+    std::vector<double> pos;
+    download_particles(pos, &r.particle_origin);
     r.positions.resize(N * nd);
     r.diameters.resize(N);
     // diameters of the last diameter update: D = D0*kappa (ENG:5733)
@@ -1026,9 +1152,8 @@ void Engine::observe(std::uint64_t step, bool capture, const ObserverFn& observe
             adam_pending_ = false;
             hctl_.adam_go = 0u;
         }
-        std::vector<double> pos(N_ * P_);
-        check(cudaMemcpyAsync(pos.data(), a_.pos, pos.size() * 8, cudaMemcpyDeviceToHost, st_), "D2H pos");
-        check(cudaStreamSynchronize(st_), "sync");
+        std::vector<double> pos;
+        download_particles(pos, nullptr);
         xs.resize(N_ * ndim_);
         TraceSample ts;
         ts.step = step;

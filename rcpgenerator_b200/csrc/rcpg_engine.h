@@ -124,12 +124,21 @@ class Engine {
     bool step_host();
     bool advance_graph(std::uint64_t max_new_steps);
     void capture_graph();
+    // one step of the step graph: gate, conditional build, pair-kernel switch,
+    // controller, ADAM (kernels run only where the step needs them)
+    void capture_step();
+    template <typename Body>
+    void add_conditional(int type, unsigned long long handle, unsigned size, Body body);
+    std::uint64_t kernels_per_build() const;
     void destroy_graph();
     void handle_overflow_and_resume();
     void after_stop();
     void observe(std::uint64_t step, bool capture, const ObserverFn& observer,
                  std::vector<TraceSample>* trace);
     void download_histories();
+    // particle records [N*P] and particle_origin (optional) of the current
+    // state in the reference's order (graph mode stores them in cell order)
+    void download_particles(std::vector<double>& pos, std::vector<std::uint64_t>* origin);
     void check(cudaError_t e, const char* what);
 
     // configuration
@@ -169,6 +178,7 @@ class Engine {
     cudaGraphExec_t graph_exec_ = nullptr;
     cudaGraph_t graph_ = nullptr;
     std::uint64_t graph_nodes_per_step_ = 0;
+    cudaStream_t body_st_ = nullptr;  // captures the bodies of the step graph's conditional nodes
     std::uint32_t* pinned_ = nullptr;
     DevCtl* hctl_pinned_ = nullptr;
     cudaEvent_t sync_ev_ = nullptr;  // blocking-sync event (set_blocking_sync)

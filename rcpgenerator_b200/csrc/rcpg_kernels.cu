@@ -31,6 +31,13 @@ __device__ __forceinline__ bool ctl_idle(const DevCtl* ctl) {
     return (st | ha) != 0u;
 }
 
+// Value of a step graph's pair-kernel switch: 0 = FP64 kernel, 1 = mixed
+// kernel, 2 = no pair kernel (the forces are computed elsewhere or the run
+// has stopped).
+__device__ __forceinline__ unsigned forces_case(bool run, std::uint32_t pair_fp32, int mixed) {
+    return !run ? 2u : ((pair_fp32 != 0u && mixed) ? 1u : 0u);
+}
+
 // no pair-list build in this step
 __device__ __forceinline__ bool build_off(const DevCtl* ctl) {
     const std::uint32_t st = ctl->stopped, ha = ctl->halted, rb = ctl->rebuild_flag;
@@ -52,6 +59,7 @@ __global__ void __launch_bounds__(256) k_adam_refresh(DevArrays a, int do_adam, 
     const bool adam = do_adam && adam_go;
     const bool refresh = do_refresh && !stopped && mode == REBUILD_CHECK;
     if (!adam && !refresh) return;
+    bind_buffers(a);
     const double alpha = ctl->adam_alpha, ib1 = ctl->adam_inv_b1, ib2 = ctl->adam_inv_b2;
     const double fh = ctl->fix_height_scale;
     const double rk = ctl->refresh_kappa, kmin = ctl->kappa_min, theta = ctl->theta;
@@ -203,6 +211,7 @@ __global__ void __launch_bounds__(256) k_build_bin(DevArrays a) {
     if (build_off(ctl)) return;
     const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
     if (i >= a.N) return;
+    bind_buffers(a);
     double x[ND], D0;
     load_pos<ND>(a.pos, i, x, D0);
     int k = 0;  // size class
@@ -213,7 +222,7 @@ __global__ void __launch_bounds__(256) k_build_bin(DevArrays a) {
         const int cd = cell_coord(x[d], ctl->cls_scale[k][d], ctl->cls_ncell[k][d]);
         c += static_cast<std::uint32_t>(cd) * mul;
         mul *= static_cast<std::uint32_t>(ctl->cls_ncell[k][d]);
-        a.x_last[i * ND + d] = x[d];
+        if (!a.permute) a.x_last[i * ND + d] = x[d];  // cell-order storage: the permutation writes it
     }
     a.cell_of[i] = c;
     a.cell_rank[i] = atomicAdd(&a.cell_count[c], 1u);
@@ -288,9 +297,23 @@ __device__ __forceinline__ bool tiled_build_ok(const DevCtl* ctl);
 // particle over 32 lanes instead.
 constexpr std::uint64_t kTiledMinN = 20000;
 
+// the tiled search builds the rows (rows in particle order: exact mode and
+// the stand-alone pair build)
 template <int ND>
-__device__ __forceinline__ bool use_tiled(const DevCtl* ctl, std::uint64_t N) {
-    return (N >= kTiledMinN) & tiled_build_ok<ND>(ctl);
+__device__ __forceinline__ bool use_tiled(const DevArrays& a) {
+    return !a.permute && a.sorted_rows && (a.N >= kTiledMinN) && tiled_build_ok<ND>(a.ctl);
+}
+
+// the cell-order search builds the rows (graph mode, ndim 2 and 3, one size
+// class, at least 3 cells per axis)
+template <int ND>
+__device__ __forceinline__ bool use_cells(const DevArrays& a) {
+    if (ND > 3 || !a.permute || a.N < kTiledMinN) return false;
+    const DevCtl* ctl = a.ctl;
+    bool ok = ctl->nclass <= 1;
+    RCPG_UNROLL
+    for (int d = 0; d < (ND <= 3 ? ND : 3); ++d) ok = ok & (ctl->ncell[d] >= 3);
+    return ok;
 }
 
 // Builds without the tiled search: the members of each cell in ascending
@@ -301,7 +324,7 @@ __device__ __forceinline__ bool use_tiled(const DevCtl* ctl, std::uint64_t N) {
 template <int ND>
 __global__ void __launch_bounds__(256) k_build_cell_sort(DevArrays a) {
     const DevCtl* ctl = a.ctl;
-    if (build_off(ctl) | use_tiled<ND>(ctl, a.N)) return;
+    if (build_off(ctl) || use_tiled<ND>(a)) return;
     const std::uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ctl->ncells) return;
     const std::uint32_t q0 = a.cell_start[c], q1 = a.cell_start[c + 1];
@@ -314,12 +337,59 @@ __global__ void __launch_bounds__(256) k_build_cell_sort(DevArrays a) {
         }
         a.work[p] = v;
     }
+    if (a.permute) return;  // cell-order storage: k_build_permute moves the particles themselves
     constexpr int P = pos_stride(ND);
     for (std::uint32_t q = q0; q < q1; ++q) {
         const double2* src = reinterpret_cast<const double2*>(a.pos + static_cast<std::uint64_t>(a.work[q]) * P);
         double2* dst = reinterpret_cast<double2*>(a.spos + static_cast<std::uint64_t>(q) * P);
         RCPG_UNROLL
         for (int h = 0; h < P / 2; ++h) dst[h] = src[h];
+    }
+}
+
+// Cell-order storage (graph mode): particle q of the new order is particle
+// work[q] of the current one (cells in grid order, each cell's members in
+// their current order, written by k_build_cell_sort). Moves the per-particle
+// state into the other buffer set, anchors the refresh trigger there
+// (x_last = x, every build re-anchors every particle) and, once every block
+// has finished (all have read the current set), flips DevCtl::buf.
+template <int ND>
+__global__ void __launch_bounds__(256) k_build_permute(DevArrays a) {
+    DevCtl* ctl = a.ctl;
+    if (build_off(ctl)) return;
+    const std::uint32_t b = ctl->buf;
+    const DevArrays src = bound_arrays(a, b), dst = bound_arrays(a, b ^ 1u);
+    constexpr int P = pos_stride(ND);
+    const std::uint64_t N = a.N;
+    for (std::uint64_t q = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const std::uint64_t o = a.work[q];
+        const double2* ps = reinterpret_cast<const double2*>(src.pos + o * P);
+        double2* pd = reinterpret_cast<double2*>(dst.pos + q * P);
+        RCPG_UNROLL
+        for (int h = 0; h < P / 2; ++h) {
+            const double2 w = ps[h];
+            pd[h] = w;
+            if (2 * h < ND) a.x_last[q * ND + 2 * h] = w.x;
+            if (2 * h + 1 < ND) a.x_last[q * ND + 2 * h + 1] = w.y;
+        }
+        RCPG_UNROLL
+        for (int d = 0; d < ND; ++d) {
+            dst.m[q * ND + d] = src.m[o * ND + d];
+            dst.v[q * ND + d] = src.v[o * ND + d];
+        }
+        dst.origin[q] = src.origin[o];
+        dst.caps[q] = src.caps[o];
+        dst.ref_rank[q] = src.ref_rank[o];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const std::uint32_t done = atomicAdd(&ctl->permute_done, 1u);
+        if (done == gridDim.x - 1) {
+            ctl->permute_done = 0u;
+            ctl->buf = b ^ 1u;
+        }
     }
 }
 
@@ -340,7 +410,14 @@ template <int ND>
 __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArrays a) {
     DevCtl* ctl = a.ctl;
     const std::uint64_t N = a.N;
-    if (build_off(ctl) | use_tiled<ND>(ctl, N)) return;
+    const bool other = use_tiled<ND>(a) || use_cells<ND>(a);
+    if (a.cond_forces && blockIdx.x == 0 && threadIdx.x == 0 && !build_off(ctl)) {
+        // last kernel of the build in a step graph: the pair kernel runs
+        // unless another search computed this step's forces
+        const std::uint32_t fd = other ? ctl->forces_done : 0u;
+        cudaGraphSetConditional(a.cond_forces, forces_case(fd == 0u, ctl->pair_fp32, a.mixed));
+    }
+    if (build_off(ctl) || other) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->forces_done = 0u;
     __shared__ std::uint32_t buf[kWarpSearchWarps][kWarpRowSmem];
     __shared__ std::uint32_t block_need;
@@ -358,11 +435,17 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
     }
     const int K = ctl->nclass > 1 ? ctl->nclass : 1;
     std::uint32_t* row = buf[w];
+    // cell-order storage: slot t is particle t, and the cells' members are
+    // contiguous in pos itself
+    bind_buffers(a);
+    const bool perm = a.permute != 0;
+    const double* cpos = perm ? a.pos : a.spos;
     const std::uint64_t warps = static_cast<std::uint64_t>(gridDim.x) * kWarpSearchWarps;
     for (std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(kWarpSearchWarps) + w; t < N; t += warps) {
-        const std::uint32_t i = a.work[t];
+        const std::uint32_t i = perm ? static_cast<std::uint32_t>(t) : a.work[t];
+        const std::uint32_t ri = perm ? a.ref_rank[i] : i;  // the reference's index (half-row count)
         double xi[ND], D0i;
-        load_pos<ND>(a.spos, t, xi, D0i);
+        load_pos<ND>(cpos, t, xi, D0i);
         const double Di = xmul(D0i, kap);
         std::uint32_t n = 0, n_half = 0;  // n: warp-uniform row length so far
         // every grid: cells within the largest cutoff of particle i and a member
@@ -441,10 +524,10 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
                     const std::uint32_t own_cnt = __shfl_sync(0xffffffffu, cntc, own);
                     if (k < tot) {
                         const std::uint32_t q = own_q0 + (k - (own_incl - own_cnt));
-                        j = a.work[q];
+                        j = perm ? q : a.work[q];
                         if (j != i) {
                             double xj[ND], D0j;
-                            load_pos<ND>(a.spos, q, xj, D0j);
+                            load_pos<ND>(cpos, q, xj, D0j);
                             const double Dj = xmul(D0j, kap);
                             ok = (ND <= 3 || j > i) ? in_shell<ND>(xi, xj, Di, Dj, bx, ibx, t_shell)
                                                     : in_shell<ND>(xi, xj, Dj, Di, bx, ibx, t_shell);
@@ -456,7 +539,7 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
                         const std::uint32_t slot = n + __popc(mask & ((1u << lane) - 1u));
                         if (slot < static_cast<std::uint32_t>(kWarpRowSmem)) row[slot] = j;
                         else if (slot < S) a.nbr[static_cast<std::uint64_t>(slot) * N + t] = j;
-                        if (j > i) ++n_half;
+                        if (perm ? (a.ref_rank[j] > ri) : (j > i)) ++n_half;
                     }
                     n += static_cast<std::uint32_t>(__popc(mask));
                 }
@@ -468,7 +551,7 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
         if (lane == 0) {
             const std::uint32_t cap = a.caps[i];
             if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-                ctl->cap_error_particle = i;
+                ctl->cap_error_particle = ri;
                 ctl->cap_error_cap = cap;
             }
             atomicMax(&block_need, n);
@@ -544,18 +627,15 @@ template <> struct TileShape<3> {
     static constexpr int stage = 1280;
 };
 constexpr int kTileThreads = 256;
-constexpr int kTileRow = 32;  // staged row entries per thread (sorted rows)
-constexpr int kTileOvl = 16;  // staged overlap candidates per thread (mixed precision)
+constexpr int kTileRow = 32;  // staged row entries per thread
 
-// dynamic shared memory of k_build_search_tiled<ND, SORT>: the staged rows
-// (SORT only) follow the staged particles
-template <int ND, bool SORT>
+// dynamic shared memory of k_build_search_tiled<ND>: staged records, ids, row
+// slots, halo cell offsets, inner list, local cells, then the staged rows
+template <int ND>
 constexpr std::size_t tile_smem_bytes() {
     using TS = TileShape<ND <= 3 ? ND : 3>;
-    return static_cast<std::size_t>(TS::stage) * pos_stride(ND) * 8 + (SORT ? 0 : 16ull * TS::stage) +
-           2ull * TS::stage * 4 +
-           (TS::halo_cells + 2) * 4 + 2ull * TS::stage * 2 +
-           static_cast<std::size_t>(SORT ? kTileRow : kTileOvl) * kTileThreads * 2;
+    return static_cast<std::size_t>(TS::stage) * pos_stride(ND) * 8 + 2ull * TS::stage * 4 +
+           (TS::halo_cells + 2) * 4 + 2ull * TS::stage * 2 + static_cast<std::size_t>(kTileRow) * kTileThreads * 2;
 }
 
 template <int ND>
@@ -608,7 +688,10 @@ __device__ __forceinline__ void finish_row(std::uint32_t* mine, int stride, int 
     }
 }
 
-template <int ND, bool SORT>
+// Rows sorted by partner index (exact mode, rcpg_pairs_full): the reference's
+// summation order. Particles stay in their own order; row slots follow the
+// cells (work[q] = particle of slot q).
+template <int ND>
 __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArrays a) {
     constexpr int NDT = ND <= 3 ? ND : 3;
     using TS = TileShape<NDT>;
@@ -617,71 +700,42 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     constexpr int HC = TS::halo_cells;
     DevCtl* ctl = a.ctl;
     if (ND > 3) return;
-    if (build_off(ctl) | !use_tiled<ND>(ctl, a.N)) return;
+    if (build_off(ctl) || !use_tiled<ND>(a)) return;
     extern __shared__ __align__(16) unsigned char tile_smem[];
     double* s_pos = reinterpret_cast<double*>(tile_smem);
-    // mixed precision: FP32 positions relative to the tile's corner (halo
-    // cells across the periodic boundary unwrapped) and the FP32 diameter
-    float4* s_xf = reinterpret_cast<float4*>(s_pos + STAGE * P);
-    std::uint32_t* s_id = reinterpret_cast<std::uint32_t*>(SORT ? reinterpret_cast<unsigned char*>(s_xf)
-                                                                : reinterpret_cast<unsigned char*>(s_xf + STAGE));
+    std::uint32_t* s_id = reinterpret_cast<std::uint32_t*>(s_pos + STAGE * P);
     std::uint32_t* s_slot = s_id + STAGE;
     std::uint32_t* s_cstart = s_slot + STAGE;
     std::uint16_t* s_inner = reinterpret_cast<std::uint16_t*>(s_cstart + HC + 2);
     std::uint16_t* s_cell = s_inner + STAGE;
-    // [kTileRow][kTileThreads] staged row entries (SORT) or
-    // [kTileOvl][kTileThreads] staged overlap candidates (mixed precision)
-    std::uint16_t* s_rows = s_cell + STAGE;
+    std::uint16_t* s_rows = s_cell + STAGE;  // [kTileRow][kTileThreads] staged row entries
     __shared__ unsigned long long s_warp2[kTileThreads / 32];
     __shared__ std::uint32_t s_need, s_ninner;
-    __shared__ ForceSums s_red[kTileThreads / 32];
     const std::uint64_t N = a.N;
     const std::uint32_t S = a.S;
     // box of the minimum image in shared memory (the loops store through other
-    // pointers, so loads through ctl would be repeated); walls read from ctl
+    // pointers, so loads through ctl would be repeated)
     __shared__ double bx[ND], ibx[ND];
-    // per-thread sums that change once per particle (fused forces)
-    __shared__ double s_mag[kTileThreads], s_Dsum[kTileThreads];
-    __shared__ std::uint32_t s_magc[kTileThreads];
     if (threadIdx.x < ND) {
         bx[threadIdx.x] = ctl->g.box[threadIdx.x];
         ibx[threadIdx.x] = ctl->g.inv_box[threadIdx.x];
     }
-    s_mag[threadIdx.x] = 0.0;
-    s_Dsum[threadIdx.x] = 0.0;
-    s_magc[threadIdx.x] = 0u;
-    const Geometry& g = ctl->g;
     const double kap = ctl->build_kappa, t_shell = ctl->build_t_shell;
-    const bool fuse = !SORT && ctl->forces_done != 0u;
-    const bool mixed = ctl->pair_fp32 != 0u;
-    const float kapf = static_cast<float>(kap), tf = static_cast<float>(t_shell);
-    __shared__ float hbf[ND];  // half box, FP32 (mixed minimum image)
-    if (threadIdx.x < ND) hbf[threadIdx.x] = static_cast<float>(0.5 * ctl->g.box[threadIdx.x]);
     int nc[ND], nt[ND];
-    // cell width (origin of a tile's relative coordinates: its first cell's
-    // corner) and tile extent per axis (the 2-D height is chosen per build)
-    __shared__ double cellw[ND];
+    // tile extent per axis (the 2-D height is chosen per build)
     __shared__ int s_ts[ND];
     std::uint32_t tiles = 1;
     RCPG_UNROLL
     for (int d = 0; d < ND; ++d) {
         nc[d] = ctl->ncell[d];
         const int tsd = (ND == 2 && d == 1) ? ctl->tile_rows : TS::t(d);
-        if (threadIdx.x == 0) {
-            s_ts[d] = tsd;
-            cellw[d] = ctl->g.box[d] / static_cast<double>(nc[d]);
-        }
+        if (threadIdx.x == 0) s_ts[d] = tsd;
         nt[d] = (nc[d] + tsd - 1) / tsd;
         tiles *= static_cast<std::uint32_t>(nt[d]);
     }
-    __syncthreads();  // s_ts, cellw, bx, ibx, hbf
+    __syncthreads();  // s_ts, bx, ibx
     if (threadIdx.x == 0) s_need = 0u;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) ctl->nsum_blocks = gridDim.x;
     std::uint16_t* mine = s_rows + threadIdx.x;
-    // graph-mode sums of the fused forces; the wall terms join the pair
-    // chains (the reduction adds pair and wall terms anyway)
-    double fU = 0.0, fLc = 0.0, fdk = 0.0, fFm = 0.0, fmaxov = 0.0;
-    std::uint32_t fcount = 0;
     for (std::uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         int t0[ND], hw[ND];
         std::uint32_t rem = tile;
@@ -699,7 +753,6 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
         // 1. particle count of every halo cell, 2. block scans -> staging offsets
         std::uint32_t cs = 0, cnt = 0;
         bool inner_cell = false;
-        int wrap[ND];  // -1 / +1: halo cell across the lower / upper periodic boundary
         if (static_cast<int>(threadIdx.x) < H) {
             int r = threadIdx.x;
             std::uint32_t c = 0, mul = 1;
@@ -710,14 +763,8 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                 r /= hw[d];
                 inner_cell = inner_cell && l >= 1 && l <= hw[d] - 2;
                 int gc = t0[d] - 1 + l;
-                wrap[d] = 0;
-                if (gc < 0) {
-                    gc += nc[d];
-                    wrap[d] = -1;
-                } else if (gc >= nc[d]) {
-                    gc -= nc[d];
-                    wrap[d] = 1;
-                }
+                if (gc < 0) gc += nc[d];
+                else if (gc >= nc[d]) gc -= nc[d];
                 c += static_cast<std::uint32_t>(gc) * mul;
                 mul *= static_cast<std::uint32_t>(nc[d]);
             }
@@ -758,17 +805,6 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                 double2* sp = reinterpret_cast<double2*>(s_pos + dst * P);
                 RCPG_UNROLL
                 for (int h = 0; h < P / 2; ++h) sp[h] = src[h];
-                if (!SORT && mixed) {
-                    double xs[ND], D0s;
-                    load_pos<ND>(s_pos, dst, xs, D0s);
-                    float r4[4] = {0.0f, 0.0f, 0.0f, static_cast<float>(D0s) * kapf};
-                    RCPG_UNROLL
-                    for (int d = 0; d < (ND < 3 ? ND : 3); ++d) {
-                        const double xu = wrap[d] ? xadd(xs[d], wrap[d] * bx[d]) : xs[d];
-                        r4[d] = static_cast<float>(xsub(xu, xmul(static_cast<double>(t0[d]), cellw[d])));
-                    }
-                    s_xf[dst] = make_float4(r4[0], r4[1], r4[2], r4[3]);
-                }
                 s_slot[dst] = q;
                 s_cell[dst] = static_cast<std::uint16_t>(threadIdx.x);
                 if (inner_cell) {
@@ -780,8 +816,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
         __syncthreads();
         if (!fits) {
             // more halo particles than the staging area: rows of this tile from
-            // global memory, and the forces of this step by the separate pass
-            if (threadIdx.x == 0) ctl->forces_done = 0u;
+            // global memory
             for (int h = threadIdx.x; h < H; h += blockDim.x) {
                 int hl[ND];
                 int r = h;
@@ -857,7 +892,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
             }
             continue;
         }
-        // 4. rows (and forces) of the tile's own particles from shared memory
+        // 4. rows of the tile's own particles from shared memory
         for (std::uint32_t u = threadIdx.x; u < s_ninner; u += blockDim.x) {
             const std::uint32_t k = s_inner[u];
             int hl[ND];
@@ -875,146 +910,30 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
             load_pos<ND>(s_pos, k, xi, D0i);
             const double Di = xmul(D0i, kap);
             std::uint32_t n = 0, n_half = 0;
-            double fi[ND];
             // the cells x-1, x, x+1 of one halo row are consecutive halo cells,
             // so their staged particles form one contiguous range: 3^(ndim-1)
             // ranges, visited in the order of the 3^ndim cells (axis 0 fastest)
             constexpr int NROW = (ND == 2) ? 3 : 9;
             const int hbase = hl[0] - 1 + (ND == 2 ? (hl[1] - 1) * hw[0]
                                                    : (hl[1] - 1) * hw[0] + (hl[ND - 1] - 1) * hw[0] * hw[1]);
-            // candidate loop; MX: mixed precision (graph mode, unsorted rows only)
-            auto scan = [&](auto mixed_tag) {
-                constexpr bool MX = decltype(mixed_tag)::value;
-                float fif[ND];
-                RCPG_UNROLL
-                for (int d = 0; d < ND; ++d) {
-                    fi[d] = 0.0;
-                    fif[d] = 0.0f;
-                }
-                const float Dif = static_cast<float>(D0i) * kapf;
-                for (int rr = 0; rr < NROW; ++rr) {
-                    const int hc = hbase + (rr % 3) * hw[0] + (ND == 2 ? 0 : (rr / 3) * hw[0] * hw[1]);
-                    const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 3];
-                    for (std::uint32_t pp = p0; pp < p1; ++pp) {
-                        if (pp == k) continue;
-                        bool overlap;
-                        double dx[ND], d2, Dj;
-                        float dxf[ND], d2f, rsum;
-                        double xj[ND], D0j;
-                        load_pos<ND>(s_pos, pp, xj, D0j);
-                        if constexpr (MX) {
-                            // FP32 shell test on the FP64 difference, widened by
-                            // kShellMarginF so that the row holds every pair of the
-                            // FP64 shell (the list only has to hold the overlaps)
-                            d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
-                            rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
-                            const float rc = rsum + tf;
-                            if (!(d2f < rc * rc * kShellMarginF)) continue;
-                            overlap = d2f < rsum * rsum;
-                        } else {
-                            Dj = xmul(D0j, kap);
-                            d2 = pair_disp<ND>(xi, xj, bx, ibx, dx);
-                            const double r_c = shell_cut<ND>(Di, Dj, t_shell);  // ndim <= 3: symmetric
-                            if (!(d2 < xmul(r_c, r_c))) continue;
-                            overlap = false;
-                            if constexpr (!SORT) {
-                                const double r_ij = xmul(0.5, xadd(Di, Dj));
-                                overlap = d2 < xmul(r_ij, r_ij);
-                            }
-                        }
-                        const std::uint32_t j = s_id[pp];
-                        if constexpr (SORT) {
-                            if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = static_cast<std::uint16_t>(pp);
-                            else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
-                        } else {
-                            if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
-                            if (fuse && overlap) {
-                                PairTerms pt;
-                                if constexpr (MX) pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
-                                else pair_terms_f64<ND>(dx, d2, xmul(0.5, xadd(Di, Dj)), fi, pt);
-                                if (j > i) {
-                                    fU = xadd(fU, pt.U);
-                                    fLc = xadd(fLc, pt.Lc);
-                                    fdk = xadd(fdk, pt.dk);
-                                    fFm = xadd(fFm, pt.Fm);
-                                    fmaxov = fmax(fmaxov, pt.U);
-                                    ++fcount;
-                                }
-                            }
-                        }
-                        ++n;
-                        if (j > i) ++n_half;
-                    }
-                }
-                if constexpr (MX) {
-                    RCPG_UNROLL
-                    for (int d = 0; d < ND; ++d) fi[d] = static_cast<double>(fif[d]);
-                }
-            };
-            // Mixed precision, two passes. 1: every candidate is tested on the
-            // tile-relative FP32 positions (widened by kShellMarginF, so the row
-            // holds every pair of the FP64 shell), the row is written, and the
-            // possible overlaps are staged. 2: the staged candidates are decided
-            // on the FP64 difference -- the test k_forces makes -- and their
-            // forces summed in row order. Separating the passes keeps the lanes
-            // of a warp on the same instructions in the frequent test.
-            auto scan_mixed = [&]() {
-                const float4 pi4 = s_xf[k];
-                std::uint32_t nov = 0;
-                float fif[ND];
-                RCPG_UNROLL
-                for (int d = 0; d < ND; ++d) fif[d] = 0.0f;
-                auto force_of = [&](std::uint32_t pp) {
+            for (int rr = 0; rr < NROW; ++rr) {
+                const int hc = hbase + (rr % 3) * hw[0] + (ND == 2 ? 0 : (rr / 3) * hw[0] * hw[1]);
+                const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 3];
+                for (std::uint32_t pp = p0; pp < p1; ++pp) {
+                    if (pp == k) continue;
                     double xj[ND], D0j;
                     load_pos<ND>(s_pos, pp, xj, D0j);
-                    float dxf[ND];
-                    const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
-                    const float rsum = 0.5f * (pi4.w + s_xf[pp].w);
-                    if (!(d2f < rsum * rsum)) return;
-                    PairTerms pt;
-                    pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
-                    if (s_id[pp] > i) {
-                        fU = xadd(fU, pt.U);
-                        fLc = xadd(fLc, pt.Lc);
-                        fdk = xadd(fdk, pt.dk);
-                        fFm = xadd(fFm, pt.Fm);
-                        fmaxov = fmax(fmaxov, pt.U);
-                        ++fcount;
-                    }
-                };
-                for (int rr = 0; rr < NROW; ++rr) {
-                    const int hc = hbase + (rr % 3) * hw[0] + (ND == 2 ? 0 : (rr / 3) * hw[0] * hw[1]);
-                    const std::uint32_t p0 = s_cstart[hc], p1 = s_cstart[hc + 3];
-                    for (std::uint32_t pp = p0; pp < p1; ++pp) {
-                        const float4 pj = s_xf[pp];
-                        const float ex = pj.x - pi4.x, ey = pj.y - pi4.y, ez = ND == 3 ? pj.z - pi4.z : 0.0f;
-                        const float d2r = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, ex * ex));
-                        const float rsum = 0.5f * (pi4.w + pj.w);
-                        const float rc = rsum + tf;
-                        if (!(d2r < rc * rc * kShellMarginF) || pp == k) continue;
-                        const std::uint32_t j = s_id[pp];
-                        if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
-                        ++n;
-                        if (j > i) ++n_half;
-                        if (fuse && d2r < rsum * rsum * kShellMarginF) {
-                            if (nov < static_cast<std::uint32_t>(kTileOvl))
-                                mine[nov * kTileThreads] = static_cast<std::uint16_t>(pp);
-                            else
-                                force_of(pp);  // more possible overlaps than staged: at once
-                            ++nov;
-                        }
-                    }
+                    const double Dj = xmul(D0j, kap);
+                    double dx[ND];
+                    const double d2 = pair_disp<ND>(xi, xj, bx, ibx, dx);
+                    const double r_c = shell_cut<ND>(Di, Dj, t_shell);  // ndim <= 3: symmetric
+                    if (!(d2 < xmul(r_c, r_c))) continue;
+                    const std::uint32_t j = s_id[pp];
+                    if (n < static_cast<std::uint32_t>(kTileRow)) mine[n * kTileThreads] = static_cast<std::uint16_t>(pp);
+                    else if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = j;
+                    ++n;
+                    if (j > i) ++n_half;
                 }
-                const std::uint32_t ns = nov < static_cast<std::uint32_t>(kTileOvl) ? nov : kTileOvl;
-                for (std::uint32_t e = 0; e < ns; ++e) force_of(mine[e * kTileThreads]);
-                RCPG_UNROLL
-                for (int d = 0; d < ND; ++d) fi[d] = static_cast<double>(fif[d]);
-            };
-            if constexpr (!SORT) {
-                if (mixed) scan_mixed();
-                else scan(std::false_type{});
-            } else {
-                scan(std::false_type{});
             }
             const std::uint32_t cap = a.caps[i];
             if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
@@ -1024,23 +943,9 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
             atomicMax(&s_need, n);
             if (n > S) {
                 a.nbr_cnt[q] = 0;  // overflow: empty row, rebuilt after the capacity grows
-                if (fuse) ctl->forces_done = 0u;
                 continue;
             }
-            if constexpr (!SORT) {
-                a.nbr_cnt[q] = n;
-                if (fuse) {
-                    wall_forces<ND>(xi, Di, g, fi, fU, fdk, fFm, fcount);
-                    const double f2 = force_norm2<ND>(fi);
-                    if (f2 > 1.0E-16) {
-                        s_mag[threadIdx.x] = xadd(s_mag[threadIdx.x], xsqrt(f2));
-                        ++s_magc[threadIdx.x];
-                    }
-                    s_Dsum[threadIdx.x] = xadd(s_Dsum[threadIdx.x], Di);
-                    RCPG_UNROLL
-                    for (int d = 0; d < ND; ++d) a.F[static_cast<std::uint64_t>(i) * ND + d] = fi[d];
-                }
-            } else if (n <= static_cast<std::uint32_t>(kTileRow)) {
+            if (n <= static_cast<std::uint32_t>(kTileRow)) {
                 // sort the staged indices by particle id, write the row
                 for (std::uint32_t e = 1; e < n; ++e) {
                     const std::uint16_t v = mine[e * kTileThreads];
@@ -1066,21 +971,253 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     }
     __syncthreads();
     if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
+}
+
+// ---- cell-order search (graph mode, ndim 2 and 3, one size class) ---------
+// With cell-order storage the members of the cells x-1, x, x+1 of one grid
+// row are one contiguous range of particles (two where the row wraps), so a
+// particle's candidates are 3^(ndim-1) contiguous ranges of pos. One thread
+// per particle, consecutive particles per block: the block's candidates are a
+// few contiguous windows that stay in L1, and the particle's own record, row
+// length and force are coalesced. Rows hold partner indices in scan order
+// (rows of the grid in order, x ascending within a row). The step's forces are
+// computed in the same pass (graph mode): FP64 pair terms on the reference's
+// predicate, or (mixed precision) the shell test and the pair terms in FP32 on
+// FP64 differences, the shell widened by kShellMarginF so that the rows hold
+// every pair of the FP64 shell.
+constexpr int kCellThreads = 256;
+
+// The pair terms of one candidate pp of particle q (FP64 or mixed), the row
+// entry when it is in the shell; returns 1 when it entered the row.
+template <int ND, bool MX>
+struct CellScan {
+    const double* __restrict__ pos;
+    std::uint32_t* __restrict__ nbr;
+    std::uint64_t N, q;
+    std::uint32_t S;
+    double xi[ND], Di, kap, t_shell;
+    double bx[ND], ibx[ND];
+    float hbf[ND], Dif, kapf, tf;
+    bool fuse;
+    std::uint32_t n;
+    double fi[ND];
+    float fif[ND];
+    double U, Lc, dk, Fm, maxov;
+    std::uint32_t count;
+
+    __device__ __forceinline__ void candidate(std::uint64_t p) {
+        double xj[ND], D0j;
+        load_pos_g<ND>(pos, p, xj, D0j, 1);
+        PairTerms pt;
+        bool overlap;
+        if constexpr (MX) {
+            float dxf[ND];
+            const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
+            const float rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
+            const float rc = rsum + tf;
+            if (!(d2f < rc * rc * kShellMarginF)) return;
+            overlap = fuse && d2f < rsum * rsum;
+            if (overlap) pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
+        } else {
+            const double Dj = xmul(D0j, kap);
+            double dx[ND];
+            const double d2 = pair_disp<ND>(xi, xj, bx, ibx, dx);
+            const double r_c = shell_cut<ND>(Di, Dj, t_shell);  // ndim <= 3: symmetric
+            if (!(d2 < xmul(r_c, r_c))) return;
+            const double r_ij = xmul(0.5, xadd(Di, Dj));
+            overlap = fuse && d2 < xmul(r_ij, r_ij);
+            if (overlap) pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
+        }
+        if (n < S) nbr[static_cast<std::uint64_t>(n) * N + q] = static_cast<std::uint32_t>(p);
+        ++n;
+        if (overlap && p > q) {  // pair scalars once per pair, from the lower index
+            U = xadd(U, pt.U);
+            Lc = xadd(Lc, pt.Lc);
+            dk = xadd(dk, pt.dk);
+            Fm = xadd(Fm, pt.Fm);
+            maxov = fmax(maxov, pt.U);
+            ++count;
+        }
+    }
+};
+
+template <int ND, bool MX>
+__device__ __forceinline__ void cells_particle(CellScan<ND, MX>& cs, const std::uint32_t* __restrict__ cell_start,
+                                               const int* nc, const double* scale) {
+    constexpr int NDC = ND <= 3 ? ND : 3;
+    int ci[NDC];
+    RCPG_UNROLL
+    for (int d = 0; d < NDC; ++d) ci[d] = cell_coord(cs.xi[d], scale[d], nc[d]);
+    constexpr int NROW = (NDC == 2) ? 3 : 9;
+    const int xl = ci[0] - 1, xh = ci[0] + 1;
+    for (int r = 0; r < NROW; ++r) {
+        // the row's cell index of x = 0 (axes above 0 wrap periodically)
+        std::uint32_t row = 0;
+        {
+            int c1 = ci[1] + (r % 3) - 1;
+            c1 = c1 < 0 ? c1 + nc[1] : (c1 >= nc[1] ? c1 - nc[1] : c1);
+            std::uint32_t base = static_cast<std::uint32_t>(c1) * static_cast<std::uint32_t>(nc[0]);
+            if constexpr (NDC == 3) {
+                int c2 = ci[2] + (r / 3) - 1;
+                c2 = c2 < 0 ? c2 + nc[2] : (c2 >= nc[2] ? c2 - nc[2] : c2);
+                base += static_cast<std::uint32_t>(c2) * static_cast<std::uint32_t>(nc[0]) *
+                        static_cast<std::uint32_t>(nc[1]);
+            }
+            row = base;
+        }
+        // cells x-1, x, x+1 of the row: one contiguous range, or two when the
+        // row wraps (the wrapped cell is visited in its place: x - 1 first, x + 1 last)
+        std::uint32_t a0, a1, b0 = 0, b1 = 0;
+        if (xl >= 0 && xh < nc[0]) {
+            a0 = cell_start[row + xl];
+            a1 = cell_start[row + xh + 1];
+        } else if (xl < 0) {
+            a0 = cell_start[row + nc[0] - 1];
+            a1 = cell_start[row + nc[0]];
+            b0 = cell_start[row];
+            b1 = cell_start[row + 2];
+        } else {
+            a0 = cell_start[row + xl];
+            a1 = cell_start[row + nc[0]];
+            b0 = cell_start[row];
+            b1 = cell_start[row + 1];
+        }
+        for (std::uint32_t p = a0; p < a1; ++p)
+            if (p != cs.q) cs.candidate(p);
+        for (std::uint32_t p = b0; p < b1; ++p)
+            if (p != cs.q) cs.candidate(p);
+    }
+}
+
+template <int ND>
+__global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a) {
+    DevCtl* ctl = a.ctl;
+    if (build_off(ctl) || !use_cells<ND>(a)) return;
+    bind_buffers(a);
+    __shared__ ForceSums s_red[kCellThreads / 32];
+    __shared__ std::uint32_t s_need;
+    if (threadIdx.x == 0) s_need = 0u;
+    const std::uint64_t N = a.N;
+    const std::uint32_t S = a.S;
+    const Geometry g = ctl->g;  // register copy: the loops store through other pointers
+    const bool fuse = ctl->forces_done != 0u;
+    const bool mixed = ctl->pair_fp32 != 0u;
+    int nc[ND];
+    double scale[ND];
+    RCPG_UNROLL
+    for (int d = 0; d < ND; ++d) {
+        nc[d] = ctl->ncell[d];
+        scale[d] = ctl->cell_scale[d];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) ctl->nsum_blocks = gridDim.x;
+    double sU = 0.0, sLc = 0.0, sdk = 0.0, sFm = 0.0, smax = 0.0, smag = 0.0, sD = 0.0;
+    std::uint32_t scount = 0, smagc = 0, need = 0;
+    bool overflow = false;
+    for (std::uint64_t q = blockIdx.x * static_cast<std::uint64_t>(kCellThreads) + threadIdx.x; q < N;
+         q += static_cast<std::uint64_t>(gridDim.x) * kCellThreads) {
+        double fi[ND];
+        double xi[ND], D0i;
+        load_pos_g<ND>(a.pos, q, xi, D0i, 1);
+        const double Di = xmul(D0i, ctl->build_kappa);
+        std::uint32_t n = 0;
+        auto run = [&](auto mixed_tag) {
+            constexpr bool MX = decltype(mixed_tag)::value;
+            CellScan<ND, MX> cs;
+            cs.pos = a.pos;
+            cs.nbr = a.nbr;
+            cs.N = N;
+            cs.q = q;
+            cs.S = S;
+            cs.kap = ctl->build_kappa;
+            cs.t_shell = ctl->build_t_shell;
+            cs.Di = Di;
+            cs.kapf = static_cast<float>(cs.kap);
+            cs.tf = static_cast<float>(cs.t_shell);
+            cs.Dif = static_cast<float>(D0i) * cs.kapf;
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) {
+                cs.xi[d] = xi[d];
+                cs.bx[d] = g.box[d];
+                cs.ibx[d] = g.inv_box[d];
+                cs.hbf[d] = static_cast<float>(0.5 * g.box[d]);
+                cs.fi[d] = 0.0;
+                cs.fif[d] = 0.0f;
+            }
+            cs.fuse = fuse;
+            cs.n = 0;
+            cs.U = cs.Lc = cs.dk = cs.Fm = cs.maxov = 0.0;
+            cs.count = 0;
+            cells_particle<ND, MX>(cs, a.cell_start, nc, scale);
+            n = cs.n;
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) fi[d] = MX ? static_cast<double>(cs.fif[d]) : cs.fi[d];
+            sU = xadd(sU, cs.U);
+            sLc = xadd(sLc, cs.Lc);
+            sdk = xadd(sdk, cs.dk);
+            sFm = xadd(sFm, cs.Fm);
+            smax = fmax(smax, cs.maxov);
+            scount += cs.count;
+        };
+        if (mixed) run(std::true_type{});
+        else run(std::false_type{});
+        // the reference's capacity check counts the partners after i in its
+        // own order; a row that fits the capacity in full needs no count
+        const std::uint32_t cap = a.caps[q];
+        if (n > cap && n <= S) {
+            const std::uint32_t rq = a.ref_rank[q];
+            std::uint32_t n_half = 0;
+            for (std::uint32_t k = 0; k < n; ++k)
+                n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
+            if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
+                ctl->cap_error_particle = rq;
+                ctl->cap_error_cap = cap;
+            }
+        }
+        need = max(need, n);
+        if (n > S) {
+            a.nbr_cnt[q] = 0u;  // overflow: empty row, rebuilt after the capacity grows
+            overflow = true;
+            continue;
+        }
+        a.nbr_cnt[q] = n;
+        if (fuse) {
+            std::uint32_t wc = 0;
+            wall_forces<ND>(xi, Di, g, fi, sU, sdk, sFm, wc);
+            scount += wc;
+            const double f2 = force_norm2<ND>(fi);
+            if (f2 > 1.0E-16) {
+                smag = xadd(smag, xsqrt(f2));
+                ++smagc;
+            }
+            sD = xadd(sD, Di);
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) a.F[q * ND + d] = fi[d];
+        }
+    }
+    if (overflow && fuse) ctl->forces_done = 0u;
+    // block maximum of the row lengths, one atomic per block
+    RCPG_UNROLL
+    for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_xor_sync(0xffffffffu, need, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && need) atomicMax(&s_need, need);
     if (fuse) {
         ForceSums fs;
         sums_zero(fs);
-        fs.pair_U = fU;
-        fs.pair_Lc = fLc;
-        fs.pair_dk = fdk;
-        fs.pair_Fm = fFm;
-        fs.pair_maxov = fmaxov;
-        fs.sum_mag = s_mag[threadIdx.x];
-        fs.sum_D = s_Dsum[threadIdx.x];
-        fs.pair_count = fcount;
-        fs.mag_count = s_magc[threadIdx.x];
-        block_reduce_sums<kTileThreads>(fs, s_red);
+        fs.pair_U = sU;
+        fs.pair_Lc = sLc;
+        fs.pair_dk = sdk;
+        fs.pair_Fm = sFm;
+        fs.pair_maxov = smax;
+        fs.sum_mag = smag;
+        fs.sum_D = sD;
+        fs.pair_count = scount;
+        fs.mag_count = smagc;
+        block_reduce_sums<kCellThreads>(fs, s_red);  // ends with a block barrier before thread 0 reads
         if (threadIdx.x == 0) a.block_sums[blockIdx.x] = fs;
+    } else {
+        __syncthreads();
     }
+    if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
 }
 
 // ===========================================================================
@@ -1101,7 +1238,11 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
         const std::uint32_t st = ctl->stopped, ha = ctl->halted, fd = ctl->forces_done, p32 = ctl->pair_fp32;
         if ((st | ha | fd) != 0u || MIXED != (!EXACT && p32 != 0u)) return;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->nsum_blocks = gridDim.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.ctl->nsum_blocks = gridDim.x;
+        a.ctl->pair_kernel_runs += 1ull;
+    }
+    bind_buffers(a);
     const std::uint64_t N = a.N;
     const Geometry& g = ctl->g;
     double bx[ND];
@@ -1119,7 +1260,10 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
     // persistent grid: row slots t = blockIdx*256 + tid, then strides of the grid
     for (std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x; t < N;
          t += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
-        const std::uint64_t i = a.work ? a.work[t] : t;
+        // row slot t belongs to particle work[t] (rows in cell order over
+        // particles in their own order) or to particle t (cell-order storage,
+        // rows in particle order)
+        const std::uint64_t i = (a.permute || !a.work) ? t : a.work[t];
         double xi[ND], D0i;
         load_pos_g<ND>(a.pos, i, xi, D0i, 1);
         const double Di = xmul(D0i, kap);
@@ -1396,26 +1540,28 @@ __global__ void __launch_bounds__(kCtlThreads) k_controller(DevArrays a, int ope
     if (threadIdx.x == 0 && s_publish) publish_step(ctl, cs, a.ndim);
 }
 
+// First node of a step in a captured step graph: opens the build when the
+// step rebuilds its rows, and sets the pair-kernel switch for a step without
+// a build (a build's last kernel sets it once the search has decided).
+__global__ void k_step_gate(DevArrays a, unsigned long long cond_build) {
+    const DevCtl* ctl = a.ctl;
+    const std::uint32_t st = ctl->stopped, ha = ctl->halted, rb = ctl->rebuild_flag, p32 = ctl->pair_fp32;
+    const bool live = (st | ha) == 0u;
+    const bool build = live && rb != 0u;
+    cudaGraphSetConditional(cond_build, build ? 1u : 0u);
+    cudaGraphSetConditional(a.cond_forces, forces_case(live && !build, p32, a.mixed));
+}
+
 // fix_height stretch of the last coordinate without an ADAM step (used when
 // the stretch and the ADAM pass are not fused).
 template <int ND>
 __global__ void k_fix_height(DevArrays a) {
     const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
     if (i >= a.N) return;
+    bind_buffers(a);
     const double s = a.ctl->fix_height_scale;
     double* p = a.pos + i * pos_stride(ND) + (ND - 1);
     *p = xmul(*p, s);
-}
-
-template <int ND>
-__global__ void k_half_counts(DevArrays a, std::uint32_t* out) {
-    const std::uint64_t t = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
-    if (t >= a.N) return;
-    const std::uint64_t i = a.work ? a.work[t] : t;
-    const std::uint32_t n = a.nbr_cnt[t];
-    std::uint32_t h = 0;
-    for (std::uint32_t k = 0; k < n; ++k) h += a.nbr[static_cast<std::uint64_t>(k) * a.N + t] > i;
-    out[i] = h;
 }
 
 // Rows in cell order -> rows in particle order (dst[k*N + work[t]] = src[k*N + t]).
@@ -1430,30 +1576,72 @@ __global__ void k_rows_to_particle_order(std::uint64_t N, const std::uint32_t* w
     for (std::uint32_t k = 0; k < n; ++k) dst[static_cast<std::uint64_t>(k) * N + i] = src[static_cast<std::uint64_t>(k) * N + t];
 }
 
+template <int ND>
+__global__ void k_cell_order_to_particle_order(DevArrays a, std::uint32_t* nbr_out, std::uint32_t* cnt_out,
+                                               double* F_out) {
+    const std::uint64_t q = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (q >= a.N) return;
+    bind_buffers(a);
+    const std::uint64_t N = a.N, i = a.origin[q];
+    const std::uint32_t n = min(a.nbr_cnt[q], a.S);
+    cnt_out[i] = n;
+    for (std::uint32_t k = 0; k < n; ++k)
+        nbr_out[static_cast<std::uint64_t>(k) * N + i] =
+            static_cast<std::uint32_t>(a.origin[a.nbr[static_cast<std::uint64_t>(k) * N + q]]);
+    RCPG_UNROLL
+    for (int d = 0; d < ND; ++d) F_out[i * ND + d] = a.F[q * ND + d];
+}
+
 // ===========================================================================
 // R. spatial reorder: key -> stable LSD radix sort -> gather
 // ===========================================================================
+// Sort key of the reference's spatial reorder: 21-bit Morton code in 3-D,
+// the x coordinate otherwise (ENG:4850-4948).
 template <int ND>
-__global__ void k_reorder_keys(DevArrays a) {
-    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
-    if (i >= a.N) return;
-    double x[ND], D0;
-    load_pos<ND>(a.pos, i, x, D0);
-    std::uint64_t key;
+__device__ __forceinline__ std::uint64_t reorder_key(const double* x, const Geometry& g) {
     if (ND == 3) {
-        const Geometry& g = a.ctl->g;
         std::uint64_t code = 0;
 #pragma unroll
         for (int d = 0; d < 3 && d < ND; ++d) {
             const double scale = (static_cast<double>(1u << 21) - 1.0) / g.box[d];
             code |= morton_spread21(morton_axis(x[d], g.box[d], scale)) << d;
         }
-        key = code;
-    } else {
-        key = double_order_key(x[0]);
+        return code;
     }
-    a.sort_keys[0][i] = key;
+    return double_order_key(x[0]);
+}
+
+template <int ND>
+__global__ void k_reorder_keys(DevArrays a) {
+    const std::uint64_t i = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= a.N) return;
+    double x[ND], D0;
+    load_pos<ND>(a.pos, i, x, D0);
+    a.sort_keys[0][i] = reorder_key<ND>(x, a.ctl->g);
     a.sort_vals[0][i] = static_cast<std::uint32_t>(i);
+}
+
+// Cell-order storage: the reference's reorder only changes the order in which
+// results are returned. Keys are placed at each particle's reference index,
+// so the stable sort breaks ties by the previous reference order as the
+// reference's sort does; the particles themselves do not move.
+template <int ND>
+__global__ void k_reorder_keys_ranked(DevArrays a) {
+    const std::uint64_t q = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (q >= a.N) return;
+    bind_buffers(a);
+    double x[ND], D0;
+    load_pos<ND>(a.pos, q, x, D0);
+    const std::uint32_t r = a.ref_rank[q];
+    a.sort_keys[0][r] = reorder_key<ND>(x, a.ctl->g);
+    a.sort_vals[0][r] = static_cast<std::uint32_t>(q);
+}
+
+__global__ void k_reorder_ranks(DevArrays a, const std::uint32_t* perm) {
+    const std::uint64_t k = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x;
+    if (k >= a.N) return;
+    bind_buffers(a);
+    a.ref_rank[perm[k]] = static_cast<std::uint32_t>(k);
 }
 
 constexpr int kSortThreads = 256;
@@ -1639,7 +1827,8 @@ template <int ND>
 void reorder_impl(const DevArrays& a, cudaStream_t st) {
     const unsigned nb = force_blocks(a.N);
     const std::uint32_t n = static_cast<std::uint32_t>(a.N);
-    k_reorder_keys<ND><<<nb, kForceBlock, 0, st>>>(a);
+    if (a.permute) k_reorder_keys_ranked<ND><<<nb, kForceBlock, 0, st>>>(a);
+    else k_reorder_keys<ND><<<nb, kForceBlock, 0, st>>>(a);
     const std::uint32_t tiles = (n + kSortTile - 1) / kSortTile;
     int cur = 0;
     for (int pass = 0; pass < 8; ++pass) {
@@ -1652,6 +1841,10 @@ void reorder_impl(const DevArrays& a, cudaStream_t st) {
         cur ^= 1;
     }
     const std::uint32_t* perm = a.sort_vals[cur];
+    if (a.permute) {
+        k_reorder_ranks<<<nb, kForceBlock, 0, st>>>(a, perm);
+        return;
+    }
     k_reorder_gather<ND><<<nb, kForceBlock, 0, st>>>(a, perm);
     k_reorder_gather_v<ND><<<nb, kForceBlock, 0, st>>>(a, perm);
     k_reorder_commit<ND><<<nb, kForceBlock, 0, st>>>(a);
@@ -1689,22 +1882,22 @@ void forces_nd(const DevArrays& a, cudaStream_t st) {
 }
 
 // persistent grid of the tiled build: as many blocks as fit on the GPU at once
-template <int ND, bool SORT>
+template <int ND>
 void launch_tiled(const DevArrays& a, cudaStream_t st) {
     int dev = 0;
     cudaGetDevice(&dev);
-    constexpr std::size_t smem = tile_smem_bytes<ND, SORT>();
+    constexpr std::size_t smem = tile_smem_bytes<ND>();
     static int grid[64] = {};
     if (dev >= 0 && dev < 64 && grid[dev] == 0) {
-        cudaFuncSetAttribute(k_build_search_tiled<ND, SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_build_search_tiled<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
         int sms = 148, per_sm = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_search_tiled<ND, SORT>, kTileThreads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_search_tiled<ND>, kTileThreads, smem);
         grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
     }
     const int blocks = (dev >= 0 && dev < 64) ? grid[dev] : 148;
-    k_build_search_tiled<ND, SORT><<<static_cast<unsigned>(blocks), kTileThreads, smem, st>>>(a);
+    k_build_search_tiled<ND><<<static_cast<unsigned>(blocks), kTileThreads, smem, st>>>(a);
 }
 
 // e0 / e1 (optional): events recorded around the search kernels only
@@ -1717,10 +1910,16 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st, cudaEvent_t e0 = nullptr,
     scan_exclusive(a.cell_count, a.cell_start, a.C_alloc + 1, a.scan_tmp, a.ctl, st);
     k_build_scatter<<<nb, kForceBlock, 0, st>>>(a);
     k_build_cell_sort<ND><<<(a.C_alloc + 255) / 256, 256, 0, st>>>(a);
+    if (a.permute) k_build_permute<ND><<<nb, 256, 0, st>>>(a);
     if (e0) cudaEventRecord(e0, st);
-    if (ND <= 3 && a.N >= kTiledMinN) {  // smaller packings never take the tiled path
-        if (a.sorted_rows) launch_tiled<ND, true>(a, st);
-        else launch_tiled<ND, false>(a, st);
+    if (ND <= 3 && a.N >= kTiledMinN) {  // smaller packings take the warp search
+        if (a.permute) {
+            const unsigned need = static_cast<unsigned>((a.N + kCellThreads - 1) / kCellThreads),
+                           g = resident_grid<k_build_search_cells<ND>>(kCellThreads);
+            k_build_search_cells<ND><<<need < g ? need : g, kCellThreads, 0, st>>>(a);
+        } else if (a.sorted_rows) {
+            launch_tiled<ND>(a, st);
+        }
     }
     const unsigned need = static_cast<unsigned>((a.N + kWarpSearchWarps - 1) / kWarpSearchWarps),
                    g = resident_grid<k_build_search<ND>>(32 * kWarpSearchWarps);
@@ -1755,8 +1954,9 @@ void launch_rebuild_timed(const DevArrays& a, cudaStream_t st, cudaEvent_t e0, c
 }
 
 void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st) {
-    // k_forces reads a 4-double particle record (ndim <= 3) with one 256-bit load
-    if (a.P == 4 && (reinterpret_cast<std::uintptr_t>(a.pos) & 31u) != 0)
+    // k_forces (and the cell-order search) read a 4-double particle record
+    // (ndim <= 3) with one 256-bit load
+    if (a.P == 4 && (((reinterpret_cast<std::uintptr_t>(a.pos) | reinterpret_cast<std::uintptr_t>(a.pos_alt)) & 31u) != 0))
         throw std::invalid_argument("rcpgenerator_b200: particle records must be 32-byte aligned");
     if (exact_terms) {
         RCPG_DISPATCH_ND(a.ndim, (forces_nd<ND, true, false>(a, st)));
@@ -1764,6 +1964,18 @@ void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st) {
         RCPG_DISPATCH_ND(a.ndim, (forces_nd<ND, false, false>(a, st)));
         if (a.mixed) RCPG_DISPATCH_ND(a.ndim, (forces_nd<ND, false, true>(a, st)));
     }
+}
+
+void launch_forces_variant(const DevArrays& a, int mixed, cudaStream_t st) {
+    if (mixed) {
+        RCPG_DISPATCH_ND(a.ndim, (forces_nd<ND, false, true>(a, st)));
+    } else {
+        RCPG_DISPATCH_ND(a.ndim, (forces_nd<ND, false, false>(a, st)));
+    }
+}
+
+void launch_step_gate(const DevArrays& a, unsigned long long cond_build, cudaStream_t st) {
+    k_step_gate<<<1, 1, 0, st>>>(a, cond_build);
 }
 
 void launch_reduce_exact(const DevArrays& a, cudaStream_t st) {
@@ -1827,11 +2039,6 @@ void launch_fix_height(const DevArrays& a, cudaStream_t st) {
     RCPG_DISPATCH_ND(a.ndim, (k_fix_height<ND><<<nb, kForceBlock, 0, st>>>(a)));
 }
 
-void launch_half_counts(const DevArrays& a, std::uint32_t* out, cudaStream_t st) {
-    const unsigned nb = force_blocks(a.N);
-    RCPG_DISPATCH_ND(a.ndim, (k_half_counts<ND><<<nb, kForceBlock, 0, st>>>(a, out)));
-}
-
 void launch_pack(std::uint64_t N, int ndim, const double* x, const double* D, double* pos,
                  cudaStream_t st) {
     const unsigned nb = force_blocks(N);
@@ -1855,6 +2062,12 @@ void launch_rows_to_particle_order(std::uint64_t N, const std::uint32_t* work, c
                                    const std::uint32_t* src_cnt, std::uint32_t* dst,
                                    std::uint32_t* dst_cnt, cudaStream_t st) {
     k_rows_to_particle_order<<<force_blocks(N), kForceBlock, 0, st>>>(N, work, src, src_cnt, dst, dst_cnt);
+}
+
+void launch_cell_order_to_particle_order(const DevArrays& a, std::uint32_t* nbr_out, std::uint32_t* cnt_out,
+                                         double* F_out, cudaStream_t st) {
+    RCPG_DISPATCH_ND(a.ndim, (k_cell_order_to_particle_order<ND><<<force_blocks(a.N), kForceBlock, 0, st>>>(
+                                 a, nbr_out, cnt_out, F_out)));
 }
 
 void launch_mean_force_blocks(const DevArrays& a, cudaStream_t st) {

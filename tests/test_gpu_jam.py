@@ -1,0 +1,39 @@
+"""A packing of the N = 1M 2-D bidisperse workload's kind at N = 100,000, run
+to the reference's convergence gate (ENG:5603-5655: mean force < 5e-3 and
+max overlap < 5e-4 three checks in a row) in mixed and in FP64 pair
+precision. Mixed precision switches to FP64 pair terms once the max overlap
+falls below 1e-5, and its jamming fraction must stay within 1e-3 of the FP64
+run's (the tolerance the mixed path is held to); both runs end by the gate,
+not by the step cap.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CFG = dict(phi=0.30, N=100_000, Ndim=2, box=[1.0, 1.0], walls=[0, 0],
+           dist={"type": "bidisperse", "d1": 1.0, "d2": 1.4, "p": 0.5}, seed=123)
+
+
+def test_mixed_precision_jams_within_1e3_of_fp64(cuda_device):
+    import rcpgenerator_b200 as rb
+    init = rb.initialize_particles(CFG)
+    inp = {"positions": init["positions"], "diameters": init["diameters"]}
+    out = {}
+    for prec in ("mixed", "f64"):
+        out[prec] = rb.run_packing_observed(inp, {"box": init["box"], "walls": init["walls"],
+                                                  "pair_precision": prec}, 0, False, 0, None, {},
+                                            as_arrays=True)["result"]
+    m, f = out["mixed"], out["f64"]
+    for r in (m, f):
+        # ended by the convergence gate: final overlap and force below its thresholds
+        assert r["max_min_dist"] < 5e-4
+        assert r["force_history"][-1] < 5e-3
+        assert np.isfinite(r["positions"]).all()
+        assert 0.80 < r["phi"] < 0.90
+    assert m["engine_stats"]["fp64_switch_step"] > 0
+    assert np.isnan(f["engine_stats"]["pair_force_rel_error"])
+    assert abs(m["phi"] - f["phi"]) <= 1e-3
