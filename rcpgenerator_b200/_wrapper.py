@@ -185,9 +185,15 @@ class Packing:
     def _current_phi(self) -> float:
         if not self.positions or not self.diameters or not self.box:
             raise ValueError("Current realized state is unavailable")
-        box_volume = math.prod(self.box)
+        # plain left-to-right sums as the reference (WRP:267-280); Python's
+        # sum() of floats is compensated and rounds differently
+        box_volume = 1.0
+        for length in self.box:
+            box_volume *= length
         coeff = math.pi ** (self.Ndim / 2.0) / math.gamma(self.Ndim / 2.0 + 1.0)
-        volume = sum(coeff * (d / 2.0) ** self.Ndim for d in self.diameters)
+        volume = 0.0
+        for d in self.diameters:
+            volume += coeff * (d / 2.0) ** self.Ndim
         modifier = 1.0
         if self.walls and self.walls[0] < 0:
             t = -self.walls[0]

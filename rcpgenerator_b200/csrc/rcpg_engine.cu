@@ -502,9 +502,10 @@ void Engine::profile_build_kernel(std::uint32_t reps, double* avg_ms, double* al
     check(cudaStreamSynchronize(st_), "sync");
     double total = 0.0;
     for (std::uint32_t c : cnt) total += c;
-    // per particle: staged record (8P), id and row slot (8), row length (4),
-    // row entries (4k), and in graph mode the fused force F_i (8*ndim)
-    const double per = 8.0 * P_ + 12.0 + (exact_ ? 0.0 : 8.0 * ndim_);
+    // per particle: its record (8P), row length (4) and row entries (4k); the
+    // tiled search (exact mode) also stages id and row slot (8), the cell-order
+    // search (graph mode) writes the fused force F_i (8*ndim)
+    const double per = 8.0 * P_ + 4.0 + (exact_ ? 8.0 : 8.0 * ndim_);
     *avg_ms = reps ? total_ms / reps : 0.0;
     *alg_bytes = static_cast<double>(N_) * per + 4.0 * total;
     pull_ctl();
