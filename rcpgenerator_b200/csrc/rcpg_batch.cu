@@ -301,10 +301,7 @@ __device__ void b_build(const View& V, Shared& sh) {
             }
         }
         const std::uint32_t cap = V.caps[i];
-        if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-            ctl->cap_error_particle = i;
-            ctl->cap_error_cap = cap;
-        }
+        if (n_half > cap) report_cap_error(ctl, i, cap);
         need = need > n ? need : n;
         V.nbr_cnt[t] = n > S ? 0u : n;
     }

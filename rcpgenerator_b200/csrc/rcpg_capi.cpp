@@ -19,6 +19,7 @@
 #include "rcpg_batch.h"
 #include "rcpg_engine.h"
 #include "rcpg_init.h"
+#include "rcpg_setup.h"
 
 using rcpg::DevArrays;
 using rcpg::DevCtl;
@@ -230,9 +231,12 @@ int32_t rcpg_run_packing(const rcpg_packing_input* in, const rcpg_run_options* o
                          rcpg_result** out, char* err, size_t errlen) {
     if (!in || !out) return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: null argument");
     *out = nullptr;
-    if (!have_device(err, errlen)) return RCPG_ECUDA;
     try {
-        rcpg::Engine eng(make_input(in, opt));
+        // argument errors first (they need no GPU), then the device
+        const rcpg::EngineInput ei = make_input(in, opt);
+        rcpg::check_run_input(ei);
+        if (!have_device(err, errlen)) return RCPG_ECUDA;
+        rcpg::Engine eng(ei);
         std::vector<rcpg::TraceSample> trace;
         rcpg::ObserverFn fn;
         if (observer) {

@@ -55,8 +55,10 @@ struct DevCtl {
     std::uint32_t halted;         // stopped because of an error / capacity overflow
     std::uint32_t row_need;       // largest full row seen by a build
     std::uint32_t cap_error;      // a half row exceeded the reference capacity
-    std::uint32_t cap_error_particle;
-    std::uint32_t cap_error_cap;
+    // ~(particle << 32 | capacity) of the lowest-indexed particle over its
+    // capacity (the maximum of the complements: the reference's loop reports
+    // the first particle in index order); 0 = none
+    unsigned long long cap_error_key;
     std::uint32_t nbuilds;        // pair-list builds performed
     std::uint32_t fuse_forces;    // a tiled build also computes the step's forces (graph mode)
     std::uint32_t forces_done;    // this step's forces were computed by the build
@@ -150,6 +152,10 @@ struct DevArrays {
     // the kernels are launched outside such a graph.
     unsigned long long cond_forces;
 };
+
+// Particle index and capacity of the first over-capacity particle.
+inline std::uint32_t cap_error_particle(const DevCtl& c) { return static_cast<std::uint32_t>((~c.cap_error_key) >> 32); }
+inline std::uint32_t cap_error_capacity(const DevCtl& c) { return static_cast<std::uint32_t>(~c.cap_error_key); }
 
 // The arrays of the buffer set `buf` (host twin of bind_buffers).
 RCPG_HD DevArrays bound_arrays(DevArrays a, std::uint32_t buf) {

@@ -12,6 +12,13 @@
 namespace rcpg {
 namespace {
 
+// A half row over its reference capacity (the reference's overflow error,
+// ENG:647-658); the lowest particle index is kept.
+__device__ __forceinline__ void report_cap_error(DevCtl* ctl, std::uint32_t particle, std::uint32_t cap) {
+    atomicMax(&ctl->cap_error_key, ~((static_cast<unsigned long long>(particle) << 32) | cap));
+    ctl->cap_error = 1u;
+}
+
 // Points the per-particle arrays of `a` at the buffer set that holds the
 // particle state now (cell-order storage, graph mode); no-op otherwise.
 __device__ __forceinline__ void bind_buffers(DevArrays& a) {

@@ -415,9 +415,9 @@ void Engine::upload_initial() {
     }
     if (hctl_.cap_error) {
         throw EngineError(-ENOSPC, std::string("rcpgenerator: particle ") +
-                                       std::to_string(hctl_.cap_error_particle) +
+                                       std::to_string(cap_error_particle(hctl_)) +
                                        " exceeded its neighbor capacity (" +
-                                       std::to_string(hctl_.cap_error_cap) +
+                                       std::to_string(cap_error_capacity(hctl_)) +
                                        " slots) during pair-list construction (kdtree own-write). "
                                        "This usually means the per-particle neighbor allocation is too small for the size ratio in this packing. "
                                        "Recommendation: pass a larger neighbor_max (the per-particle base; e.g. neighbor_max=1500 -- capacity scales as 50*(D_i/D_min)^omega + neighbor_max), or reduce the size ratio.");
@@ -713,9 +713,9 @@ bool Engine::step_host() {
     }
     if (hctl_.cap_error) {
         throw EngineError(-ENOSPC, std::string("rcpgenerator: particle ") +
-                                       std::to_string(hctl_.cap_error_particle) +
+                                       std::to_string(cap_error_particle(hctl_)) +
                                        " exceeded its neighbor capacity (" +
-                                       std::to_string(hctl_.cap_error_cap) +
+                                       std::to_string(cap_error_capacity(hctl_)) +
                                        " slots) during pair-list construction (kdtree own-write). "
                                        "This usually means the per-particle neighbor allocation is too small for the size ratio in this packing. "
                                        "Recommendation: pass a larger neighbor_max (the per-particle base; e.g. neighbor_max=1500 -- capacity scales as 50*(D_i/D_min)^omega + neighbor_max), or reduce the size ratio.");
@@ -904,9 +904,9 @@ bool Engine::advance_graph(std::uint64_t max_new_steps) {
         if (hctl_.halted) {
             if (hctl_.cap_error) {
                 throw EngineError(-ENOSPC, std::string("rcpgenerator: particle ") +
-                                               std::to_string(hctl_.cap_error_particle) +
+                                               std::to_string(cap_error_particle(hctl_)) +
                                                " exceeded its neighbor capacity (" +
-                                               std::to_string(hctl_.cap_error_cap) +
+                                               std::to_string(cap_error_capacity(hctl_)) +
                                                " slots) during pair-list construction (kdtree own-write). "
                                                "This usually means the per-particle neighbor allocation is too small for the size ratio in this packing. "
                                                "Recommendation: pass a larger neighbor_max (the per-particle base; e.g. neighbor_max=1500 -- capacity scales as 50*(D_i/D_min)^omega + neighbor_max), or reduce the size ratio.");

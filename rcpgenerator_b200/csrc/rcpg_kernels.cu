@@ -550,10 +550,7 @@ __global__ void __launch_bounds__(32 * kWarpSearchWarps) k_build_search(DevArray
         for (int o = 16; o > 0; o >>= 1) n_half += __shfl_xor_sync(0xffffffffu, n_half, o);
         if (lane == 0) {
             const std::uint32_t cap = a.caps[i];
-            if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-                ctl->cap_error_particle = ri;
-                ctl->cap_error_cap = cap;
-            }
+            if (n_half > cap) report_cap_error(ctl, ri, cap);
             atomicMax(&block_need, n);
             a.nbr_cnt[t] = n > S ? 0u : n;  // overflow: empty row, rebuilt after the capacity grows
         }
@@ -882,10 +879,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                         }
                     }
                     const std::uint32_t cap = a.caps[i];
-                    if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-                        ctl->cap_error_particle = i;
-                        ctl->cap_error_cap = cap;
-                    }
+                    if (n_half > cap) report_cap_error(ctl, i, cap);
                     atomicMax(&s_need, n);
                     finish_row(nullptr, 0, 0, n, S, a.nbr, a.nbr_cnt, N, q);
                 }
@@ -936,10 +930,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
                 }
             }
             const std::uint32_t cap = a.caps[i];
-            if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-                ctl->cap_error_particle = i;
-                ctl->cap_error_cap = cap;
-            }
+            if (n_half > cap) report_cap_error(ctl, i, cap);
             atomicMax(&s_need, n);
             if (n > S) {
                 a.nbr_cnt[q] = 0;  // overflow: empty row, rebuilt after the capacity grows
@@ -1168,10 +1159,7 @@ __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a
             std::uint32_t n_half = 0;
             for (std::uint32_t k = 0; k < n; ++k)
                 n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
-            if (n_half > cap && atomicCAS(&ctl->cap_error, 0u, 1u) == 0u) {
-                ctl->cap_error_particle = rq;
-                ctl->cap_error_cap = cap;
-            }
+            if (n_half > cap) report_cap_error(ctl, rq, cap);
         }
         need = max(need, n);
         if (n > S) {

@@ -91,6 +91,16 @@ std::vector<std::uint32_t> pair_caps(const std::vector<double>& D, int ndim,
 // ---------------------------------------------------------------------------
 // setup (ENG:4353-4990)
 // ---------------------------------------------------------------------------
+void check_run_input(const EngineInput& in) {
+    const std::size_t nd = static_cast<std::size_t>(in.ndim);
+    if (in.positions.size() != in.N * nd || in.diameters.size() != in.N)
+        throw std::invalid_argument("rcpgenerator_b200: positions/diameters size mismatch");
+    // the reference's own checks and texts (ENG:4440, :4446)
+    if (!in.box.empty() && in.box.size() != nd) throw std::runtime_error("Error: --box length mismatch");
+    if (!in.walls.empty() && in.walls.size() != nd)
+        throw std::runtime_error("Error: --walls expects Ndim entries");
+}
+
 RunSetup prepare_run(const EngineInput& in) {
     RunSetup out;
     if (in.N == 0) throw std::invalid_argument("rcpgenerator_b200: no particles");
@@ -123,12 +133,11 @@ RunSetup prepare_run(const EngineInput& in) {
         trigger_scale = std::min(1.28 * rho, 1.9);
     }
 
+    check_run_input(in);
     std::vector<double> box = in.box;
     std::vector<std::int8_t> walls = in.walls;
     if (box.empty()) box.assign(nd, 1.0);
-    else if (box.size() != nd) throw std::runtime_error("Error: --box length mismatch");
     if (walls.empty()) walls.assign(nd, 0);
-    else if (walls.size() != nd) throw std::runtime_error("Error: --walls expects Ndim entries");
 
     double phi_modifier = 1;
     if (walls[0] < 0) {

@@ -56,6 +56,9 @@ struct RunSetup {
 };
 
 // Throws std::invalid_argument / std::runtime_error with the reference's messages.
+// The input checks of the run set-up that need no GPU: sizes, box and walls
+// lengths (std::invalid_argument / std::runtime_error with the reference's texts).
+void check_run_input(const EngineInput& in);
 RunSetup prepare_run(const EngineInput& in);
 
 // Per-row capacity of the reference pair layout (ENG:4527-4566).
