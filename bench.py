@@ -487,6 +487,8 @@ def run_single(args) -> int:
         ms = float(t.item())
         dist.barrier()
     bprof = eng.profile_build_kernel(reps=10)
+    # without the late-phase windows the pair kernel is timed on this state
+    prof = None if not args.no_late else eng.profile_pair_kernel(reps=20)
     res = eng.result(as_arrays=True)
     eng.close()
     # the same window in FP64 pair arithmetic
@@ -494,7 +496,6 @@ def run_single(args) -> int:
     eng2, (ms2, done2, _, _) = early(other)
     eng2.close()
     late = {}
-    prof = None
     if not args.no_late:
         for prec in (args.pair_precision, other):
             late[prec], p = late_phase(rb, pos, dia, init, prec, local, args.late_steps)

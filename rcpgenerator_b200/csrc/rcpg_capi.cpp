@@ -627,10 +627,19 @@ int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, co
         a.cell_rank = u32(N);
         a.cell_list = u32(N);
         a.work = u32(N);
+        // the engine's cell grids: one per size class for wide size distributions
+        DevCtl cls;
+        std::memset(&cls, 0, sizeof(cls));
+        rcpg::set_size_classes(D, cls);
         {
-            const double cutoff = (Dmax + t_shell) * (1.0 + 1e-6);
-            double cells = 1.0;
-            for (int d = 0; d < ndim; ++d) cells *= std::max(1.0, std::floor((box ? box[d] : 1.0) / cutoff));
+            double cells = 0.0;
+            for (int k = 0; k < cls.nclass; ++k) {
+                const double dmax = cls.nclass > 1 ? cls.class_d0max[k] : Dmax;
+                const double cutoff = (dmax + t_shell) * (1.0 + 1e-6);
+                double ck = 1.0;
+                for (int d = 0; d < ndim; ++d) ck *= std::max(1.0, std::floor((box ? box[d] : 1.0) / cutoff));
+                cells += ck;
+            }
             double cap = std::min(cells + 64.0, 8.0 * static_cast<double>(N) + 1024.0);
             a.C_alloc = static_cast<std::uint32_t>(std::min(cap, 2.0e9));
         }
@@ -651,6 +660,9 @@ int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, co
         h.rebuild_flag = 1u;
         h.fuse_forces = 1u;
         h.pair_fp32 = static_cast<std::uint32_t>(pair_precision);
+        h.nclass = cls.nclass;
+        std::memcpy(h.class_d0, cls.class_d0, sizeof(h.class_d0));
+        std::memcpy(h.class_d0max, cls.class_d0max, sizeof(h.class_d0max));
         std::vector<std::uint64_t> ident(N);
         for (std::uint64_t i = 0; i < N; ++i) ident[i] = i;
         std::vector<std::uint32_t> ident32(ident.begin(), ident.end());

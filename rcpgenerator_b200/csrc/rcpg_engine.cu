@@ -93,7 +93,7 @@ void pinned_ctl_release(DevCtl* p) {
 // grid is as wide as the cutoff of its largest member, so a small particle
 // does not scan cells sized for the largest one. One class when
 // D0max/D0min <= kClassRatio.
-static void set_size_classes(const std::vector<double>& D0, DevCtl& h) {
+void set_size_classes(const std::vector<double>& D0, DevCtl& h) {
     constexpr double kClassRatio = 2.5;
     double lo = D0.empty() ? 1.0 : D0[0], hi = lo;
     for (double v : D0) {

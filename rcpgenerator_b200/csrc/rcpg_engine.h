@@ -58,6 +58,10 @@ cudaError_t pool_alloc_async(void** p, std::size_t bytes, cudaStream_t st);
 DevCtl* pinned_ctl_acquire();
 void pinned_ctl_release(DevCtl* p);
 
+// Size classes of the cell grids (one grid per doubling of D0 when
+// max/min D0 > 2.5, else one grid) into h.nclass, class_d0, class_d0max.
+void set_size_classes(const std::vector<double>& D0, DevCtl& h);
+
 class EngineError : public std::runtime_error {
    public:
     EngineError(int code, const std::string& msg) : std::runtime_error(msg), code_(code) {}
