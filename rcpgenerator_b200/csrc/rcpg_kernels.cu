@@ -967,28 +967,35 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
 // ---- cell-order search (graph mode, ndim 2 and 3, one size class) ---------
 // With cell-order storage the members of the cells x-1, x, x+1 of one grid
 // row are one contiguous range of particles (two where the row wraps), so a
-// particle's candidates are 3^(ndim-1) contiguous ranges of pos. One thread
-// per particle, consecutive particles per block: the block's candidates are a
-// few contiguous windows that stay in L1, and the particle's own record, row
-// length and force are coalesced. Rows hold partner indices in scan order
-// (rows of the grid in order, x ascending within a row). The step's forces are
-// computed in the same pass (graph mode): FP64 pair terms on the reference's
-// predicate, or (mixed precision) the shell test and the pair terms in FP32 on
-// FP64 differences, the shell widened by kShellMarginF so that the rows hold
-// every pair of the FP64 shell.
-constexpr int kCellThreads = 256;
+// particle's candidates are 3^(ndim-1) contiguous ranges of pos. A warp takes
+// 32 consecutive particles; their ranges of one row offset overlap, and their
+// union is one contiguous window, which the warp copies into shared memory
+// with coalesced loads before any lane scans it (the cells at the wrap of a
+// row, and windows that do not fit, are read from global memory). One thread
+// per particle then tests its candidates in scan order -- rows of the grid in
+// order, x ascending within a row -- so rows hold partner indices in that
+// order. The step's forces are computed in the same pass (graph mode): FP64
+// pair terms on the reference's predicate, or (mixed precision) the shell
+// test and the pair terms in FP32 on FP64 differences, the shell widened by
+// kShellMarginF so that the rows hold every pair of the FP64 shell.
+constexpr int kCellWarps = 4;  // warps per block
+constexpr int kCellThreads = 32 * kCellWarps;
+// staged particle records per warp (2-D: the 3 windows of ~40 particles at the
+// bench's occupancy; 3-D: the 9 windows of ~45)
+template <int ND> struct CellStage { static constexpr int cap = 192; };
+template <> struct CellStage<3> { static constexpr int cap = 416; };
 
-// The pair terms of one candidate pp of particle q (FP64 or mixed), the row
-// entry when it is in the shell; returns 1 when it entered the row.
+// One particle's candidate tests (FP64 or mixed) and its row and force sums.
 template <int ND, bool MX>
 struct CellScan {
-    const double* __restrict__ pos;
     std::uint32_t* __restrict__ nbr;
     std::uint64_t N, q;
     std::uint32_t S;
     double xi[ND], Di, kap, t_shell;
-    double bx[ND], ibx[ND];
-    float hbf[ND], Dif, kapf, tf;
+    const double* bx;   // box (shared memory)
+    const double* ibx;  // 1 / box (shared memory)
+    const float* hbf;   // half box, FP32 (shared memory)
+    float Dif, kapf, tf;
     bool fuse;
     std::uint32_t n;
     double fi[ND];
@@ -996,9 +1003,8 @@ struct CellScan {
     double U, Lc, dk, Fm, maxov;
     std::uint32_t count;
 
-    __device__ __forceinline__ void candidate(std::uint64_t p) {
-        double xj[ND], D0j;
-        load_pos_g<ND>(pos, p, xj, D0j, 1);
+    // candidate p with record (xj, D0j): shell test, row entry, pair terms
+    __device__ __forceinline__ void test(std::uint64_t p, const double* xj, double D0j) {
         PairTerms pt;
         bool overlap;
         if constexpr (MX) {
@@ -1032,162 +1038,228 @@ struct CellScan {
     }
 };
 
-template <int ND, bool MX>
-__device__ __forceinline__ void cells_particle(CellScan<ND, MX>& cs, const std::uint32_t* __restrict__ cell_start,
-                                               const int* nc, const double* scale) {
-    constexpr int NDC = ND <= 3 ? ND : 3;
-    int ci[NDC];
-    RCPG_UNROLL
-    for (int d = 0; d < NDC; ++d) ci[d] = cell_coord(cs.xi[d], scale[d], nc[d]);
-    constexpr int NROW = (NDC == 2) ? 3 : 9;
+// Candidate ranges of row offset r (0 .. 3^(ndim-1) - 1) of the particle in
+// cell ci: [a0, a1) and, where the row wraps in x, [b0, b1) (the wrapped cell
+// is visited in its place: x - 1 first, x + 1 last).
+template <int NDC>
+__device__ __forceinline__ void cell_row_ranges(int r, const int* ci, const int* nc,
+                                                const std::uint32_t* __restrict__ cell_start, std::uint32_t& a0,
+                                                std::uint32_t& a1, std::uint32_t& b0, std::uint32_t& b1) {
+    int c1 = ci[1] + (r % 3) - 1;
+    c1 = c1 < 0 ? c1 + nc[1] : (c1 >= nc[1] ? c1 - nc[1] : c1);
+    std::uint32_t row = static_cast<std::uint32_t>(c1) * static_cast<std::uint32_t>(nc[0]);
+    if constexpr (NDC == 3) {
+        int c2 = ci[2] + (r / 3) - 1;
+        c2 = c2 < 0 ? c2 + nc[2] : (c2 >= nc[2] ? c2 - nc[2] : c2);
+        row += static_cast<std::uint32_t>(c2) * static_cast<std::uint32_t>(nc[0]) * static_cast<std::uint32_t>(nc[1]);
+    }
     const int xl = ci[0] - 1, xh = ci[0] + 1;
-    for (int r = 0; r < NROW; ++r) {
-        // the row's cell index of x = 0 (axes above 0 wrap periodically)
-        std::uint32_t row = 0;
-        {
-            int c1 = ci[1] + (r % 3) - 1;
-            c1 = c1 < 0 ? c1 + nc[1] : (c1 >= nc[1] ? c1 - nc[1] : c1);
-            std::uint32_t base = static_cast<std::uint32_t>(c1) * static_cast<std::uint32_t>(nc[0]);
-            if constexpr (NDC == 3) {
-                int c2 = ci[2] + (r / 3) - 1;
-                c2 = c2 < 0 ? c2 + nc[2] : (c2 >= nc[2] ? c2 - nc[2] : c2);
-                base += static_cast<std::uint32_t>(c2) * static_cast<std::uint32_t>(nc[0]) *
-                        static_cast<std::uint32_t>(nc[1]);
-            }
-            row = base;
-        }
-        // cells x-1, x, x+1 of the row: one contiguous range, or two when the
-        // row wraps (the wrapped cell is visited in its place: x - 1 first, x + 1 last)
-        std::uint32_t a0, a1, b0 = 0, b1 = 0;
-        if (xl >= 0 && xh < nc[0]) {
-            a0 = cell_start[row + xl];
-            a1 = cell_start[row + xh + 1];
-        } else if (xl < 0) {
-            a0 = cell_start[row + nc[0] - 1];
-            a1 = cell_start[row + nc[0]];
-            b0 = cell_start[row];
-            b1 = cell_start[row + 2];
-        } else {
-            a0 = cell_start[row + xl];
-            a1 = cell_start[row + nc[0]];
-            b0 = cell_start[row];
-            b1 = cell_start[row + 1];
-        }
-        for (std::uint32_t p = a0; p < a1; ++p)
-            if (p != cs.q) cs.candidate(p);
-        for (std::uint32_t p = b0; p < b1; ++p)
-            if (p != cs.q) cs.candidate(p);
+    b0 = b1 = 0;
+    if (xl >= 0 && xh < nc[0]) {
+        a0 = cell_start[row + xl];
+        a1 = cell_start[row + xh + 1];
+    } else if (xl < 0) {
+        a0 = cell_start[row + nc[0] - 1];
+        a1 = cell_start[row + nc[0]];
+        b0 = cell_start[row];
+        b1 = cell_start[row + 2];
+    } else {
+        a0 = cell_start[row + xl];
+        a1 = cell_start[row + nc[0]];
+        b0 = cell_start[row];
+        b1 = cell_start[row + 1];
     }
 }
 
 template <int ND>
 __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a) {
+    constexpr int NDC = ND <= 3 ? ND : 3;
+    constexpr int NROW = (NDC == 2) ? 3 : 9;
+    constexpr int CAP = CellStage<NDC>::cap;
+    constexpr int P = pos_stride(ND);
     DevCtl* ctl = a.ctl;
     if (build_off(ctl) || !use_cells<ND>(a)) return;
     bind_buffers(a);
-    __shared__ ForceSums s_red[kCellThreads / 32];
+    extern __shared__ __align__(16) double cell_stage[];  // [kCellWarps][CAP][P]
+    __shared__ ForceSums s_red[kCellWarps];
     __shared__ std::uint32_t s_need;
+    __shared__ std::uint32_t s_win[kCellWarps][NROW][3];  // window base, end, stage offset
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* stage = cell_stage + static_cast<std::size_t>(warp) * CAP * P;
     if (threadIdx.x == 0) s_need = 0u;
     const std::uint64_t N = a.N;
     const std::uint32_t S = a.S;
-    const Geometry g = ctl->g;  // register copy: the loops store through other pointers
+    // block-wide constants in shared memory (fewer registers per thread)
+    __shared__ Geometry s_g;
+    __shared__ double s_scale[NDC];
+    __shared__ float s_hbf[ND];
+    __shared__ int s_nc[NDC];
+    if (threadIdx.x == 0) {
+        s_g = ctl->g;
+        for (int d = 0; d < NDC; ++d) {
+            s_nc[d] = ctl->ncell[d];
+            s_scale[d] = ctl->cell_scale[d];
+        }
+        for (int d = 0; d < ND; ++d) s_hbf[d] = static_cast<float>(0.5 * ctl->g.box[d]);
+    }
     const bool fuse = ctl->forces_done != 0u;
     const bool mixed = ctl->pair_fp32 != 0u;
-    int nc[ND];
-    double scale[ND];
-    RCPG_UNROLL
-    for (int d = 0; d < ND; ++d) {
-        nc[d] = ctl->ncell[d];
-        scale[d] = ctl->cell_scale[d];
-    }
+    __syncthreads();
+    const Geometry& g = s_g;
+    const int* nc = s_nc;
+    const double* scale = s_scale;
     if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) ctl->nsum_blocks = gridDim.x;
     double sU = 0.0, sLc = 0.0, sdk = 0.0, sFm = 0.0, smax = 0.0, smag = 0.0, sD = 0.0;
     std::uint32_t scount = 0, smagc = 0, need = 0;
     bool overflow = false;
-    for (std::uint64_t q = blockIdx.x * static_cast<std::uint64_t>(kCellThreads) + threadIdx.x; q < N;
-         q += static_cast<std::uint64_t>(gridDim.x) * kCellThreads) {
-        double fi[ND];
-        double xi[ND], D0i;
-        load_pos_g<ND>(a.pos, q, xi, D0i, 1);
-        const double Di = xmul(D0i, ctl->build_kappa);
-        std::uint32_t n = 0;
-        auto run = [&](auto mixed_tag) {
-            constexpr bool MX = decltype(mixed_tag)::value;
-            CellScan<ND, MX> cs;
-            cs.pos = a.pos;
-            cs.nbr = a.nbr;
-            cs.N = N;
-            cs.q = q;
-            cs.S = S;
-            cs.kap = ctl->build_kappa;
-            cs.t_shell = ctl->build_t_shell;
-            cs.Di = Di;
-            cs.kapf = static_cast<float>(cs.kap);
-            cs.tf = static_cast<float>(cs.t_shell);
-            cs.Dif = static_cast<float>(D0i) * cs.kapf;
-            RCPG_UNROLL
-            for (int d = 0; d < ND; ++d) {
-                cs.xi[d] = xi[d];
-                cs.bx[d] = g.box[d];
-                cs.ibx[d] = g.inv_box[d];
-                cs.hbf[d] = static_cast<float>(0.5 * g.box[d]);
-                cs.fi[d] = 0.0;
-                cs.fif[d] = 0.0f;
+    const std::uint64_t wstride = static_cast<std::uint64_t>(gridDim.x) * kCellWarps * 32;
+    for (std::uint64_t q0 = (static_cast<std::uint64_t>(blockIdx.x) * kCellWarps + warp) * 32; q0 < N;
+         q0 += wstride) {
+        const std::uint64_t q = q0 + lane;
+        const bool valid = q < N;
+        double xi[ND], D0i = 0.0;
+        int ci[NDC];
+        RCPG_UNROLL
+        for (int d = 0; d < ND; ++d) xi[d] = 0.0;
+        if (valid) load_pos_g<ND>(a.pos, q, xi, D0i, 1);
+        RCPG_UNROLL
+        for (int d = 0; d < NDC; ++d) ci[d] = cell_coord(xi[d], scale[d], nc[d]);
+        // 1. the warp's window of every row offset: the union of its lanes'
+        // main ranges (consecutive particles: overlapping, contiguous ranges)
+        std::uint32_t total = 0;
+        for (int r = 0; r < NROW; ++r) {
+            std::uint32_t a0 = 0, a1 = 0, b0, b1;
+            if (valid) cell_row_ranges<NDC>(r, ci, nc, a.cell_start, a0, a1, b0, b1);
+            const std::uint32_t u0 = __reduce_min_sync(0xffffffffu, valid ? a0 : 0xffffffffu);
+            const std::uint32_t u1 = __reduce_max_sync(0xffffffffu, valid ? a1 : 0u);
+            const std::uint32_t len = u1 > u0 ? u1 - u0 : 0u;
+            if (lane == 0) {
+                s_win[warp][r][0] = u0;
+                s_win[warp][r][1] = u0 + len;
+                s_win[warp][r][2] = total;
             }
-            cs.fuse = fuse;
-            cs.n = 0;
-            cs.U = cs.Lc = cs.dk = cs.Fm = cs.maxov = 0.0;
-            cs.count = 0;
-            cells_particle<ND, MX>(cs, a.cell_start, nc, scale);
-            n = cs.n;
-            RCPG_UNROLL
-            for (int d = 0; d < ND; ++d) fi[d] = MX ? static_cast<double>(cs.fif[d]) : cs.fi[d];
-            sU = xadd(sU, cs.U);
-            sLc = xadd(sLc, cs.Lc);
-            sdk = xadd(sdk, cs.dk);
-            sFm = xadd(sFm, cs.Fm);
-            smax = fmax(smax, cs.maxov);
-            scount += cs.count;
-        };
-        if (mixed) run(std::true_type{});
-        else run(std::false_type{});
-        // the reference's capacity check counts the partners after i in its
-        // own order; a row that fits the capacity in full needs no count
-        const std::uint32_t cap = a.caps[q];
-        if (n > cap && n <= S) {
-            const std::uint32_t rq = a.ref_rank[q];
-            std::uint32_t n_half = 0;
-            for (std::uint32_t k = 0; k < n; ++k)
-                n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
-            if (n_half > cap) report_cap_error(ctl, rq, cap);
+            total += len;
         }
-        need = max(need, n);
-        if (n > S) {
-            a.nbr_cnt[q] = 0u;  // overflow: empty row, rebuilt after the capacity grows
-            overflow = true;
-            continue;
-        }
-        a.nbr_cnt[q] = n;
-        if (fuse) {
-            std::uint32_t wc = 0;
-            wall_forces<ND>(xi, Di, g, fi, sU, sdk, sFm, wc);
-            scount += wc;
-            const double f2 = force_norm2<ND>(fi);
-            if (f2 > 1.0E-16) {
-                smag = xadd(smag, xsqrt(f2));
-                ++smagc;
+        __syncwarp();
+        const bool staged = total <= static_cast<std::uint32_t>(CAP);
+        // 2. copy the windows' records (coalesced, 16 bytes per lane and load)
+        if (staged) {
+            for (int r = 0; r < NROW; ++r) {
+                const std::uint32_t u0 = s_win[warp][r][0], u1 = s_win[warp][r][1], off = s_win[warp][r][2];
+                const double2* src = reinterpret_cast<const double2*>(a.pos + static_cast<std::uint64_t>(u0) * P);
+                double2* dst = reinterpret_cast<double2*>(stage + static_cast<std::size_t>(off) * P);
+                const std::uint32_t nw = (u1 - u0) * (P / 2);
+                for (std::uint32_t k = lane; k < nw; k += 32) dst[k] = __ldg(src + k);
             }
-            sD = xadd(sD, Di);
-            RCPG_UNROLL
-            for (int d = 0; d < ND; ++d) a.F[q * ND + d] = fi[d];
         }
+        __syncwarp();
+        if (valid) {
+            const double Di = xmul(D0i, ctl->build_kappa);
+            double fi[ND];
+            std::uint32_t n = 0;
+            auto run = [&](auto mixed_tag) {
+                constexpr bool MX = decltype(mixed_tag)::value;
+                CellScan<ND, MX> cs;
+                cs.nbr = a.nbr;
+                cs.N = N;
+                cs.q = q;
+                cs.S = S;
+                cs.kap = ctl->build_kappa;
+                cs.t_shell = ctl->build_t_shell;
+                cs.Di = Di;
+                cs.kapf = static_cast<float>(cs.kap);
+                cs.tf = static_cast<float>(cs.t_shell);
+                cs.Dif = static_cast<float>(D0i) * cs.kapf;
+                cs.bx = g.box;
+                cs.ibx = g.inv_box;
+                cs.hbf = s_hbf;
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) {
+                    cs.xi[d] = xi[d];
+                    cs.fi[d] = 0.0;
+                    cs.fif[d] = 0.0f;
+                }
+                cs.fuse = fuse;
+                cs.n = 0;
+                cs.U = cs.Lc = cs.dk = cs.Fm = cs.maxov = 0.0;
+                cs.count = 0;
+                for (int r = 0; r < NROW; ++r) {
+                    std::uint32_t a0, a1, b0, b1;
+                    cell_row_ranges<NDC>(r, ci, nc, a.cell_start, a0, a1, b0, b1);
+                    double xj[ND], D0j;
+                    if (staged) {
+                        // this lane's range lies inside the warp's window [u0, u1)
+                        const double* w = stage + static_cast<std::size_t>(s_win[warp][r][2]) * P;
+                        const std::uint32_t u0 = s_win[warp][r][0];
+                        for (std::uint32_t p = a0; p < a1; ++p) {
+                            if (p == q) continue;
+                            load_pos<ND>(w, p - u0, xj, D0j);
+                            cs.test(p, xj, D0j);
+                        }
+                    } else {
+                        for (std::uint32_t p = a0; p < a1; ++p) {
+                            if (p == q) continue;
+                            load_pos_g<ND>(a.pos, p, xj, D0j, 1);
+                            cs.test(p, xj, D0j);
+                        }
+                    }
+                    for (std::uint32_t p = b0; p < b1; ++p) {
+                        if (p == q) continue;
+                        load_pos_g<ND>(a.pos, p, xj, D0j, 1);
+                        cs.test(p, xj, D0j);
+                    }
+                }
+                n = cs.n;
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) fi[d] = MX ? static_cast<double>(cs.fif[d]) : cs.fi[d];
+                sU = xadd(sU, cs.U);
+                sLc = xadd(sLc, cs.Lc);
+                sdk = xadd(sdk, cs.dk);
+                sFm = xadd(sFm, cs.Fm);
+                smax = fmax(smax, cs.maxov);
+                scount += cs.count;
+            };
+            if (mixed) run(std::true_type{});
+            else run(std::false_type{});
+            // the reference's capacity check counts the partners after i in its
+            // own order; a row that fits the capacity in full needs no count
+            const std::uint32_t cap = a.caps[q];
+            if (n > cap && n <= S) {
+                const std::uint32_t rq = a.ref_rank[q];
+                std::uint32_t n_half = 0;
+                for (std::uint32_t k = 0; k < n; ++k)
+                    n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
+                if (n_half > cap) report_cap_error(ctl, rq, cap);
+            }
+            need = max(need, n);
+            if (n > S) {
+                a.nbr_cnt[q] = 0u;  // overflow: empty row, rebuilt after the capacity grows
+                overflow = true;
+            } else {
+                a.nbr_cnt[q] = n;
+                if (fuse) {
+                    std::uint32_t wc = 0;
+                    wall_forces<ND>(xi, Di, g, fi, sU, sdk, sFm, wc);
+                    scount += wc;
+                    const double f2 = force_norm2<ND>(fi);
+                    if (f2 > 1.0E-16) {
+                        smag = xadd(smag, xsqrt(f2));
+                        ++smagc;
+                    }
+                    sD = xadd(sD, Di);
+                    RCPG_UNROLL
+                    for (int d = 0; d < ND; ++d) a.F[q * ND + d] = fi[d];
+                }
+            }
+        }
+        __syncwarp();  // the stage is reused by the warp's next particles
     }
     if (overflow && fuse) ctl->forces_done = 0u;
     // block maximum of the row lengths, one atomic per block
     RCPG_UNROLL
     for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_xor_sync(0xffffffffu, need, o));
     __syncthreads();
-    if ((threadIdx.x & 31) == 0 && need) atomicMax(&s_need, need);
+    if (lane == 0 && need) atomicMax(&s_need, need);
     if (fuse) {
         ForceSums fs;
         sums_zero(fs);
@@ -1206,6 +1278,12 @@ __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a
         __syncthreads();
     }
     if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
+}
+
+// dynamic shared memory of k_build_search_cells<ND>
+template <int ND>
+constexpr std::size_t cells_smem_bytes() {
+    return static_cast<std::size_t>(kCellWarps) * CellStage<(ND <= 3 ? ND : 3)>::cap * pos_stride(ND) * 8;
 }
 
 // ===========================================================================
@@ -1431,7 +1509,7 @@ __global__ void k_reduce_exact(DevArrays a) {
 }
 
 // Fixed-order reduction of the per-block partial sums by one block.
-constexpr int kCtlThreads = 1024;
+constexpr int kCtlThreads = 256;
 
 __device__ void reduce_blocks(const DevArrays& a, ForceSums* smem, ForceSums& out) {
     const unsigned nb = a.ctl->nsum_blocks;
@@ -1888,6 +1966,26 @@ void launch_tiled(const DevArrays& a, cudaStream_t st) {
     k_build_search_tiled<ND><<<static_cast<unsigned>(blocks), kTileThreads, smem, st>>>(a);
 }
 
+// persistent grid of the cell-order search: the blocks resident at once
+template <int ND>
+void launch_cells(const DevArrays& a, cudaStream_t st) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    constexpr std::size_t smem = cells_smem_bytes<ND>();
+    static int grid[64] = {};
+    if (dev >= 0 && dev < 64 && grid[dev] == 0) {
+        cudaFuncSetAttribute(k_build_search_cells<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+        int sms = 148, per_sm = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_search_cells<ND>, kCellThreads, smem);
+        grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    const unsigned g = (dev >= 0 && dev < 64) ? static_cast<unsigned>(grid[dev]) : 148u;
+    const unsigned need = static_cast<unsigned>((a.N + kCellThreads - 1) / kCellThreads);
+    k_build_search_cells<ND><<<need < g ? need : g, kCellThreads, smem, st>>>(a);
+}
+
 // e0 / e1 (optional): events recorded around the search kernels only
 template <int ND>
 void rebuild_impl(const DevArrays& a, cudaStream_t st, cudaEvent_t e0 = nullptr, cudaEvent_t e1 = nullptr) {
@@ -1902,9 +2000,7 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st, cudaEvent_t e0 = nullptr,
     if (e0) cudaEventRecord(e0, st);
     if (ND <= 3 && a.N >= kTiledMinN) {  // smaller packings take the warp search
         if (a.permute) {
-            const unsigned need = static_cast<unsigned>((a.N + kCellThreads - 1) / kCellThreads),
-                           g = resident_grid<k_build_search_cells<ND>>(kCellThreads);
-            k_build_search_cells<ND><<<need < g ? need : g, kCellThreads, 0, st>>>(a);
+            launch_cells<ND>(a, st);
         } else if (a.sorted_rows) {
             launch_tiled<ND>(a, st);
         }

@@ -25,7 +25,7 @@ def main(argv=None) -> dict:
     ap.add_argument("--count", type=int, default=4096)
     ap.add_argument("--seed0", type=int, default=0)
     ap.add_argument("--n-min", type=int, default=64)
-    ap.add_argument("--n-max", type=int, default=2048)
+    ap.add_argument("--n-max", type=int, default=16384)
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--lr", type=float, default=1e-3)

@@ -11,7 +11,8 @@ own criterion; the time saved is in the rung, whose length also sets the
 oscillation period that follows it.
 
 Network: inputs are the first 8 moments of d/<d> (as log(m_k)/k), Ndim, a
-hard-wall flag and a container flag (11 values, standardised); 3 hidden layers
+hard-wall flag, a container flag and log N (12 values, standardised; a model
+trained without log N takes the first 11); 3 hidden layers
 of 256 GELU units; 17 outputs: phi_J and the growth curve phi(t_k)/phi_J at 16
 knots t_k = 250 * 2^(k/2) steps (k = 0..15, 250 to 45,255 steps). Weights are
 BF16 with FP32 master copies and FP32 accumulation; training and inference run
@@ -35,7 +36,7 @@ import numpy as np
 from . import _native as N
 from ._api import initialize_particles, run_packing_batch
 
-WIDTHS = (11, 256, 256, 256, 17)
+WIDTHS = (12, 256, 256, 256, 17)
 KNOT_STEPS = np.round(250.0 * 2.0 ** (np.arange(16) / 2.0)).astype(np.int64)
 N_FEATURES = WIDTHS[0]
 MODEL_PATH = Path(__file__).resolve().parent / "warmstart_model.npz"
@@ -43,17 +44,19 @@ MODEL_PATH = Path(__file__).resolve().parent / "warmstart_model.npz"
 
 # ---- descriptors and targets ---------------------------------------------------
 
-def descriptors(diameters, ndim: int, walls=()) -> np.ndarray:
-    """The network's 11 raw inputs for one packing: log(m_k)/k for the moments
+def descriptors(diameters, ndim: int, walls=(), with_n: bool = False) -> np.ndarray:
+    """The network's raw inputs for one packing: log(m_k)/k for the moments
     m_k = <(d/<d>)^k>, k = 1..8; Ndim; 1.0 if any hard wall (walls[k] > 0);
-    1.0 if a container (walls[0] < 0)."""
+    1.0 if a container (walls[0] < 0); with ``with_n`` also log N (12 values,
+    else 11)."""
     d = np.asarray(diameters, dtype=np.float64)
     r = d / d.mean()
     mom = [math.log(float(np.mean(r ** k))) / k for k in range(1, 9)]
     w = np.asarray(walls, dtype=np.int64).ravel()
     hard = float(np.any(w > 0)) if w.size else 0.0
     cont = float(w[0] < 0) if w.size else 0.0
-    return np.asarray(mom + [float(ndim), hard, cont], dtype=np.float64)
+    extra = [math.log(float(d.size))] if with_n else []
+    return np.asarray(mom + [float(ndim), hard, cont] + extra, dtype=np.float64)
 
 
 def reference_growth_steps(N: int, ndim: int) -> int:
@@ -215,7 +218,7 @@ class WarmStart:
         xs = np.where(xs > 1e-9, xs, 1.0)
         ym, ys = Y.mean(0), Y.std(0)
         ys = np.where(ys > 1e-9, ys, 1.0)
-        net = Network(seed=seed, device=device)
+        net = Network(widths=(X.shape[1],) + tuple(WIDTHS[1:]), seed=seed, device=device)
         Xn = net._dev((X - xm) / xs)
         Yn = net._dev((Y - ym) / ys)
         ow = np.ones(Y.shape[1])
@@ -260,8 +263,9 @@ class WarmStart:
 
     def plan(self, items: list) -> tuple[np.ndarray, np.ndarray]:
         """For [(input, config), ...]: predicted phi_J and growth-rung lengths."""
+        with_n = self.net.widths[0] > 11
         X = np.stack([descriptors(inp["diameters"], np.asarray(inp["positions"]).shape[1],
-                                  cfg.get("walls", [])) for inp, cfg in items])
+                                  cfg.get("walls", []), with_n) for inp, cfg in items])
         P = self.predict(X)
         gs = np.asarray([self.growth_steps_from_prediction(P[k], len(items[k][0]["diameters"]),
                                                            np.asarray(items[k][0]["positions"]).shape[1])
@@ -341,17 +345,17 @@ def draw_evaluation_packing(seed: int, N: int = 100_000, phi: float = 0.10) -> t
             {"box": init["box"], "walls": init["walls"], "neighbor_max": 0, "seed": seed})
 
 
-def generate_training_set(count: int, seed0: int = 0, n_range=(64, 2048), options: dict | None = None,
+def generate_training_set(count: int, seed0: int = 0, n_range=(64, 16384), options: dict | None = None,
                           concurrency: int = 0, chunk: int = 1024) -> tuple[np.ndarray, np.ndarray]:
     """Runs ``count`` plain packings (draw_packing, seeds seed0..) in the batch
-    engine and returns their descriptors X [count x 11] and targets
-    Y [count x 17]."""
+    engine and returns their descriptors X [count x 12] (with log N) and
+    targets Y [count x 17]."""
     X, Y = [], []
     for s0 in range(seed0, seed0 + count, chunk):
         items = [draw_packing(s, n_range) for s in range(s0, min(s0 + chunk, seed0 + count))]
         res = run_packing_batch(items, options, concurrency)
         for (inp, cfg), r in zip(items, res):
-            X.append(descriptors(inp["diameters"], np.asarray(inp["positions"]).shape[1], cfg["walls"]))
+            X.append(descriptors(inp["diameters"], np.asarray(inp["positions"]).shape[1], cfg["walls"], True))
             Y.append(targets(r))
     return np.asarray(X), np.asarray(Y)
 

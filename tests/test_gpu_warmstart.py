@@ -20,7 +20,7 @@ def test_shipped_model_predicts_phi_J_by_dimension(cuda_device):
     W, ws = _ws()
     mono = np.ones(1000)
     for nd, lo, hi in [(2, 0.82, 0.88), (3, 0.62, 0.67), (4, 0.42, 0.50)]:
-        p = ws.predict(W.descriptors(mono, nd, [0] * nd))[0]
+        p = ws.predict(W.descriptors(mono, nd, [0] * nd, ws.net.widths[0] > 11))[0]
         assert lo <= p[0] <= hi, (nd, p[0])
         # the predicted growth curve is a ratio to phi_J that ends at ~1
         assert np.all(p[1:] > 0.7) and abs(p[-1] - 1.0) < 0.02
@@ -55,7 +55,7 @@ def test_training_pipeline_from_engine_packings(cuda_device):
     trainer: a small set fits its own phi_J far better than the spread."""
     W = pytest.importorskip("rcpgenerator_b200.warmstart")
     X, Y = W.generate_training_set(48, seed0=777, n_range=(64, 256), options={"pair_precision": "mixed"})
-    assert X.shape == (48, 11) and Y.shape == (48, 17)
+    assert X.shape == (48, 12) and Y.shape == (48, 17)
     assert np.all((Y[:, 0] > 0.3) & (Y[:, 0] < 0.95))
     ws = W.WarmStart.fit(X, Y, epochs=150, batch=48, lr=2e-3)
     P = ws.predict(X)

@@ -16,7 +16,8 @@ from rcpgenerator_b200 import warmstart as W
 def test_descriptors():
     d = np.array([1.0, 1.0, 1.4, 1.4])
     x = W.descriptors(d, 3, [0, 0, 0])
-    assert x.shape == (W.N_FEATURES,)
+    assert x.shape == (11,)
+    assert W.descriptors(d, 3, [0, 0, 0], with_n=True)[11] == pytest.approx(math.log(4.0))
     r = d / d.mean()
     for k in range(1, 9):
         assert x[k - 1] == pytest.approx(math.log(np.mean(r ** k)) / k, rel=1e-14, abs=1e-15)
