@@ -746,12 +746,16 @@ void Engine::destroy_graph() {
 // Kernels of one neighbour build (launch_rebuild): prepare, bin, the scan
 // (one kernel, or three for more than 4096 tiles of cells), scatter, cell
 // sort, the permutation of cell-order storage, the cell-order search
-// (ndim <= 3, N >= 20,000) and the warp search.
+// (ndim <= 3, N >= 20,000; one kernel per pair precision the run may use) or
+// the tiled search, and the warp search.
 std::uint64_t Engine::kernels_per_build() const {
     const std::uint64_t cells = static_cast<std::uint64_t>(a_.C_alloc) + 1;
     const std::uint64_t scans = cells <= 4096 ? 1 : 3;
     std::uint64_t k = 4 + scans + (a_.permute ? 1 : 0) + 1;
-    if (ndim_ <= 3 && N_ >= 20000 && (a_.permute || a_.sorted_rows)) ++k;
+    if (ndim_ <= 3 && N_ >= 20000) {
+        if (a_.permute) k += a_.mixed ? 2 : 1;
+        else if (a_.sorted_rows) k += 1;
+    }
     return k;
 }
 

@@ -361,26 +361,52 @@ __global__ void __launch_bounds__(256) k_build_permute(DevArrays a) {
     const DevArrays src = bound_arrays(a, b), dst = bound_arrays(a, b ^ 1u);
     constexpr int P = pos_stride(ND);
     const std::uint64_t N = a.N;
-    for (std::uint64_t q = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x; q < N;
-         q += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
-        const std::uint64_t o = a.work[q];
-        const double2* ps = reinterpret_cast<const double2*>(src.pos + o * P);
-        double2* pd = reinterpret_cast<double2*>(dst.pos + q * P);
+    // two particles per thread, every load of both before any store
+    const std::uint64_t stride = static_cast<std::uint64_t>(gridDim.x) * blockDim.x;
+    for (std::uint64_t q0 = blockIdx.x * static_cast<std::uint64_t>(blockDim.x) + threadIdx.x; q0 < N;
+         q0 += 2 * stride) {
+        constexpr int U = 2;
+        double2 rec[U][P / 2];
+        double mv[U][2 * ND];
+        std::uint64_t org[U];
+        std::uint32_t cap[U], rr[U];
         RCPG_UNROLL
-        for (int h = 0; h < P / 2; ++h) {
-            const double2 w = ps[h];
-            pd[h] = w;
-            if (2 * h < ND) a.x_last[q * ND + 2 * h] = w.x;
-            if (2 * h + 1 < ND) a.x_last[q * ND + 2 * h + 1] = w.y;
+        for (int u = 0; u < U; ++u) {
+            const std::uint64_t q = q0 + u * stride;
+            if (q >= N) continue;
+            const std::uint64_t o = a.work[q];
+            const double2* ps = reinterpret_cast<const double2*>(src.pos + o * P);
+            RCPG_UNROLL
+            for (int h = 0; h < P / 2; ++h) rec[u][h] = ps[h];
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) {
+                mv[u][d] = src.m[o * ND + d];
+                mv[u][ND + d] = src.v[o * ND + d];
+            }
+            org[u] = src.origin[o];
+            cap[u] = src.caps[o];
+            rr[u] = src.ref_rank[o];
         }
         RCPG_UNROLL
-        for (int d = 0; d < ND; ++d) {
-            dst.m[q * ND + d] = src.m[o * ND + d];
-            dst.v[q * ND + d] = src.v[o * ND + d];
+        for (int u = 0; u < U; ++u) {
+            const std::uint64_t q = q0 + u * stride;
+            if (q >= N) continue;
+            double2* pd = reinterpret_cast<double2*>(dst.pos + q * P);
+            RCPG_UNROLL
+            for (int h = 0; h < P / 2; ++h) {
+                pd[h] = rec[u][h];
+                if (2 * h < ND) a.x_last[q * ND + 2 * h] = rec[u][h].x;
+                if (2 * h + 1 < ND) a.x_last[q * ND + 2 * h + 1] = rec[u][h].y;
+            }
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) {
+                dst.m[q * ND + d] = mv[u][d];
+                dst.v[q * ND + d] = mv[u][ND + d];
+            }
+            dst.origin[q] = org[u];
+            dst.caps[q] = cap[u];
+            dst.ref_rank[q] = rr[u];
         }
-        dst.origin[q] = src.origin[o];
-        dst.caps[q] = src.caps[o];
-        dst.ref_rank[q] = src.ref_rank[o];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -970,20 +996,28 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
 // particle's candidates are 3^(ndim-1) contiguous ranges of pos. A warp takes
 // 32 consecutive particles; their ranges of one row offset overlap, and their
 // union is one contiguous window, which the warp copies into shared memory
-// with coalesced loads before any lane scans it (the cells at the wrap of a
-// row, and windows that do not fit, are read from global memory). One thread
-// per particle then tests its candidates in scan order -- rows of the grid in
-// order, x ascending within a row -- so rows hold partner indices in that
-// order. The step's forces are computed in the same pass (graph mode): FP64
+// with coalesced loads before any lane scans it, as FP32 positions relative to
+// the warp's first particle (minimum image taken in FP64 before rounding) and
+// FP32 diameters (the cells at the wrap of a row, and windows that do not fit,
+// are read from global memory). One thread per particle then tests its
+// candidates in scan order -- rows of the grid in order, x ascending within a
+// row -- so rows hold partner indices in that order: an FP32 test on the
+// relative positions, with the shell widened by kPrefilter (far more than
+// their rounding), passes a candidate to the exact test on its FP64 record. The step's forces are computed in the same pass (graph mode): FP64
 // pair terms on the reference's predicate, or (mixed precision) the shell
 // test and the pair terms in FP32 on FP64 differences, the shell widened by
 // kShellMarginF so that the rows hold every pair of the FP64 shell.
 constexpr int kCellWarps = 4;  // warps per block
 constexpr int kCellThreads = 32 * kCellWarps;
-// staged particle records per warp (2-D: the 3 windows of ~40 particles at the
+// staged particles per warp (2-D: the 3 windows of ~40 particles at the
 // bench's occupancy; 3-D: the 9 windows of ~45)
 template <int ND> struct CellStage { static constexpr int cap = 192; };
 template <> struct CellStage<3> { static constexpr int cap = 416; };
+// Relative widening of r_c^2 in the FP32 prefilter of the staged candidates.
+// Their relative positions span a few cells, so their rounding moves a
+// distance by ~1e-6 of the cutoff; a candidate rejected here fails the exact
+// test by a wide margin.
+constexpr float kPrefilter = 1.001f;
 
 // One particle's candidate tests (FP64 or mixed) and its row and force sums.
 template <int ND, bool MX>
@@ -1071,21 +1105,39 @@ __device__ __forceinline__ void cell_row_ranges(int r, const int* ci, const int*
     }
 }
 
+// Position relative to xref (minimum image per axis in FP64, then rounded to
+// FP32) and the FP32 diameter of a staged candidate.
 template <int ND>
-__global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a) {
+__device__ __forceinline__ float4 rel_record(const double* x, double D0, const double* xref, const double* box) {
+    float r[3] = {0.0f, 0.0f, 0.0f};
+    RCPG_UNROLL
+    for (int d = 0; d < (ND < 3 ? ND : 3); ++d) {
+        double dd = x[d] - xref[d];
+        const double h = 0.5 * box[d];
+        if (dd > h) dd -= box[d];
+        else if (dd < -h) dd += box[d];
+        r[d] = static_cast<float>(dd);
+    }
+    return make_float4(r[0], r[1], r[2], static_cast<float>(D0));
+}
+
+// MX: the mixed-precision variant (FP32 pair terms); each variant returns at
+// once when the step's pair precision is the other one.
+template <int ND, bool MX>
+__global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells(DevArrays a) {
     constexpr int NDC = ND <= 3 ? ND : 3;
     constexpr int NROW = (NDC == 2) ? 3 : 9;
     constexpr int CAP = CellStage<NDC>::cap;
     constexpr int P = pos_stride(ND);
     DevCtl* ctl = a.ctl;
-    if (build_off(ctl) || !use_cells<ND>(a)) return;
+    if (build_off(ctl) || !use_cells<ND>(a) || MX != (ctl->pair_fp32 != 0u)) return;
     bind_buffers(a);
-    extern __shared__ __align__(16) double cell_stage[];  // [kCellWarps][CAP][P]
+    extern __shared__ __align__(16) float4 cell_stage[];  // [kCellWarps][CAP]: x, y, z relative, D0
     __shared__ ForceSums s_red[kCellWarps];
     __shared__ std::uint32_t s_need;
     __shared__ std::uint32_t s_win[kCellWarps][NROW][3];  // window base, end, stage offset
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double* stage = cell_stage + static_cast<std::size_t>(warp) * CAP * P;
+    float4* stage = cell_stage + static_cast<std::size_t>(warp) * CAP;
     if (threadIdx.x == 0) s_need = 0u;
     const std::uint64_t N = a.N;
     const std::uint32_t S = a.S;
@@ -1103,7 +1155,6 @@ __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a
         for (int d = 0; d < ND; ++d) s_hbf[d] = static_cast<float>(0.5 * ctl->g.box[d]);
     }
     const bool fuse = ctl->forces_done != 0u;
-    const bool mixed = ctl->pair_fp32 != 0u;
     __syncthreads();
     const Geometry& g = s_g;
     const int* nc = s_nc;
@@ -1124,6 +1175,10 @@ __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a
         if (valid) load_pos_g<ND>(a.pos, q, xi, D0i, 1);
         RCPG_UNROLL
         for (int d = 0; d < NDC; ++d) ci[d] = cell_coord(xi[d], scale[d], nc[d]);
+        // origin of the warp's relative positions: its first particle
+        double xref[ND];
+        RCPG_UNROLL
+        for (int d = 0; d < ND; ++d) xref[d] = __shfl_sync(0xffffffffu, xi[d], 0);
         // 1. the warp's window of every row offset: the union of its lanes'
         // main ranges (consecutive particles: overlapping, contiguous ranges)
         std::uint32_t total = 0;
@@ -1142,14 +1197,16 @@ __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a
         }
         __syncwarp();
         const bool staged = total <= static_cast<std::uint32_t>(CAP);
-        // 2. copy the windows' records (coalesced, 16 bytes per lane and load)
+        // 2. stage the windows: one particle per lane and round (its 32-byte
+        // record), as relative FP32 position and FP32 diameter
         if (staged) {
             for (int r = 0; r < NROW; ++r) {
                 const std::uint32_t u0 = s_win[warp][r][0], u1 = s_win[warp][r][1], off = s_win[warp][r][2];
-                const double2* src = reinterpret_cast<const double2*>(a.pos + static_cast<std::uint64_t>(u0) * P);
-                double2* dst = reinterpret_cast<double2*>(stage + static_cast<std::size_t>(off) * P);
-                const std::uint32_t nw = (u1 - u0) * (P / 2);
-                for (std::uint32_t k = lane; k < nw; k += 32) dst[k] = __ldg(src + k);
+                for (std::uint32_t k = lane; k < u1 - u0; k += 32) {
+                    double xs[ND], D0s;
+                    load_pos_g<ND>(a.pos, u0 + k, xs, D0s, 1);
+                    stage[off + k] = rel_record<ND>(xs, D0s, xref, g.box);
+                }
             }
         }
         __syncwarp();
@@ -1157,8 +1214,8 @@ __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a
             const double Di = xmul(D0i, ctl->build_kappa);
             double fi[ND];
             std::uint32_t n = 0;
-            auto run = [&](auto mixed_tag) {
-                constexpr bool MX = decltype(mixed_tag)::value;
+            const float4 me = rel_record<ND>(xi, D0i, xref, g.box);
+            {
                 CellScan<ND, MX> cs;
                 cs.nbr = a.nbr;
                 cs.N = N;
@@ -1189,11 +1246,15 @@ __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a
                     double xj[ND], D0j;
                     if (staged) {
                         // this lane's range lies inside the warp's window [u0, u1)
-                        const double* w = stage + static_cast<std::size_t>(s_win[warp][r][2]) * P;
+                        const float4* w = stage + s_win[warp][r][2];
                         const std::uint32_t u0 = s_win[warp][r][0];
                         for (std::uint32_t p = a0; p < a1; ++p) {
-                            if (p == q) continue;
-                            load_pos<ND>(w, p - u0, xj, D0j);
+                            const float4 c = w[p - u0];
+                            const float ex = c.x - me.x, ey = c.y - me.y, ez = NDC == 3 ? c.z - me.z : 0.0f;
+                            const float d2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, ex * ex));
+                            const float rc = 0.5f * (cs.Dif + c.w * cs.kapf) + cs.tf;
+                            if (!(d2 < rc * rc * kPrefilter) || p == q) continue;
+                            load_pos_g<ND>(a.pos, p, xj, D0j, 1);
                             cs.test(p, xj, D0j);
                         }
                     } else {
@@ -1218,9 +1279,7 @@ __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a
                 sFm = xadd(sFm, cs.Fm);
                 smax = fmax(smax, cs.maxov);
                 scount += cs.count;
-            };
-            if (mixed) run(std::true_type{});
-            else run(std::false_type{});
+            }
             // the reference's capacity check counts the partners after i in its
             // own order; a row that fits the capacity in full needs no count
             const std::uint32_t cap = a.caps[q];
@@ -1283,7 +1342,7 @@ __global__ void __launch_bounds__(kCellThreads) k_build_search_cells(DevArrays a
 // dynamic shared memory of k_build_search_cells<ND>
 template <int ND>
 constexpr std::size_t cells_smem_bytes() {
-    return static_cast<std::size_t>(kCellWarps) * CellStage<(ND <= 3 ? ND : 3)>::cap * pos_stride(ND) * 8;
+    return static_cast<std::size_t>(kCellWarps) * CellStage<(ND <= 3 ? ND : 3)>::cap * sizeof(float4);
 }
 
 // ===========================================================================
@@ -1967,23 +2026,31 @@ void launch_tiled(const DevArrays& a, cudaStream_t st) {
 }
 
 // persistent grid of the cell-order search: the blocks resident at once
-template <int ND>
-void launch_cells(const DevArrays& a, cudaStream_t st) {
+template <int ND, bool MX>
+void launch_cells_variant(const DevArrays& a, cudaStream_t st) {
     int dev = 0;
     cudaGetDevice(&dev);
     constexpr std::size_t smem = cells_smem_bytes<ND>();
     static int grid[64] = {};
     if (dev >= 0 && dev < 64 && grid[dev] == 0) {
-        cudaFuncSetAttribute(k_build_search_cells<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_build_search_cells<ND, MX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
         int sms = 148, per_sm = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_search_cells<ND>, kCellThreads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_search_cells<ND, MX>, kCellThreads, smem);
         grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
     }
     const unsigned g = (dev >= 0 && dev < 64) ? static_cast<unsigned>(grid[dev]) : 148u;
     const unsigned need = static_cast<unsigned>((a.N + kCellThreads - 1) / kCellThreads);
-    k_build_search_cells<ND><<<need < g ? need : g, kCellThreads, smem, st>>>(a);
+    k_build_search_cells<ND, MX><<<need < g ? need : g, kCellThreads, smem, st>>>(a);
+}
+
+// both precisions where the run may use FP32 pair terms (the one that does
+// not match the step returns at once)
+template <int ND>
+void launch_cells(const DevArrays& a, cudaStream_t st) {
+    launch_cells_variant<ND, false>(a, st);
+    if (a.mixed) launch_cells_variant<ND, true>(a, st);
 }
 
 // e0 / e1 (optional): events recorded around the search kernels only
@@ -1996,7 +2063,11 @@ void rebuild_impl(const DevArrays& a, cudaStream_t st, cudaEvent_t e0 = nullptr,
     scan_exclusive(a.cell_count, a.cell_start, a.C_alloc + 1, a.scan_tmp, a.ctl, st);
     k_build_scatter<<<nb, kForceBlock, 0, st>>>(a);
     k_build_cell_sort<ND><<<(a.C_alloc + 255) / 256, 256, 0, st>>>(a);
-    if (a.permute) k_build_permute<ND><<<nb, 256, 0, st>>>(a);
+    if (a.permute) {
+        // persistent grid, two particles per thread and round
+        const unsigned need = (nb + 1) / 2, g = resident_grid<k_build_permute<ND>>(256);
+        k_build_permute<ND><<<need < g ? need : g, 256, 0, st>>>(a);
+    }
     if (e0) cudaEventRecord(e0, st);
     if (ND <= 3 && a.N >= kTiledMinN) {  // smaller packings take the warp search
         if (a.permute) {
