@@ -604,12 +604,14 @@ def run_jam(args) -> int:
     for prec in ("mixed", "f64"):
         t0 = time.perf_counter()
         r = rb.run_packing_observed(inp, {"box": init["box"], "walls": init["walls"], "device": local,
-                                          "pair_precision": prec}, 0, False, 0, None, {}, as_arrays=True)["result"]
+                                          "pair_precision": prec}, 0, False, 0, None,
+                                    {"max_steps": args.jam_max_steps}, as_arrays=True)["result"]
         dt = time.perf_counter() - t0
         st = r["engine_stats"]
         runs[prec] = r
         out[prec] = {"phi_J": float(r["phi"]), "steps": int(r["steps"]), "max_overlap": float(r["max_min_dist"]),
                      "force_magnitude": float(r["force_magnitude"]), "wall_s": dt, "steps_per_s": r["steps"] / dt,
+                     "converged": bool(r["steps"] < args.jam_max_steps),
                      "pair_builds": int(st["pair_builds"]), "fp64_switch_step": int(st["fp64_switch_step"]),
                      "pair_energy_rel_error": float(st["pair_energy_rel_error"]),
                      "pair_force_rel_error": float(st["pair_force_rel_error"])}
@@ -646,6 +648,8 @@ def main() -> int:
                          "one: ADAM steps/s of packing --seed of the batch generator (profiling); "
                          "jam: one packing of --jam-config run to convergence in mixed and FP64 precision")
     ap.add_argument("--jam-config", type=int, default=2, choices=[2, 3])
+    ap.add_argument("--jam-max-steps", type=int, default=400_000,
+                    help="jam workload: step cap of each run (a run that reaches it did not converge)")
     ap.add_argument("--seed", type=int, default=4, help="one: generator seed (4: 4-D, N = 11,948)")
     ap.add_argument("--batch-count", type=int, default=128)
     ap.add_argument("--batch-stride", type=int, default=0,

@@ -1002,8 +1002,13 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
 // are read from global memory). One thread per particle then tests its
 // candidates in scan order -- rows of the grid in order, x ascending within a
 // row -- so rows hold partner indices in that order: an FP32 test on the
-// relative positions, with the shell widened by kPrefilter (far more than
-// their rounding), passes a candidate to the exact test on its FP64 record. The step's forces are computed in the same pass (graph mode): FP64
+// relative positions, with the shell widened beyond their rounding, passes a
+// candidate to the exact test on its FP64 record. The relative positions of
+// a lane and of its candidates differ by the minimum image only while the
+// lane lies more than a neighbourhood away from the wrap of the warp's frame
+// (half a box from the first particle); a warp spread over more than half
+// the box (dilute packings, containers with empty rows) has lanes that do
+// not, and those test every candidate exactly from global memory. The step's forces are computed in the same pass (graph mode): FP64
 // pair terms on the reference's predicate, or (mixed precision) the shell
 // test and the pair terms in FP32 on FP64 differences, the shell widened by
 // kShellMarginF so that the rows hold every pair of the FP64 shell.
@@ -1013,11 +1018,20 @@ constexpr int kCellThreads = 32 * kCellWarps;
 // bench's occupancy; 3-D: the 9 windows of ~45)
 template <int ND> struct CellStage { static constexpr int cap = 192; };
 template <> struct CellStage<3> { static constexpr int cap = 416; };
-// Relative widening of r_c^2 in the FP32 prefilter of the staged candidates.
-// Their relative positions span a few cells, so their rounding moves a
-// distance by ~1e-6 of the cutoff; a candidate rejected here fails the exact
-// test by a wide margin.
-constexpr float kPrefilter = 1.001f;
+// entries of a lane's list of candidates for the exact test
+constexpr int kCellList = 32;
+// Widening of the cutoff r_c in the FP32 prefilter of the staged candidates:
+// relative (kPrefilterLin, for the rounding of diameters and of the cutoff
+// arithmetic) plus an absolute term for the rounding of relative positions of
+// magnitude up to half the box h (each coordinate within 2^-24 h, so a
+// distance within sqrt(3) 2^-23 h < 2^-21 h). A candidate rejected here fails
+// the exact test.
+constexpr float kPrefilterLin = 1.0005f;
+constexpr float kPrefilterAbs = 4.76837158203125e-07f;  // 2^-21
+// A lane's relative position must lie this many cells inside the wrap of the
+// warp's frame for its staged candidates to be tested there (a pair is
+// nearer than one cell per axis).
+constexpr float kFrameGuardCells = 1.5f;
 
 // One particle's candidate tests (FP64 or mixed) and its row and force sums.
 template <int ND, bool MX>
@@ -1133,6 +1147,8 @@ __global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells
     if (build_off(ctl) || !use_cells<ND>(a) || MX != (ctl->pair_fp32 != 0u)) return;
     bind_buffers(a);
     extern __shared__ __align__(16) float4 cell_stage[];  // [kCellWarps][CAP]: x, y, z relative, D0
+    // [kCellWarps][kCellList][32]: each lane's candidates for the exact test
+    std::uint32_t* cell_lists = reinterpret_cast<std::uint32_t*>(cell_stage + kCellWarps * CAP);
     __shared__ ForceSums s_red[kCellWarps];
     __shared__ std::uint32_t s_need;
     __shared__ std::uint32_t s_win[kCellWarps][NROW][3];  // window base, end, stage offset
@@ -1145,13 +1161,20 @@ __global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells
     __shared__ Geometry s_g;
     __shared__ double s_scale[NDC];
     __shared__ float s_hbf[ND];
+    __shared__ float s_guard[NDC];  // |relative position| below which a lane uses the stage
+    __shared__ float s_eabs;        // absolute widening of the prefilter cutoff
     __shared__ int s_nc[NDC];
     if (threadIdx.x == 0) {
         s_g = ctl->g;
+        double hmax = 0.0;
         for (int d = 0; d < NDC; ++d) {
             s_nc[d] = ctl->ncell[d];
             s_scale[d] = ctl->cell_scale[d];
+            const double h = 0.5 * ctl->g.box[d];
+            hmax = fmax(hmax, h);
+            s_guard[d] = static_cast<float>(h - kFrameGuardCells / ctl->cell_scale[d]);
         }
+        s_eabs = static_cast<float>(hmax) * kPrefilterAbs;
         for (int d = 0; d < ND; ++d) s_hbf[d] = static_cast<float>(0.5 * ctl->g.box[d]);
     }
     const bool fuse = ctl->forces_done != 0u;
@@ -1240,11 +1263,39 @@ __global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells
                 cs.n = 0;
                 cs.U = cs.Lc = cs.dk = cs.Fm = cs.maxov = 0.0;
                 cs.count = 0;
+                // the stage serves this lane when its relative position keeps
+                // its candidates' differences at their minimum image
+                bool use_stage = staged;
+                use_stage = use_stage && fabsf(me.x) < s_guard[0] && fabsf(me.y) < s_guard[1];
+                if constexpr (NDC == 3) use_stage = use_stage && fabsf(me.z) < s_guard[2];
+                // prefilter cutoff of a candidate with FP32 diameter w: w * pa + pb
+                const float pa = 0.5f * cs.kapf * kPrefilterLin;
+                const float pb = __fmaf_rn(0.5f * cs.Dif + cs.tf, kPrefilterLin, s_eabs);
+                // The lane's candidates in scan order go through two phases:
+                // the FP32 prefilter (staged ones) fills the lane's list, and
+                // the exact test runs over the list, when it is full and at the
+                // end. The lanes of a warp scan ranges of different lengths and
+                // pass different candidates; the exact test, the costly part,
+                // then runs with the lanes in step over lists of similar length.
+                std::uint32_t* lst = cell_lists + static_cast<std::size_t>(warp) * (kCellList * 32) + lane;
+                std::uint32_t nl = 0;
+                auto drain = [&]() {
+                    for (std::uint32_t k = 0; k < nl; ++k) {
+                        const std::uint32_t p = lst[k * 32];
+                        double xj[ND], D0j;
+                        load_pos_g<ND>(a.pos, p, xj, D0j, 1);
+                        cs.test(p, xj, D0j);
+                    }
+                    nl = 0;
+                };
+                auto push = [&](std::uint32_t p) {
+                    lst[nl * 32] = p;
+                    if (++nl == static_cast<std::uint32_t>(kCellList)) drain();
+                };
                 for (int r = 0; r < NROW; ++r) {
                     std::uint32_t a0, a1, b0, b1;
                     cell_row_ranges<NDC>(r, ci, nc, a.cell_start, a0, a1, b0, b1);
-                    double xj[ND], D0j;
-                    if (staged) {
+                    if (use_stage) {
                         // this lane's range lies inside the warp's window [u0, u1)
                         const float4* w = stage + s_win[warp][r][2];
                         const std::uint32_t u0 = s_win[warp][r][0];
@@ -1252,24 +1303,17 @@ __global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells
                             const float4 c = w[p - u0];
                             const float ex = c.x - me.x, ey = c.y - me.y, ez = NDC == 3 ? c.z - me.z : 0.0f;
                             const float d2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, ex * ex));
-                            const float rc = 0.5f * (cs.Dif + c.w * cs.kapf) + cs.tf;
-                            if (!(d2 < rc * rc * kPrefilter) || p == q) continue;
-                            load_pos_g<ND>(a.pos, p, xj, D0j, 1);
-                            cs.test(p, xj, D0j);
+                            const float rl = __fmaf_rn(c.w, pa, pb);
+                            if (d2 < rl * rl && p != q) push(p);
                         }
                     } else {
-                        for (std::uint32_t p = a0; p < a1; ++p) {
-                            if (p == q) continue;
-                            load_pos_g<ND>(a.pos, p, xj, D0j, 1);
-                            cs.test(p, xj, D0j);
-                        }
+                        for (std::uint32_t p = a0; p < a1; ++p)
+                            if (p != q) push(p);
                     }
-                    for (std::uint32_t p = b0; p < b1; ++p) {
-                        if (p == q) continue;
-                        load_pos_g<ND>(a.pos, p, xj, D0j, 1);
-                        cs.test(p, xj, D0j);
-                    }
+                    for (std::uint32_t p = b0; p < b1; ++p)
+                        if (p != q) push(p);
                 }
+                drain();
                 n = cs.n;
                 RCPG_UNROLL
                 for (int d = 0; d < ND; ++d) fi[d] = MX ? static_cast<double>(cs.fif[d]) : cs.fi[d];
@@ -1342,7 +1386,8 @@ __global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells
 // dynamic shared memory of k_build_search_cells<ND>
 template <int ND>
 constexpr std::size_t cells_smem_bytes() {
-    return static_cast<std::size_t>(kCellWarps) * CellStage<(ND <= 3 ? ND : 3)>::cap * sizeof(float4);
+    return static_cast<std::size_t>(kCellWarps) *
+           (CellStage<(ND <= 3 ? ND : 3)>::cap * sizeof(float4) + kCellList * 32 * sizeof(std::uint32_t));
 }
 
 // ===========================================================================
@@ -1591,12 +1636,67 @@ __global__ void __launch_bounds__(kCtlThreads) k_reduce_fast(DevArrays a) {
 // Graph-mode controller: reduce, finish step s (end_step), open step s+1
 // (begin_step) and publish the parameters of the kernels that follow. With
 // open_only it just opens the next step (the first step of a run).
+// Window statistics of the histories for begin_step(step), computed by the
+// whole block: sums in a fixed tree (graph mode; the host sums in order).
+__device__ void hist_stats_block(const Histories& h, std::uint64_t step, HistStats& out, double* red) {
+    // (lo, hi) inclusive index ranges of the four force means
+    const long long S = static_cast<long long>(step);
+    const long long lo[4] = {S - 450, S - 75, S - 200, S - 3000};
+    const long long hi[4] = {S - 250, S - 1, S - 1, S - 2500};
+    double sum[4] = {0.0, 0.0, 0.0, 0.0};
+    // a window whose start precedes step 1 wraps in the unsigned step
+    // arithmetic of hist_mean, which then sums nothing: the same here
+    RCPG_UNROLL
+    for (int w = 0; w < 4; ++w)
+        if (lo[w] >= 0)
+            for (long long k = lo[w] + threadIdx.x; k <= hi[w]; k += blockDim.x) sum[w] = xadd(sum[w], h.force[k]);
+    // phi range over [step - 250, step - 1)
+    double mn = HUGE_VAL, mx = -HUGE_VAL;
+    for (long long k = S - 250 + threadIdx.x; k < S - 1; k += blockDim.x)
+        if (k >= 0) {
+            mn = fmin(mn, h.phi[k]);
+            mx = fmax(mx, h.phi[k]);
+        }
+    RCPG_UNROLL
+    for (int o = 16; o > 0; o >>= 1) {
+        RCPG_UNROLL
+        for (int w = 0; w < 4; ++w) sum[w] = xadd(sum[w], __shfl_down_sync(0xffffffffu, sum[w], o));
+        mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) {
+        RCPG_UNROLL
+        for (int w = 0; w < 4; ++w) red[warp * 6 + w] = sum[w];
+        red[warp * 6 + 4] = mn;
+        red[warp * 6 + 5] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < nw; ++k) {
+            RCPG_UNROLL
+            for (int w = 0; w < 4; ++w) red[w] = xadd(red[w], red[k * 6 + w]);
+            red[4] = fmin(red[4], red[k * 6 + 4]);
+            red[5] = fmax(red[5], red[k * 6 + 5]);
+        }
+        // the divisors of hist_mean: end - start + 1 in unsigned step arithmetic
+        const std::uint64_t u = step;
+        out.f_450_250 = xdiv(red[0], static_cast<double>((u - 250) - (u - 450) + 1));
+        out.f_75_1 = xdiv(red[1], static_cast<double>((u - 1) - (u - 75) + 1));
+        out.f_200_1 = xdiv(red[2], static_cast<double>((u - 1) - (u - 200) + 1));
+        out.f_3000_2500 = xdiv(red[3], static_cast<double>((u - 2500) - (u - 3000) + 1));
+        out.phi_range_250 = xsub(red[5], red[4]);
+    }
+}
+
 __global__ void __launch_bounds__(kCtlThreads) k_controller(DevArrays a, int open_only) {
     __shared__ ForceSums red[kCtlThreads / 32];
+    __shared__ double s_hred[(kCtlThreads / 32) * 6];
     // the controller state is worked on in shared memory: one coalesced copy
     // in and out instead of a chain of dependent global loads in one thread
     __shared__ Controller cs;
-    __shared__ int s_publish;
+    __shared__ HistStats s_stats;
+    __shared__ int s_publish, s_go;
     DevCtl* ctl = a.ctl;
     if (ctl_idle(ctl)) {
         if (threadIdx.x == 0) ctl->adam_go = 0u;
@@ -1609,9 +1709,21 @@ __global__ void __launch_bounds__(kCtlThreads) k_controller(DevArrays a, int ope
         unsigned long long* dst = reinterpret_cast<unsigned long long*>(&cs);
         for (int w = threadIdx.x; w < kWords; w += blockDim.x) dst[w] = src[w];
     }
+    // the control words thread 0 needs, loaded before the reduction so that
+    // their latency overlaps it
+    std::uint32_t row_need = 0, cap_error = 0, pair_fp32 = 0;
+    double force_mu = 0.0, mixed_switch = 0.0;
+    if (threadIdx.x == 0) {
+        row_need = ctl->row_need;
+        cap_error = ctl->cap_error;
+        pair_fp32 = ctl->pair_fp32;
+        force_mu = ctl->force_mu;
+        mixed_switch = ctl->mixed_switch;
+    }
     __syncthreads();
     ForceSums s;
     if (!open_only) reduce_blocks(a, red, s);
+    // 1. end of the finished step (thread 0)
     if (threadIdx.x == 0) {
         Controller& c = cs;
         s_publish = 0;
@@ -1619,17 +1731,17 @@ __global__ void __launch_bounds__(kCtlThreads) k_controller(DevArrays a, int ope
         if (!open_only) {
             ctl->sums = s;
             // capacity problems of the last build stop the run before its results are used
-            if (ctl->row_need > a.S || ctl->cap_error) {
+            if (row_need > a.S || cap_error) {
                 ctl->halted = 1u;
                 ctl->adam_go = 0u;
                 go = false;
             } else {
-                const StepScalars sc = finalize_sums(s, ctl->force_mu, a.ndim);
+                const StepScalars sc = finalize_sums(s, force_mu, a.ndim);
                 ctl->scal = sc;
                 end_step(c, a.hist, sc);
                 // mixed precision: FP64 pair terms from the first step whose
                 // (nonzero) max overlap is below the switch, for the rest of the run
-                if (ctl->pair_fp32 && sc.max_overlap > 0.0 && sc.max_overlap < ctl->mixed_switch) {
+                if (pair_fp32 && sc.max_overlap > 0.0 && sc.max_overlap < mixed_switch) {
                     ctl->pair_fp32 = 0u;
                     ctl->fp64_switch_step = c.steps;
                 }
@@ -1647,14 +1759,26 @@ __global__ void __launch_bounds__(kCtlThreads) k_controller(DevArrays a, int ope
             ctl->fix_height_scale = 1.0;
             if (c.steps + 1 > c.step_cap) {
                 ctl->stopped = 1u;
-            } else {
-                begin_step(c, a.hist, c.steps + 1);
-                // the stretch of a reorder step waits until after the reorder (ENG:5661 < :5758)
-                ctl->fix_height_scale = c.reorder ? 1.0 : c.fix_height_scale;
-                if (c.done || c.reorder || c.lock_now) ctl->stopped = 1u;
-                else s_publish = 1;
+                go = false;
             }
         }
+        s_go = go ? 1 : 0;
+    }
+    __syncthreads();
+    // 2. the history windows the next step's schedule may read (the block)
+    const std::uint64_t next = cs.steps + 1;
+    const bool stats = s_go && next > 250 &&
+                       ((next >= cs.mu_decay_next_tick) || (next > 2500 && next - cs.last_alpha_update > 500));
+    if (stats) hist_stats_block(a.hist, next, s_stats, s_hred);
+    __syncthreads();
+    // 3. top of the next step (thread 0)
+    if (threadIdx.x == 0 && s_go) {
+        Controller& c = cs;
+        begin_step(c, a.hist, next, stats ? &s_stats : nullptr);
+        // the stretch of a reorder step waits until after the reorder (ENG:5661 < :5758)
+        ctl->fix_height_scale = c.reorder ? 1.0 : c.fix_height_scale;
+        if (c.done || c.reorder || c.lock_now) ctl->stopped = 1u;
+        else s_publish = 1;
     }
     __syncthreads();
     {

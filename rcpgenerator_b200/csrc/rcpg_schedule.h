@@ -142,10 +142,23 @@ RCPG_HD double shell_of(double Dmin, double Dmed, double Dmax) {
     return xmul(dmin2(dmax2(xmul(Dmed, 1.02), xmul(Dmin, 2.25)), Dmax), 0.5);
 }
 
+// Window statistics of the histories that begin_step(step) reads: the phi
+// range over [step - 250, step - 1) and the force means of the learning-rate
+// rule. The graph-mode controller computes them with its whole block before
+// the serial schedule; the host computes them in the reference's order.
+struct HistStats {
+    double phi_range_250;  // phi_range(h.phi, step - 250, step - 1)
+    double f_450_250;      // hist_mean(h.force, step - 450, step - 250)
+    double f_75_1;         // hist_mean(h.force, step - 75, step - 1)
+    double f_200_1;        // hist_mean(h.force, step - 200, step - 1)
+    double f_3000_2500;    // hist_mean(h.force, step - 3000, step - 2500)
+};
+
 // ---- top of step (ENG:5520-6042) ------------------------------------------
 // Everything the reference does before its pair refresh, except the two
 // particle-wide actions it requests through flags: reorder and lock_now.
-RCPG_HD void begin_step(Controller& c, const Histories& h, std::uint64_t step) {
+// `pre` (optional) holds the history window statistics of this step.
+RCPG_HD void begin_step(Controller& c, const Histories& h, std::uint64_t step, const HistStats* pre = nullptr) {
     const std::uint64_t cooldown = 250;
     const double flat = 5e-3, decay = 0.85;
     c.steps = step;
@@ -157,7 +170,7 @@ RCPG_HD void begin_step(Controller& c, const Histories& h, std::uint64_t step) {
 
     // feedback mu decay (ENG:5528-5544)
     if (c.mu_decay_active && step >= c.mu_decay_next_tick && step > 250) {
-        const double rng = phi_range(h.phi, step - 250, step - 1);
+        const double rng = pre ? pre->phi_range_250 : phi_range(h.phi, step - 250, step - 1);
         if (rng < flat) {
             c.mu = xmul(c.mu, decay);
             if (c.mu <= c.mu_decay_target) {
@@ -213,7 +226,7 @@ RCPG_HD void begin_step(Controller& c, const Histories& h, std::uint64_t step) {
             }
         }
     } else if (c.osc_phase == OSC_FINAL && step >= c.mu_decay_next_tick && step > 250) {
-        const double rng = phi_range(h.phi, step - 250, step - 1);
+        const double rng = pre ? pre->phi_range_250 : phi_range(h.phi, step - 250, step - 1);
         if (rng < flat) {
             const double F_now = (step >= 1) ? h.force[step - 1] : 0.0;
             const bool met = (F_now < 5e-3) && (c.max_min_dist < 5e-4);
@@ -240,15 +253,15 @@ RCPG_HD void begin_step(Controller& c, const Histories& h, std::uint64_t step) {
         const std::uint64_t s250 = (step > 251) ? step - 250 : 1;  // max(step-250, 1)
         if ((step - c.last_alpha_update > 500) && (xsub(c.phi, h.phi[s250]) < 5e-4) &&
             (step > 2500) && static_cast<double>(step) > xadd(c.mu_change, 500.0)) {
-            double trend1 = xdiv(hist_mean(h.force, step - 450, step - 250),
-                                 hist_mean(h.force, step - 75, step - 1));
+            double trend1 = pre ? xdiv(pre->f_450_250, pre->f_75_1)
+                                : xdiv(hist_mean(h.force, step - 450, step - 250), hist_mean(h.force, step - 75, step - 1));
             const double trend2 = xsub(c.phi, h.phi[s250]);
             if ((c.mu_flag < 1 && trend1 < 0.85) || trend2 < -5E-4) {
                 c.last_alpha_update = step;
                 c.alpha = xdiv(c.alpha, 1.5);
             } else if (c.mu_flag < 1 && step - c.last_alpha_update > 1500) {
-                trend1 = xdiv(hist_mean(h.force, step - 200, step - 1),
-                              hist_mean(h.force, step - 3000, step - 2500));
+                trend1 = pre ? xdiv(pre->f_200_1, pre->f_3000_2500)
+                             : xdiv(hist_mean(h.force, step - 200, step - 1), hist_mean(h.force, step - 3000, step - 2500));
                 if (trend1 > 0.5) {
                     c.last_alpha_update = step;
                     c.alpha = xmul(c.alpha, 1.15);
