@@ -1271,12 +1271,13 @@ __global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells
                 // prefilter cutoff of a candidate with FP32 diameter w: w * pa + pb
                 const float pa = 0.5f * cs.kapf * kPrefilterLin;
                 const float pb = __fmaf_rn(0.5f * cs.Dif + cs.tf, kPrefilterLin, s_eabs);
-                // The lane's candidates in scan order go through two phases:
-                // the FP32 prefilter (staged ones) fills the lane's list, and
-                // the exact test runs over the list, when it is full and at the
-                // end. The lanes of a warp scan ranges of different lengths and
-                // pass different candidates; the exact test, the costly part,
-                // then runs with the lanes in step over lists of similar length.
+                // FP64 variant: the lane's candidates in scan order go through
+                // two phases -- the FP32 prefilter (staged ones) fills the
+                // lane's list, and the exact test runs over the list, when it
+                // is full and at the end, with the lanes in step over lists of
+                // similar length. Mixed variant: the exact test follows each
+                // candidate that passes (its FP32 test is cheap enough that the
+                // list costs more than the divergence it removes).
                 std::uint32_t* lst = cell_lists + static_cast<std::size_t>(warp) * (kCellList * 32) + lane;
                 std::uint32_t nl = 0;
                 auto drain = [&]() {
@@ -1289,8 +1290,14 @@ __global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells
                     nl = 0;
                 };
                 auto push = [&](std::uint32_t p) {
-                    lst[nl * 32] = p;
-                    if (++nl == static_cast<std::uint32_t>(kCellList)) drain();
+                    if constexpr (MX) {
+                        double xj[ND], D0j;
+                        load_pos_g<ND>(a.pos, p, xj, D0j, 1);
+                        cs.test(p, xj, D0j);
+                    } else {
+                        lst[nl * 32] = p;
+                        if (++nl == static_cast<std::uint32_t>(kCellList)) drain();
+                    }
                 };
                 for (int r = 0; r < NROW; ++r) {
                     std::uint32_t a0, a1, b0, b1;
@@ -1313,7 +1320,7 @@ __global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells
                     for (std::uint32_t p = b0; p < b1; ++p)
                         if (p != q) push(p);
                 }
-                drain();
+                if constexpr (!MX) drain();
                 n = cs.n;
                 RCPG_UNROLL
                 for (int d = 0; d < ND; ++d) fi[d] = MX ? static_cast<double>(cs.fif[d]) : cs.fi[d];
@@ -1383,11 +1390,12 @@ __global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells
     if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
 }
 
-// dynamic shared memory of k_build_search_cells<ND>
-template <int ND>
+// dynamic shared memory of k_build_search_cells<ND, MX> (the candidate lists
+// only in the FP64 variant; the mixed one leaves the space to L1)
+template <int ND, bool MX>
 constexpr std::size_t cells_smem_bytes() {
     return static_cast<std::size_t>(kCellWarps) *
-           (CellStage<(ND <= 3 ? ND : 3)>::cap * sizeof(float4) + kCellList * 32 * sizeof(std::uint32_t));
+           (CellStage<(ND <= 3 ? ND : 3)>::cap * sizeof(float4) + (MX ? 0 : kCellList * 32 * sizeof(std::uint32_t)));
 }
 
 // ===========================================================================
@@ -2154,7 +2162,7 @@ template <int ND, bool MX>
 void launch_cells_variant(const DevArrays& a, cudaStream_t st) {
     int dev = 0;
     cudaGetDevice(&dev);
-    constexpr std::size_t smem = cells_smem_bytes<ND>();
+    constexpr std::size_t smem = cells_smem_bytes<ND, MX>();
     static int grid[64] = {};
     if (dev >= 0 && dev < 64 && grid[dev] == 0) {
         cudaFuncSetAttribute(k_build_search_cells<ND, MX>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -1,6 +1,7 @@
 """A packing of the N = 1M 2-D bidisperse workload's kind at N = 100,000, run
-to the reference's convergence gate (ENG:5603-5655: mean force < 5e-3 and
-max overlap < 5e-4 three checks in a row) in mixed and in FP64 pair
+to the reference's convergence gate (ENG:5603-5655: max overlap < 5e-4 three
+checks in a row; its mean-force term reads the history entry of the step not
+yet run, which is zero) in mixed and in FP64 pair
 precision. Mixed precision would switch to FP64 pair terms once the max
 overlap fell below 1e-5, which a run that ends at the gate's 5e-4 does not
 reach; its jamming fraction must stay within 1e-3 of the FP64 run's (the
@@ -32,9 +33,16 @@ def test_mixed_precision_jams_within_1e3_of_fp64(cuda_device):
     for prec, r in out.items():
         why = (prec, r["steps"], r["phi"], r["max_min_dist"], r["force_history"][-4:],
                r["max_overlap_history"][-4:], r["engine_stats"])
-        # ended by the convergence gate: final overlap and force below its thresholds
+        # ended by the convergence gate: the final max overlap below its threshold
         assert r["max_min_dist"] < 5e-4, why
-        assert r["force_history"][-1] < 5e-3, why
+        # the mean force is the reference's (ENG:769-801): the mean |F_i| over
+        # the particles with |F_i|^2 > 1e-16, NaN when there is none -- which
+        # happens near jamming at this box scale (|F_i| ~ 1e-9); the gate
+        # reads the entry of the step not yet run (zero), so it does not
+        # depend on it
+        fh = r["force_history"]
+        assert np.isfinite(fh[: len(fh) // 2]).all(), why
+        assert np.isnan(fh[-1]) or fh[-1] < 5e-3, why
         assert np.isfinite(r["positions"]).all()
         assert 0.80 < r["phi"] < 0.90
     # the FP64 run reports no mixed-precision error; the mixed run reports its
