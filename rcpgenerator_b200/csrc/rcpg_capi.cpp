@@ -584,8 +584,11 @@ int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, co
                                double* scalars, int32_t* fused_out, void* stream, char* err,
                                size_t errlen) {
     if (N == 0 || N > 0xFFFFFFFFull || ndim < 2 || ndim > rcpg::kMaxDim || !x_dev || !D_dev || !nbr_dev ||
-        !cnt_dev || !F_dev || row_capacity == 0 || pair_precision < 0 || pair_precision > 1)
+        !cnt_dev || !F_dev || row_capacity == 0 || pair_precision < 0 || pair_precision > 3)
         return fail(err, errlen, RCPG_EINVAL, "rcpgenerator_b200: bad arguments to rcpg_pairs_forces_scan");
+    // bit 1: the forces of the step's pair kernel on the new rows, also after a build that fused them
+    const bool pair_kernel = (pair_precision & 2) != 0;
+    pair_precision &= 1;
     if (!have_device(err, errlen)) return RCPG_ECUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     try {
@@ -678,6 +681,8 @@ int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, co
         DevCtl after;
         cuda_ok(cudaMemcpyAsync(&after, a.ctl, sizeof(after), cudaMemcpyDeviceToHost, st), "D2H ctl");
         cuda_ok(cudaStreamSynchronize(st), "sync");
+        if (pair_kernel && after.forces_done)
+            cuda_ok(cudaMemsetAsync(&a.ctl->forces_done, 0, sizeof(std::uint32_t), st), "memset forces_done");
         rcpg::launch_forces(a, 0, st);
         rcpg::launch_reduce_fast(a, st);
         // rows, counts and forces back in the caller's particle order

@@ -76,6 +76,14 @@ struct DevCtl {
     std::uint32_t buf;
     std::uint32_t permute_done;
     std::uint64_t pair_kernel_runs;  // launches of the pair kernel that computed forces
+    // Cell units of the cell-order kernels (graph mode, one size class, set by
+    // each build): a unit is unit_w consecutive cells of one grid row (the last
+    // unit of a row may be shorter); unit_chunks units per grid row, unit_count
+    // units in all.
+    std::uint32_t unit_w;
+    std::uint32_t unit_chunks;
+    std::uint32_t unit_count;
+    std::uint32_t pad1;
 };
 
 // In graph mode every pair-list build stores the particles in cell order

@@ -125,6 +125,37 @@ __global__ void __launch_bounds__(256) k_adam_refresh(DevArrays a, int do_adam, 
 constexpr int kTileRowsMin = 4, kTileRowsMax = 12, kTileRowsPref = 8;
 constexpr int kTileStage2 = 1024;  // staged particles per 2-D tile (TileShape<2>::stage)
 
+// Shape of the cell units of the cell-order kernels (k_cells, below).
+template <int ND>
+struct UnitShape {
+    static constexpr int ndc = ND <= 3 ? ND : 3;
+    static constexpr int rows = ndc == 2 ? 3 : 9;        // neighbour rows of a unit
+    static constexpr int threads = ndc == 2 ? 128 : 64;  // block size
+    static constexpr int target = ndc == 2 ? 112 : 56;   // particles per unit
+    static constexpr int stage = ndc == 2 ? 640 : 768;   // staged records (32 bytes each)
+    static constexpr int maxw = ndc == 2 ? 256 : 128;    // cells per unit at most
+    static constexpr int slice = maxw + 3;               // cell_start entries per row (build)
+    static constexpr int windows = 3 * rows;             // main, wrapped x-1, wrapped x+1 per row
+    static constexpr int min_blocks = 6;                 // resident blocks per SM (register budget)
+};
+
+// Cells per unit for a build with `cells` cells in a grid of nc0 cells per row:
+// about `target` particles at the mean occupancy, windows that fit the stage
+// with 30 % headroom, at most maxw cells.
+template <int ND>
+__device__ __forceinline__ std::uint32_t unit_width(std::uint64_t N, double cells, int nc0) {
+    using US = UnitShape<ND>;
+    const double ppc = static_cast<double>(N) / (cells > 1.0 ? cells : 1.0);
+    const double occ = ppc > 1e-3 ? ppc : 1e-3;
+    double w = floor(static_cast<double>(US::target) / occ);
+    const double ws = floor(static_cast<double>(US::stage) / (1.3 * US::rows * occ)) - 2.0;
+    if (ws < w) w = ws;
+    if (w > static_cast<double>(US::maxw)) w = US::maxw;
+    if (w > static_cast<double>(nc0)) w = nc0;
+    if (!(w >= 1.0)) w = 1.0;
+    return static_cast<std::uint32_t>(w);
+}
+
 __global__ void k_build_prepare(DevArrays a) {
     DevCtl* ctl = a.ctl;
     if (build_off(ctl)) return;
@@ -183,6 +214,20 @@ __global__ void k_build_prepare(DevArrays a) {
             ctl->cell_scale[d] = ctl->cls_scale[0][d];
         }
         ctl->ncells = cells;
+        // cell units of the cell-order kernels (one grid: class 0's)
+        if (nd == 2 || nd == 3) {
+            const double c0 = cells_k[0];
+            const int nc0 = static_cast<int>(nc[0][0]);
+            const std::uint32_t w = nd == 2 ? unit_width<2>(a.N, c0, nc0) : unit_width<3>(a.N, c0, nc0);
+            const std::uint32_t chunks = (static_cast<std::uint32_t>(nc0) + w - 1) / w;
+            std::uint32_t rows = static_cast<std::uint32_t>(nc[0][1]);
+            if (nd == 3) rows *= static_cast<std::uint32_t>(nc[0][2]);
+            ctl->unit_w = w;
+            ctl->unit_chunks = chunks;
+            ctl->unit_count = chunks * rows;
+        } else {
+            ctl->unit_w = ctl->unit_chunks = ctl->unit_count = 0u;
+        }
         // 2-D tiles: kTileRowsPref cells high, lower where the halo's
         // particles at the mean cell occupancy (with 30 % headroom) would not
         // fit the staging area
@@ -990,412 +1035,471 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
 }
 
-// ---- cell-order search (graph mode, ndim 2 and 3, one size class) ---------
-// With cell-order storage the members of the cells x-1, x, x+1 of one grid
-// row are one contiguous range of particles (two where the row wraps), so a
-// particle's candidates are 3^(ndim-1) contiguous ranges of pos. A warp takes
-// 32 consecutive particles; their ranges of one row offset overlap, and their
-// union is one contiguous window, which the warp copies into shared memory
-// with coalesced loads before any lane scans it, as FP32 positions relative to
-// the warp's first particle (minimum image taken in FP64 before rounding) and
-// FP32 diameters (the cells at the wrap of a row, and windows that do not fit,
-// are read from global memory). One thread per particle then tests its
-// candidates in scan order -- rows of the grid in order, x ascending within a
-// row -- so rows hold partner indices in that order: an FP32 test on the
-// relative positions, with the shell widened beyond their rounding, passes a
-// candidate to the exact test on its FP64 record. The relative positions of
-// a lane and of its candidates differ by the minimum image only while the
-// lane lies more than a neighbourhood away from the wrap of the warp's frame
-// (half a box from the first particle); a warp spread over more than half
-// the box (dilute packings, containers with empty rows) has lanes that do
-// not, and those test every candidate exactly from global memory. The step's forces are computed in the same pass (graph mode): FP64
-// pair terms on the reference's predicate, or (mixed precision) the shell
-// test and the pair terms in FP32 on FP64 differences, the shell widened by
-// kShellMarginF so that the rows hold every pair of the FP64 shell.
-constexpr int kCellWarps = 4;  // warps per block
-constexpr int kCellThreads = 32 * kCellWarps;
-// staged particles per warp (2-D: the 3 windows of ~40 particles at the
-// bench's occupancy; 3-D: the 9 windows of ~45)
-template <int ND> struct CellStage { static constexpr int cap = 192; };
-template <> struct CellStage<3> { static constexpr int cap = 416; };
-// entries of a lane's list of candidates for the exact test
-constexpr int kCellList = 32;
-// Widening of the cutoff r_c in the FP32 prefilter of the staged candidates:
-// relative (kPrefilterLin, for the rounding of diameters and of the cutoff
-// arithmetic) plus an absolute term for the rounding of relative positions of
-// magnitude up to half the box h (each coordinate within 2^-24 h, so a
-// distance within sqrt(3) 2^-23 h < 2^-21 h). A candidate rejected here fails
-// the exact test.
-constexpr float kPrefilterLin = 1.0005f;
-constexpr float kPrefilterAbs = 4.76837158203125e-07f;  // 2^-21
-// A lane's relative position must lie this many cells inside the wrap of the
-// warp's frame for its staged candidates to be tested there (a pair is
-// nearer than one cell per axis).
-constexpr float kFrameGuardCells = 1.5f;
+// ---- cell units: the cell-order search and pair kernel (graph mode) -------
+// With cell-order storage the members of consecutive cells of one grid row
+// are one contiguous range of particles. A unit is a chunk of unit_w
+// consecutive cells of one grid row (2-D: row y; 3-D: row (y, z)), sized by
+// each build so that it holds about UnitShape::target particles and its
+// windows fit the stage. A block takes one unit at a time:
+//   1. the cell_start entries of the unit's 3^(ndim-1) neighbour rows: cells
+//      cx0-1 .. cx1 of each (the main window), plus, where the unit touches
+//      the end of the grid row, the cell at the row's other end (the wrapped
+//      x-1 / x+1 cell);
+//   2. the FP64 records of those windows -- contiguous ranges of pos -- into
+//      shared memory, with coalesced 256-bit loads by the whole block;
+//   3. one thread per particle of the unit, every partner read from shared
+//      memory (windows that do not fit the stage are read from pos instead:
+//      same code, other pointer).
+// k_cells<ND, MX, BUILD>:
+//   BUILD  the neighbour search of a build. A particle's candidates in scan
+//          order -- rows of the grid in order (row offset r = (dy+1) +
+//          3 (dz+1)), cells x-1, x, x+1 within a row (a wrapped cell in its
+//          place) -- go through the reference's predicate in FP64, or (MX) the
+//          mixed-precision shell test (FP32 on FP64 differences, widened by
+//          kShellMarginF so that the rows hold every pair of the FP64 shell);
+//          rows hold the partners in that order, and the step's forces are
+//          computed in the same pass.
+//   !BUILD the pair kernel of a step without a build: each particle's row
+//          entries (coalesced reads of nbr) are found in the staged windows by
+//          a binary search over the windows' first particles (every partner
+//          lies in one: the build took the rows from the same windows) and
+//          summed in row order with the arithmetic of k_forces, so the build
+//          and the pair kernel give the same forces bit for bit.
+// MX: FP32 pair terms; each variant returns at once when the step's pair
+// precision is the other one.
 
-// One particle's candidate tests (FP64 or mixed) and its row and force sums.
+// 32-byte particle record (ndim <= 3) from global memory, one 256-bit load
+__device__ __forceinline__ void ld_record(const double* p, double2& lo, double2& hi) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(lo.x), "=d"(lo.y), "=d"(hi.x), "=d"(hi.y)
+        : "l"(p));
+}
+
+template <int ND>
+__device__ __forceinline__ void unpack_record(const double2& lo, const double2& hi, double* x, double& D0) {
+    x[0] = lo.x;
+    x[1] = lo.y;
+    if constexpr (ND == 3) {
+        x[2] = hi.x;
+        D0 = hi.y;
+    } else {
+        D0 = hi.x;
+    }
+}
+
+// Per-particle pair sums in the arithmetic of k_forces: FP32 (MX) or FP64
+// accumulators for the pair scalars, the force in FP32 (MX) or FP64.
 template <int ND, bool MX>
-struct CellScan {
-    std::uint32_t* __restrict__ nbr;
-    std::uint64_t N, q;
-    std::uint32_t S;
-    double xi[ND], Di, kap, t_shell;
-    const double* bx;   // box (shared memory)
-    const double* ibx;  // 1 / box (shared memory)
-    const float* hbf;   // half box, FP32 (shared memory)
-    float Dif, kapf, tf;
-    bool fuse;
-    std::uint32_t n;
+struct UnitPair {
+    using Acc = std::conditional_t<MX, float, double>;
+    double xi[ND], Di, kap;
+    float Dif, kapf;
     double fi[ND];
     float fif[ND];
-    double U, Lc, dk, Fm, maxov;
-    std::uint32_t count;
+    Acc sU, sLc, sdk, sFm, smax;
+    std::uint32_t scount;
 
-    // candidate p with record (xj, D0j): shell test, row entry, pair terms
-    __device__ __forceinline__ void test(std::uint64_t p, const double* xj, double D0j) {
+    __device__ __forceinline__ void begin(const double* x, double D0, double k) {
+        kap = k;
+        kapf = static_cast<float>(k);
+        Di = xmul(D0, k);
+        Dif = static_cast<float>(D0) * kapf;
+        RCPG_UNROLL
+        for (int d = 0; d < ND; ++d) {
+            xi[d] = x[d];
+            fi[d] = 0.0;
+            fif[d] = 0.0f;
+        }
+        sU = sLc = sdk = sFm = smax = Acc(0);
+        scount = 0;
+    }
+
+    __device__ __forceinline__ void add_scalars(const PairTerms& pt) {
+        if constexpr (MX) {
+            sU += static_cast<float>(pt.U);
+            sLc += static_cast<float>(pt.Lc);
+            sdk += static_cast<float>(pt.dk);
+            sFm += static_cast<float>(pt.Fm);
+            smax = fmaxf(smax, static_cast<float>(pt.U));
+        } else {
+            sU = xadd(sU, pt.U);
+            sLc = xadd(sLc, pt.Lc);
+            sdk = xadd(sdk, pt.dk);
+            sFm = xadd(sFm, pt.Fm);
+            smax = fmax(smax, pt.U);
+        }
+        ++scount;
+    }
+
+    // Partner with record (xj, D0j) of a row (as k_forces): pair terms of an
+    // overlapping pair; scalars once per pair, from the lower index.
+    __device__ __forceinline__ void row_partner(bool upper, const double* xj, double D0j, const double* bx,
+                                                const double* ibx, const float* hbf) {
         PairTerms pt;
-        bool overlap;
+        if constexpr (MX) {
+            float dxf[ND];
+            const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
+            const float rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
+            if (!(d2f < rsum * rsum)) return;
+            pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
+        } else {
+            const double r_ij = xmul(0.5, xadd(Di, xmul(D0j, kap)));
+            double dx[ND];
+            const double d2 = pair_disp<ND>(xi, xj, bx, ibx, dx);
+            if (!(d2 < xmul(r_ij, r_ij))) return;
+            pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
+        }
+        if (upper) add_scalars(pt);
+    }
+
+    // Candidate of a build: the shell test; on a pass the pair terms when
+    // `fuse` and the pair overlaps. Returns whether the candidate is a partner.
+    __device__ __forceinline__ bool candidate(bool upper, const double* xj, double D0j, const double* bx,
+                                              const double* ibx, const float* hbf, double t_shell, float tf,
+                                              bool fuse) {
+        PairTerms pt;
         if constexpr (MX) {
             float dxf[ND];
             const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
             const float rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
             const float rc = rsum + tf;
-            if (!(d2f < rc * rc * kShellMarginF)) return;
-            overlap = fuse && d2f < rsum * rsum;
-            if (overlap) pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
+            if (!(d2f < rc * rc * kShellMarginF)) return false;
+            if (!(fuse && d2f < rsum * rsum)) return true;
+            pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
         } else {
             const double Dj = xmul(D0j, kap);
             double dx[ND];
             const double d2 = pair_disp<ND>(xi, xj, bx, ibx, dx);
             const double r_c = shell_cut<ND>(Di, Dj, t_shell);  // ndim <= 3: symmetric
-            if (!(d2 < xmul(r_c, r_c))) return;
+            if (!(d2 < xmul(r_c, r_c))) return false;
             const double r_ij = xmul(0.5, xadd(Di, Dj));
-            overlap = fuse && d2 < xmul(r_ij, r_ij);
-            if (overlap) pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
+            if (!(fuse && d2 < xmul(r_ij, r_ij))) return true;
+            pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
         }
-        if (n < S) nbr[static_cast<std::uint64_t>(n) * N + q] = static_cast<std::uint32_t>(p);
-        ++n;
-        if (overlap && p > q) {  // pair scalars once per pair, from the lower index
-            U = xadd(U, pt.U);
-            Lc = xadd(Lc, pt.Lc);
-            dk = xadd(dk, pt.dk);
-            Fm = xadd(Fm, pt.Fm);
-            maxov = fmax(maxov, pt.U);
-            ++count;
-        }
+        if (upper) add_scalars(pt);
+        return true;
+    }
+
+    __device__ __forceinline__ void force(double* f) const {
+        RCPG_UNROLL
+        for (int d = 0; d < ND; ++d) f[d] = MX ? static_cast<double>(fif[d]) : fi[d];
     }
 };
 
-// Candidate ranges of row offset r (0 .. 3^(ndim-1) - 1) of the particle in
-// cell ci: [a0, a1) and, where the row wraps in x, [b0, b1) (the wrapped cell
-// is visited in its place: x - 1 first, x + 1 last).
-template <int NDC>
-__device__ __forceinline__ void cell_row_ranges(int r, const int* ci, const int* nc,
-                                                const std::uint32_t* __restrict__ cell_start, std::uint32_t& a0,
-                                                std::uint32_t& a1, std::uint32_t& b0, std::uint32_t& b1) {
-    int c1 = ci[1] + (r % 3) - 1;
-    c1 = c1 < 0 ? c1 + nc[1] : (c1 >= nc[1] ? c1 - nc[1] : c1);
-    std::uint32_t row = static_cast<std::uint32_t>(c1) * static_cast<std::uint32_t>(nc[0]);
-    if constexpr (NDC == 3) {
-        int c2 = ci[2] + (r / 3) - 1;
-        c2 = c2 < 0 ? c2 + nc[2] : (c2 >= nc[2] ? c2 - nc[2] : c2);
-        row += static_cast<std::uint32_t>(c2) * static_cast<std::uint32_t>(nc[0]) * static_cast<std::uint32_t>(nc[1]);
-    }
-    const int xl = ci[0] - 1, xh = ci[0] + 1;
-    b0 = b1 = 0;
-    if (xl >= 0 && xh < nc[0]) {
-        a0 = cell_start[row + xl];
-        a1 = cell_start[row + xh + 1];
-    } else if (xl < 0) {
-        a0 = cell_start[row + nc[0] - 1];
-        a1 = cell_start[row + nc[0]];
-        b0 = cell_start[row];
-        b1 = cell_start[row + 2];
-    } else {
-        a0 = cell_start[row + xl];
-        a1 = cell_start[row + nc[0]];
-        b0 = cell_start[row];
-        b1 = cell_start[row + 1];
-    }
-}
-
-// Position relative to xref (minimum image per axis in FP64, then rounded to
-// FP32) and the FP32 diameter of a staged candidate.
-template <int ND>
-__device__ __forceinline__ float4 rel_record(const double* x, double D0, const double* xref, const double* box) {
-    float r[3] = {0.0f, 0.0f, 0.0f};
-    RCPG_UNROLL
-    for (int d = 0; d < (ND < 3 ? ND : 3); ++d) {
-        double dd = x[d] - xref[d];
-        const double h = 0.5 * box[d];
-        if (dd > h) dd -= box[d];
-        else if (dd < -h) dd += box[d];
-        r[d] = static_cast<float>(dd);
-    }
-    return make_float4(r[0], r[1], r[2], static_cast<float>(D0));
-}
-
-// MX: the mixed-precision variant (FP32 pair terms); each variant returns at
-// once when the step's pair precision is the other one.
-template <int ND, bool MX>
-__global__ void __launch_bounds__(kCellThreads, MX ? 4 : 3) k_build_search_cells(DevArrays a) {
-    constexpr int NDC = ND <= 3 ? ND : 3;
-    constexpr int NROW = (NDC == 2) ? 3 : 9;
-    constexpr int CAP = CellStage<NDC>::cap;
-    constexpr int P = pos_stride(ND);
+template <int ND, bool MX, bool BUILD>
+__global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blocks) k_cells(DevArrays a) {
+    using US = UnitShape<ND>;
+    constexpr int NDC = US::ndc, R = US::rows, T = US::threads, NW = US::windows;
+    constexpr int CR = NDC == 2 ? 1 : 4;  // row offset of the unit's own row
     DevCtl* ctl = a.ctl;
-    if (build_off(ctl) || !use_cells<ND>(a) || MX != (ctl->pair_fp32 != 0u)) return;
+    if constexpr (BUILD) {
+        if (build_off(ctl) || !use_cells<ND>(a) || MX != (ctl->pair_fp32 != 0u)) return;
+    } else {
+        const std::uint32_t st = ctl->stopped, ha = ctl->halted, fd = ctl->forces_done, p32 = ctl->pair_fp32;
+        if ((st | ha | fd) != 0u || MX != (p32 != 0u) || !use_cells<ND>(a)) return;
+    }
     bind_buffers(a);
-    extern __shared__ __align__(16) float4 cell_stage[];  // [kCellWarps][CAP]: x, y, z relative, D0
-    // [kCellWarps][kCellList][32]: each lane's candidates for the exact test
-    std::uint32_t* cell_lists = reinterpret_cast<std::uint32_t*>(cell_stage + kCellWarps * CAP);
-    __shared__ ForceSums s_red[kCellWarps];
-    __shared__ std::uint32_t s_need;
-    __shared__ std::uint32_t s_win[kCellWarps][NROW][3];  // window base, end, stage offset
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float4* stage = cell_stage + static_cast<std::size_t>(warp) * CAP;
-    if (threadIdx.x == 0) s_need = 0u;
+    extern __shared__ __align__(16) double u_stage[];  // [US::stage][4]: the staged records
+    std::uint32_t* s_cs = reinterpret_cast<std::uint32_t*>(u_stage + 4 * US::stage);  // [R][US::slice] (build)
+    // windows, flat index w = 3 r + kind (0 main, 1 wrapped x-1, 2 wrapped x+1):
+    // first particle, length, index of the first record in `recs`
+    __shared__ std::uint32_t s_wb[NW], s_wl[NW], s_ws[NW];
+    // the pair kernel's lookup: the non-empty windows sorted by first particle
+    __shared__ std::uint32_t s_lb[NW], s_ll[NW], s_ls[NW];
+    __shared__ std::uint32_t s_qa, s_qb, s_total, s_nl, s_need;
+    __shared__ ForceSums s_red[T / 32];
+    // the thread's column of the block sums (its particles in order), in
+    // shared memory: they change once per particle
+    __shared__ double s_acc[7][T];
+    __shared__ std::uint32_t s_accn[2][T];
     const std::uint64_t N = a.N;
     const std::uint32_t S = a.S;
-    // block-wide constants in shared memory (fewer registers per thread)
-    __shared__ Geometry s_g;
-    __shared__ double s_scale[NDC];
-    __shared__ float s_hbf[ND];
-    __shared__ float s_guard[NDC];  // |relative position| below which a lane uses the stage
-    __shared__ float s_eabs;        // absolute widening of the prefilter cutoff
-    __shared__ int s_nc[NDC];
-    if (threadIdx.x == 0) {
-        s_g = ctl->g;
-        double hmax = 0.0;
-        for (int d = 0; d < NDC; ++d) {
-            s_nc[d] = ctl->ncell[d];
-            s_scale[d] = ctl->cell_scale[d];
-            const double h = 0.5 * ctl->g.box[d];
-            hmax = fmax(hmax, h);
-            s_guard[d] = static_cast<float>(h - kFrameGuardCells / ctl->cell_scale[d]);
-        }
-        s_eabs = static_cast<float>(hmax) * kPrefilterAbs;
-        for (int d = 0; d < ND; ++d) s_hbf[d] = static_cast<float>(0.5 * ctl->g.box[d]);
-    }
-    const bool fuse = ctl->forces_done != 0u;
-    __syncthreads();
-    const Geometry& g = s_g;
-    const int* nc = s_nc;
-    const double* scale = s_scale;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) ctl->nsum_blocks = gridDim.x;
-    double sU = 0.0, sLc = 0.0, sdk = 0.0, sFm = 0.0, smax = 0.0, smag = 0.0, sD = 0.0;
-    std::uint32_t scount = 0, smagc = 0, need = 0;
-    bool overflow = false;
-    const std::uint64_t wstride = static_cast<std::uint64_t>(gridDim.x) * kCellWarps * 32;
-    for (std::uint64_t q0 = (static_cast<std::uint64_t>(blockIdx.x) * kCellWarps + warp) * 32; q0 < N;
-         q0 += wstride) {
-        const std::uint64_t q = q0 + lane;
-        const bool valid = q < N;
-        double xi[ND], D0i = 0.0;
-        int ci[NDC];
-        RCPG_UNROLL
-        for (int d = 0; d < ND; ++d) xi[d] = 0.0;
-        if (valid) load_pos_g<ND>(a.pos, q, xi, D0i, 1);
-        RCPG_UNROLL
-        for (int d = 0; d < NDC; ++d) ci[d] = cell_coord(xi[d], scale[d], nc[d]);
-        // origin of the warp's relative positions: its first particle
-        double xref[ND];
-        RCPG_UNROLL
-        for (int d = 0; d < ND; ++d) xref[d] = __shfl_sync(0xffffffffu, xi[d], 0);
-        // 1. the warp's window of every row offset: the union of its lanes'
-        // main ranges (consecutive particles: overlapping, contiguous ranges)
-        std::uint32_t total = 0;
-        for (int r = 0; r < NROW; ++r) {
-            std::uint32_t a0 = 0, a1 = 0, b0, b1;
-            if (valid) cell_row_ranges<NDC>(r, ci, nc, a.cell_start, a0, a1, b0, b1);
-            const std::uint32_t u0 = __reduce_min_sync(0xffffffffu, valid ? a0 : 0xffffffffu);
-            const std::uint32_t u1 = __reduce_max_sync(0xffffffffu, valid ? a1 : 0u);
-            const std::uint32_t len = u1 > u0 ? u1 - u0 : 0u;
-            if (lane == 0) {
-                s_win[warp][r][0] = u0;
-                s_win[warp][r][1] = u0 + len;
-                s_win[warp][r][2] = total;
-            }
-            total += len;
-        }
-        __syncwarp();
-        const bool staged = total <= static_cast<std::uint32_t>(CAP);
-        // 2. stage the windows: one particle per lane and round (its 32-byte
-        // record), as relative FP32 position and FP32 diameter
-        if (staged) {
-            for (int r = 0; r < NROW; ++r) {
-                const std::uint32_t u0 = s_win[warp][r][0], u1 = s_win[warp][r][1], off = s_win[warp][r][2];
-                for (std::uint32_t k = lane; k < u1 - u0; k += 32) {
-                    double xs[ND], D0s;
-                    load_pos_g<ND>(a.pos, u0 + k, xs, D0s, 1);
-                    stage[off + k] = rel_record<ND>(xs, D0s, xref, g.box);
-                }
-            }
-        }
-        __syncwarp();
-        if (valid) {
-            const double Di = xmul(D0i, ctl->build_kappa);
-            double fi[ND];
-            std::uint32_t n = 0;
-            const float4 me = rel_record<ND>(xi, D0i, xref, g.box);
-            {
-                CellScan<ND, MX> cs;
-                cs.nbr = a.nbr;
-                cs.N = N;
-                cs.q = q;
-                cs.S = S;
-                cs.kap = ctl->build_kappa;
-                cs.t_shell = ctl->build_t_shell;
-                cs.Di = Di;
-                cs.kapf = static_cast<float>(cs.kap);
-                cs.tf = static_cast<float>(cs.t_shell);
-                cs.Dif = static_cast<float>(D0i) * cs.kapf;
-                cs.bx = g.box;
-                cs.ibx = g.inv_box;
-                cs.hbf = s_hbf;
-                RCPG_UNROLL
-                for (int d = 0; d < ND; ++d) {
-                    cs.xi[d] = xi[d];
-                    cs.fi[d] = 0.0;
-                    cs.fif[d] = 0.0f;
-                }
-                cs.fuse = fuse;
-                cs.n = 0;
-                cs.U = cs.Lc = cs.dk = cs.Fm = cs.maxov = 0.0;
-                cs.count = 0;
-                // the stage serves this lane when its relative position keeps
-                // its candidates' differences at their minimum image
-                bool use_stage = staged;
-                use_stage = use_stage && fabsf(me.x) < s_guard[0] && fabsf(me.y) < s_guard[1];
-                if constexpr (NDC == 3) use_stage = use_stage && fabsf(me.z) < s_guard[2];
-                // prefilter cutoff of a candidate with FP32 diameter w: w * pa + pb
-                const float pa = 0.5f * cs.kapf * kPrefilterLin;
-                const float pb = __fmaf_rn(0.5f * cs.Dif + cs.tf, kPrefilterLin, s_eabs);
-                // FP64 variant: the lane's candidates in scan order go through
-                // two phases -- the FP32 prefilter (staged ones) fills the
-                // lane's list, and the exact test runs over the list, when it
-                // is full and at the end, with the lanes in step over lists of
-                // similar length. Mixed variant: the exact test follows each
-                // candidate that passes (its FP32 test is cheap enough that the
-                // list costs more than the divergence it removes).
-                std::uint32_t* lst = cell_lists + static_cast<std::size_t>(warp) * (kCellList * 32) + lane;
-                std::uint32_t nl = 0;
-                auto drain = [&]() {
-                    for (std::uint32_t k = 0; k < nl; ++k) {
-                        const std::uint32_t p = lst[k * 32];
-                        double xj[ND], D0j;
-                        load_pos_g<ND>(a.pos, p, xj, D0j, 1);
-                        cs.test(p, xj, D0j);
-                    }
-                    nl = 0;
-                };
-                auto push = [&](std::uint32_t p) {
-                    if constexpr (MX) {
-                        double xj[ND], D0j;
-                        load_pos_g<ND>(a.pos, p, xj, D0j, 1);
-                        cs.test(p, xj, D0j);
-                    } else {
-                        lst[nl * 32] = p;
-                        if (++nl == static_cast<std::uint32_t>(kCellList)) drain();
-                    }
-                };
-                for (int r = 0; r < NROW; ++r) {
-                    std::uint32_t a0, a1, b0, b1;
-                    cell_row_ranges<NDC>(r, ci, nc, a.cell_start, a0, a1, b0, b1);
-                    if (use_stage) {
-                        // this lane's range lies inside the warp's window [u0, u1)
-                        const float4* w = stage + s_win[warp][r][2];
-                        const std::uint32_t u0 = s_win[warp][r][0];
-                        for (std::uint32_t p = a0; p < a1; ++p) {
-                            const float4 c = w[p - u0];
-                            const float ex = c.x - me.x, ey = c.y - me.y, ez = NDC == 3 ? c.z - me.z : 0.0f;
-                            const float d2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, ex * ex));
-                            const float rl = __fmaf_rn(c.w, pa, pb);
-                            if (d2 < rl * rl && p != q) push(p);
-                        }
-                    } else {
-                        for (std::uint32_t p = a0; p < a1; ++p)
-                            if (p != q) push(p);
-                    }
-                    for (std::uint32_t p = b0; p < b1; ++p)
-                        if (p != q) push(p);
-                }
-                if constexpr (!MX) drain();
-                n = cs.n;
-                RCPG_UNROLL
-                for (int d = 0; d < ND; ++d) fi[d] = MX ? static_cast<double>(cs.fif[d]) : cs.fi[d];
-                sU = xadd(sU, cs.U);
-                sLc = xadd(sLc, cs.Lc);
-                sdk = xadd(sdk, cs.dk);
-                sFm = xadd(sFm, cs.Fm);
-                smax = fmax(smax, cs.maxov);
-                scount += cs.count;
-            }
-            // the reference's capacity check counts the partners after i in its
-            // own order; a row that fits the capacity in full needs no count
-            const std::uint32_t cap = a.caps[q];
-            if (n > cap && n <= S) {
-                const std::uint32_t rq = a.ref_rank[q];
-                std::uint32_t n_half = 0;
-                for (std::uint32_t k = 0; k < n; ++k)
-                    n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
-                if (n_half > cap) report_cap_error(ctl, rq, cap);
-            }
-            need = max(need, n);
-            if (n > S) {
-                a.nbr_cnt[q] = 0u;  // overflow: empty row, rebuilt after the capacity grows
-                overflow = true;
-            } else {
-                a.nbr_cnt[q] = n;
-                if (fuse) {
-                    std::uint32_t wc = 0;
-                    wall_forces<ND>(xi, Di, g, fi, sU, sdk, sFm, wc);
-                    scount += wc;
-                    const double f2 = force_norm2<ND>(fi);
-                    if (f2 > 1.0E-16) {
-                        smag = xadd(smag, xsqrt(f2));
-                        ++smagc;
-                    }
-                    sD = xadd(sD, Di);
-                    RCPG_UNROLL
-                    for (int d = 0; d < ND; ++d) a.F[q * ND + d] = fi[d];
-                }
-            }
-        }
-        __syncwarp();  // the stage is reused by the warp's next particles
-    }
-    if (overflow && fuse) ctl->forces_done = 0u;
-    // block maximum of the row lengths, one atomic per block
+    const Geometry& g = ctl->g;
+    double bx[ND], ibx[ND];
+    float hbf[ND];
     RCPG_UNROLL
-    for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_xor_sync(0xffffffffu, need, o));
-    __syncthreads();
-    if (lane == 0 && need) atomicMax(&s_need, need);
+    for (int d = 0; d < ND; ++d) {
+        bx[d] = g.box[d];
+        ibx[d] = g.inv_box[d];
+        hbf[d] = static_cast<float>(0.5 * g.box[d]);
+    }
+    int nc[NDC];
+    RCPG_UNROLL
+    for (int d = 0; d < NDC; ++d) nc[d] = ctl->ncell[d];
+    const double scale0 = ctl->cell_scale[0];
+    const std::uint32_t W = ctl->unit_w, chunks = ctl->unit_chunks, units = ctl->unit_count;
+    const double kap = BUILD ? ctl->build_kappa : ctl->force_kappa;
+    const double t_shell = ctl->build_t_shell;
+    const float tf = static_cast<float>(t_shell);
+    const bool fuse = BUILD ? (ctl->forces_done != 0u) : true;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) {
+        ctl->nsum_blocks = gridDim.x;
+        if constexpr (!BUILD) ctl->pair_kernel_runs += 1ull;
+    }
+    if (threadIdx.x == 0) s_need = 0u;
+    const int col = threadIdx.x;
+    RCPG_UNROLL
+    for (int f = 0; f < 7; ++f) s_acc[f][col] = 0.0;
+    s_accn[0][col] = s_accn[1][col] = 0u;
+    std::uint32_t need = 0;
+    bool overflow = false;
+    for (std::uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
+        const std::uint32_t row0 = u / chunks;
+        const int cx0 = static_cast<int>((u - row0 * chunks) * W);
+        const int cx1 = min(cx0 + static_cast<int>(W), nc[0]);
+        const int y0 = static_cast<int>(row0 % static_cast<std::uint32_t>(nc[1]));
+        const int z0 = NDC == 3 ? static_cast<int>(row0 / static_cast<std::uint32_t>(nc[1])) : 0;
+        const int cl = max(cx0 - 1, 0), ch = min(cx1 + 1, nc[0]);
+        const int cnt = ch - cl + 1;  // cell_start entries of one row's slice
+        // first cell of the grid row at row offset r
+        auto rowbase = [&](int r) -> std::uint64_t {
+            int y = y0 + (r % 3) - 1;
+            y = y < 0 ? y + nc[1] : (y >= nc[1] ? y - nc[1] : y);
+            std::uint64_t row = static_cast<std::uint64_t>(y);
+            if constexpr (NDC == 3) {
+                int z = z0 + (r / 3) - 1;
+                z = z < 0 ? z + nc[2] : (z >= nc[2] ? z - nc[2] : z);
+                row += static_cast<std::uint64_t>(z) * static_cast<std::uint64_t>(nc[1]);
+            }
+            return row * static_cast<std::uint64_t>(nc[0]);
+        };
+        __syncthreads();  // the previous unit is finished with the shared arrays
+        // 1. cell_start entries
+        if constexpr (BUILD) {
+            for (int t = threadIdx.x; t < R * cnt; t += T) {
+                const int r = t / cnt, c = t - r * cnt;
+                s_cs[r * US::slice + c] = a.cell_start[rowbase(r) + static_cast<std::uint64_t>(cl + c)];
+            }
+        }
+        if (threadIdx.x < R) {
+            const int r = threadIdx.x;
+            const std::uint32_t* cs = a.cell_start + rowbase(r);
+            const std::uint32_t mb = cs[cl], me = cs[ch];
+            std::uint32_t lb = 0, le = 0, rb = 0, re = 0;
+            if (cx0 == 0) {
+                lb = cs[nc[0] - 1];
+                le = cs[nc[0]];
+            }
+            if (cx1 == nc[0]) {
+                rb = cs[0];
+                re = cs[1];
+            }
+            s_wb[3 * r] = mb;
+            s_wl[3 * r] = me - mb;
+            s_wb[3 * r + 1] = lb;
+            s_wl[3 * r + 1] = le - lb;
+            s_wb[3 * r + 2] = rb;
+            s_wl[3 * r + 2] = re - rb;
+            if (r == CR) {
+                s_qa = cs[cx0];
+                s_qb = cs[cx1];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            std::uint32_t tot = 0;
+            for (int w = 0; w < NW; ++w) {
+                s_ws[w] = tot;
+                tot += s_wl[w];
+            }
+            s_total = tot;
+            if (tot > static_cast<std::uint32_t>(US::stage))  // not staged: records read from pos
+                for (int w = 0; w < NW; ++w) s_ws[w] = s_wb[w];
+            if constexpr (!BUILD) {
+                // non-empty windows sorted by first particle (insertion sort)
+                std::uint32_t n = 0;
+                for (int w = 0; w < NW; ++w) {
+                    if (s_wl[w] == 0u) continue;
+                    std::uint32_t p = n++;
+                    while (p > 0 && s_lb[p - 1] > s_wb[w]) {
+                        s_lb[p] = s_lb[p - 1];
+                        s_ll[p] = s_ll[p - 1];
+                        s_ls[p] = s_ls[p - 1];
+                        --p;
+                    }
+                    s_lb[p] = s_wb[w];
+                    s_ll[p] = s_wl[w];
+                    s_ls[p] = s_ws[w];
+                }
+                s_nl = n;
+            }
+        }
+        __syncthreads();
+        const std::uint32_t total = s_total;
+        const bool staged = total <= static_cast<std::uint32_t>(US::stage);
+        // 2. stage the windows: each thread copies records tid, tid + T, ... of
+        // their concatenation, four loads in flight before the stores
+        if (staged) {
+            int wc = 0;
+            for (std::uint32_t e0 = threadIdx.x; e0 < total; e0 += 4u * T) {
+                double2 lo[4], hi[4];
+                RCPG_UNROLL
+                for (int k = 0; k < 4; ++k) {
+                    const std::uint32_t e = e0 + static_cast<std::uint32_t>(k * T);
+                    if (e < total) {
+                        while (e - s_ws[wc] >= s_wl[wc]) ++wc;
+                        const std::uint64_t p = s_wb[wc] + (e - s_ws[wc]);
+                        ld_record(a.pos + 4 * p, lo[k], hi[k]);
+                    }
+                }
+                RCPG_UNROLL
+                for (int k = 0; k < 4; ++k) {
+                    const std::uint32_t e = e0 + static_cast<std::uint32_t>(k * T);
+                    if (e < total) {
+                        double2* dst = reinterpret_cast<double2*>(u_stage + 4 * static_cast<std::size_t>(e));
+                        dst[0] = lo[k];
+                        dst[1] = hi[k];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        const double* recs = staged ? u_stage : a.pos;  // record s at recs + 4 s
+        auto record = [&](std::uint32_t s, double* x, double& D0) {
+            const double2* r2 = reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(s));
+            unpack_record<ND>(r2[0], r2[1], x, D0);
+        };
+        const std::uint32_t own_b = s_wb[3 * CR], own_s = s_ws[3 * CR];
+        // 3. the unit's particles
+        for (std::uint32_t q = s_qa + threadIdx.x; q < s_qb; q += T) {
+            double xq[ND], D0q;
+            record(own_s + (q - own_b), xq, D0q);
+            UnitPair<ND, MX> up;
+            up.begin(xq, D0q, kap);
+            std::uint32_t n = 0;
+            if constexpr (BUILD) {
+                // the binning's cell (same arithmetic and positions), held
+                // inside the unit so that every slice index stays in range
+                const int cx = min(max(cell_coord(xq[0], scale0, nc[0]), cx0), cx1 - 1);
+                const int lo = cx == 0 ? 0 : (cx == nc[0] - 1 ? nc[0] - 2 : cx - 1);
+                const int hi = cx == 0 ? 2 : (cx == nc[0] - 1 ? nc[0] : cx + 2);
+                auto scan = [&](std::uint32_t pb, std::uint32_t pe, std::uint32_t s0) {
+                    for (std::uint32_t p = pb; p < pe; ++p) {
+                        if (p == q) continue;
+                        double xj[ND], D0j;
+                        record(s0 + (p - pb), xj, D0j);
+                        if (up.candidate(p > q, xj, D0j, bx, ibx, hbf, t_shell, tf, fuse)) {
+                            if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = p;
+                            ++n;
+                        }
+                    }
+                };
+                for (int r = 0; r < R; ++r) {
+                    const std::uint32_t* sl = s_cs + r * US::slice;
+                    const std::uint32_t mb = s_wb[3 * r], ms = s_ws[3 * r];
+                    if (cx == 0) scan(s_wb[3 * r + 1], s_wb[3 * r + 1] + s_wl[3 * r + 1], s_ws[3 * r + 1]);
+                    const std::uint32_t pb = sl[lo - cl], pe = sl[hi - cl];
+                    scan(pb, pe, ms + (pb - mb));
+                    if (cx == nc[0] - 1) scan(s_wb[3 * r + 2], s_wb[3 * r + 2] + s_wl[3 * r + 2], s_ws[3 * r + 2]);
+                }
+                // the reference's capacity check counts the partners after q in
+                // its own order; a row that fits the capacity in full needs no count
+                const std::uint32_t cap = a.caps[q];
+                if (n > cap && n <= S) {
+                    const std::uint32_t rq = a.ref_rank[q];
+                    std::uint32_t n_half = 0;
+                    for (std::uint32_t k = 0; k < n; ++k)
+                        n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
+                    if (n_half > cap) report_cap_error(ctl, rq, cap);
+                }
+                need = max(need, n);
+                if (n > S) {
+                    a.nbr_cnt[q] = 0u;  // overflow: empty row, rebuilt after the capacity grows
+                    overflow = true;
+                    continue;
+                }
+                a.nbr_cnt[q] = n;
+                if (!fuse) continue;
+            } else {
+                n = min(a.nbr_cnt[q], S);
+                const std::uint32_t nl = s_nl;
+                constexpr std::uint32_t kChunk = 4;
+                for (std::uint32_t k0 = 0; k0 < n; k0 += kChunk) {
+                    std::uint32_t jj[kChunk];
+                    RCPG_UNROLL
+                    for (std::uint32_t v = 0; v < kChunk; ++v)
+                        jj[v] = (k0 + v < n) ? __ldg(a.nbr + static_cast<std::uint64_t>(k0 + v) * N + q) : 0u;
+                    RCPG_UNROLL
+                    for (std::uint32_t v = 0; v < kChunk; ++v) {
+                        if (k0 + v >= n) break;
+                        const std::uint32_t j = jj[v];
+                        if (j >= N) continue;
+                        // last window starting at or before j
+                        std::uint32_t lo = 0, len = nl;
+                        while (len > 1) {
+                            const std::uint32_t h = len >> 1;
+                            if (s_lb[lo + h] <= j) lo += h;
+                            len -= h;
+                        }
+                        double xj[ND], D0j;
+                        if (nl && j - s_lb[lo] < s_ll[lo]) {
+                            record(s_ls[lo] + (j - s_lb[lo]), xj, D0j);
+                        } else {
+                            double2 rl, rh;
+                            ld_record(a.pos + 4 * static_cast<std::uint64_t>(j), rl, rh);
+                            unpack_record<ND>(rl, rh, xj, D0j);
+                        }
+                        up.row_partner(j > q, xj, D0j, bx, ibx, hbf);
+                    }
+                }
+            }
+            double f[ND];
+            up.force(f);
+            s_acc[0][col] = xadd(s_acc[0][col], static_cast<double>(up.sU));
+            s_acc[1][col] = xadd(s_acc[1][col], static_cast<double>(up.sLc));
+            s_acc[2][col] = xadd(s_acc[2][col], static_cast<double>(up.sdk));
+            s_acc[3][col] = xadd(s_acc[3][col], static_cast<double>(up.sFm));
+            s_acc[4][col] = fmax(s_acc[4][col], static_cast<double>(up.smax));
+            std::uint32_t wc = 0;
+            wall_forces<ND>(xq, up.Di, g, f, s_acc[0][col], s_acc[2][col], s_acc[3][col], wc);
+            s_accn[0][col] += up.scount + wc;
+            const double f2 = force_norm2<ND>(f);
+            if (f2 > 1.0E-16) {
+                s_acc[5][col] = xadd(s_acc[5][col], xsqrt(f2));
+                ++s_accn[1][col];
+            }
+            s_acc[6][col] = xadd(s_acc[6][col], up.Di);
+            RCPG_UNROLL
+            for (int d = 0; d < ND; ++d) a.F[static_cast<std::uint64_t>(q) * ND + d] = f[d];
+        }
+    }
+    if constexpr (BUILD) {
+        if (overflow && fuse) ctl->forces_done = 0u;
+        // block maximum of the row lengths, one atomic per block
+        RCPG_UNROLL
+        for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_xor_sync(0xffffffffu, need, o));
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0 && need) atomicMax(&s_need, need);
+    }
     if (fuse) {
         ForceSums fs;
         sums_zero(fs);
-        fs.pair_U = sU;
-        fs.pair_Lc = sLc;
-        fs.pair_dk = sdk;
-        fs.pair_Fm = sFm;
-        fs.pair_maxov = smax;
-        fs.sum_mag = smag;
-        fs.sum_D = sD;
-        fs.pair_count = scount;
-        fs.mag_count = smagc;
-        block_reduce_sums<kCellThreads>(fs, s_red);  // ends with a block barrier before thread 0 reads
+        fs.pair_U = s_acc[0][col];
+        fs.pair_Lc = s_acc[1][col];
+        fs.pair_dk = s_acc[2][col];
+        fs.pair_Fm = s_acc[3][col];
+        fs.pair_maxov = s_acc[4][col];
+        fs.sum_mag = s_acc[5][col];
+        fs.sum_D = s_acc[6][col];
+        fs.pair_count = s_accn[0][col];
+        fs.mag_count = s_accn[1][col];
+        block_reduce_sums<T>(fs, s_red);  // ends with a block barrier before thread 0 reads
         if (threadIdx.x == 0) a.block_sums[blockIdx.x] = fs;
     } else {
         __syncthreads();
     }
-    if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
+    if constexpr (BUILD) {
+        if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
+    }
 }
 
-// dynamic shared memory of k_build_search_cells<ND, MX> (the candidate lists
-// only in the FP64 variant; the mixed one leaves the space to L1)
-template <int ND, bool MX>
+// dynamic shared memory of k_cells<ND, *, BUILD>: the stage, and the build's
+// cell_start slices
+template <int ND, bool BUILD>
 constexpr std::size_t cells_smem_bytes() {
-    return static_cast<std::size_t>(kCellWarps) *
-           (CellStage<(ND <= 3 ? ND : 3)>::cap * sizeof(float4) + (MX ? 0 : kCellList * 32 * sizeof(std::uint32_t)));
+    using US = UnitShape<ND>;
+    return static_cast<std::size_t>(US::stage) * 4 * sizeof(double) +
+           (BUILD ? static_cast<std::size_t>(US::rows) * US::slice * sizeof(std::uint32_t) : 0);
 }
 
 // ===========================================================================
@@ -1415,6 +1519,9 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
         // one round trip for every flag of the early exit
         const std::uint32_t st = ctl->stopped, ha = ctl->halted, fd = ctl->forces_done, p32 = ctl->pair_fp32;
         if ((st | ha | fd) != 0u || MIXED != (!EXACT && p32 != 0u)) return;
+    }
+    if constexpr (!EXACT) {
+        if (a.permute && use_cells<ND>(a)) return;  // the cell-unit pair kernel takes the step
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.ctl->nsum_blocks = gridDim.x;
@@ -2132,8 +2239,36 @@ void adam_nd(const DevArrays& a, int do_adam, int do_refresh, cudaStream_t st) {
 
 // persistent force grid: at most the blocks resident at once (the block-sum
 // buffers hold at least force_blocks(N) entries)
+// persistent grid of the cell-unit kernels: the blocks resident at once (at
+// most 4096, the engine's block-sum entries)
+template <int ND, bool MX, bool BUILD>
+void launch_cells_variant(const DevArrays& a, cudaStream_t st) {
+    if constexpr (ND <= 3) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        constexpr std::size_t smem = cells_smem_bytes<ND, BUILD>();
+        constexpr int T = UnitShape<ND>::threads;
+        static int grid[64] = {};
+        if (dev >= 0 && dev < 64 && grid[dev] == 0) {
+            cudaFuncSetAttribute(k_cells<ND, MX, BUILD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+            int sms = 148, per_sm = 1;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cells<ND, MX, BUILD>, T, smem);
+            const int gr = sms * (per_sm > 0 ? per_sm : 1);
+            grid[dev] = gr < 4096 ? gr : 4096;
+        }
+        const unsigned g = (dev >= 0 && dev < 64) ? static_cast<unsigned>(grid[dev]) : 148u;
+        k_cells<ND, MX, BUILD><<<g, T, smem, st>>>(a);
+    }
+}
+
+// The pair kernel: k_forces over the rows and, with cell-order storage (graph
+// mode, ndim <= 3), the cell-unit pair kernel; the one that does not apply to
+// the step returns at once.
 template <int ND, bool EXACT, bool MIXED>
 void forces_nd(const DevArrays& a, cudaStream_t st) {
+    if (!EXACT && a.permute && ND <= 3 && a.N >= kTiledMinN) launch_cells_variant<ND, MIXED, false>(a, st);
     const unsigned need = force_blocks(a.N), g = resident_grid<k_forces<ND, EXACT, MIXED>>(kForceBlock);
     k_forces<ND, EXACT, MIXED><<<need < g ? need : g, kForceBlock, 0, st>>>(a);
 }
@@ -2157,32 +2292,12 @@ void launch_tiled(const DevArrays& a, cudaStream_t st) {
     k_build_search_tiled<ND><<<static_cast<unsigned>(blocks), kTileThreads, smem, st>>>(a);
 }
 
-// persistent grid of the cell-order search: the blocks resident at once
-template <int ND, bool MX>
-void launch_cells_variant(const DevArrays& a, cudaStream_t st) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    constexpr std::size_t smem = cells_smem_bytes<ND, MX>();
-    static int grid[64] = {};
-    if (dev >= 0 && dev < 64 && grid[dev] == 0) {
-        cudaFuncSetAttribute(k_build_search_cells<ND, MX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-        int sms = 148, per_sm = 1;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_search_cells<ND, MX>, kCellThreads, smem);
-        grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
-    }
-    const unsigned g = (dev >= 0 && dev < 64) ? static_cast<unsigned>(grid[dev]) : 148u;
-    const unsigned need = static_cast<unsigned>((a.N + kCellThreads - 1) / kCellThreads);
-    k_build_search_cells<ND, MX><<<need < g ? need : g, kCellThreads, smem, st>>>(a);
-}
-
 // both precisions where the run may use FP32 pair terms (the one that does
 // not match the step returns at once)
 template <int ND>
 void launch_cells(const DevArrays& a, cudaStream_t st) {
-    launch_cells_variant<ND, false>(a, st);
-    if (a.mixed) launch_cells_variant<ND, true>(a, st);
+    launch_cells_variant<ND, false, true>(a, st);
+    if (a.mixed) launch_cells_variant<ND, true, true>(a, st);
 }
 
 // e0 / e1 (optional): events recorded around the search kernels only

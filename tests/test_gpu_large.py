@@ -1,5 +1,6 @@
 """Parity at N >= 20,000, where the neighbour build of ndim <= 3 packings with
-one size class switches to the tiled search (k_build_search_tiled), against
+one size class switches to the tiled search (k_build_search_tiled, rows in
+particle order) or, in the graph engine, to the cell-unit search (k_cells), against
 the reference engine's own outputs (tests/golden/large_*.npz, written by
 tests/golden/make_large_golden.py from the compiled reference):
 
@@ -14,7 +15,9 @@ tests/golden/make_large_golden.py from the compiled reference):
   rows are summed in scan order instead of ascending order); in mixed
   precision its rows are a superset of the FP64 shell (every extra pair lies
   within the 1e-5 relative widening) and its forces are within 1e-4 of the
-  largest FP64 force.
+  largest FP64 force;
+* the cell-unit pair kernel of the steps without a build gives the fused
+  build's forces on the same rows bit for bit.
 
 The power-law case (size ratio 10) has several size classes and takes the warp
 search at this N; it pins that path at large N the same way.
@@ -190,6 +193,23 @@ def test_scan_build_fp64_fused_forces(cuda_device, native, golden, case):
     for k in (0, 2, 3, 4):
         assert abs(sc[k] - ref[k]) <= 1e-12 * abs(ref[k]), k
     assert abs(sc[5] - float(g["mean_force"])) <= 1e-12 * abs(float(g["mean_force"]))
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if FUSED[c]])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_cell_pair_kernel_equals_fused_build(cuda_device, native, golden, case, precision):
+    """The pair kernel of the steps without a build (cell units: row entries
+    looked up in the staged windows) sums the same rows in the same order as
+    the build that fused the forces: identical forces, FP64 and mixed."""
+    g = golden(f"large_{case}.npz")
+    _, cnt, _, F, sc, fused = _scan_build(native, g, precision)
+    _, cnt2, _, F2, sc2, fused2 = _scan_build(native, g, precision + 2)
+    assert fused == fused2 == 1
+    assert np.array_equal(cnt.cpu().numpy(), cnt2.cpu().numpy())
+    assert np.array_equal(F, F2)
+    assert sc[1] == sc2[1] and sc[6] == sc2[6]
+    for k in (0, 2, 3, 4, 5):
+        assert abs(sc[k] - sc2[k]) <= 1e-12 * abs(sc[k]), k
 
 
 def _mic_d2_rc2(g, own, other, t):
