@@ -211,18 +211,35 @@ RCPG_UNROLL
 // FP32 (ENG:4105-4139 with FP32 operands); the force is added to the FP32
 // per-particle sum fi, the scalar terms go to the FP64 accumulators. The
 // overlap-dependent terms carry a relative error of about 1e-7 / overlap.
+// The scalar terms of the FP32 pair path, kept in FP32: the per-particle sums
+// of that path are FP32, so the terms never need an FP64 round trip.
+struct PairTermsF {
+    float U, Lc, dk, Fm;
+};
+
 template <int ND>
-__device__ __forceinline__ void pair_terms_mixed(const float* dxf, float d2, float rsum, float* fi,
-                                                 PairTerms& pt) {
+__device__ __forceinline__ void pair_terms_mixed_f(const float* dxf, float d2, float rsum, float* fi,
+                                                   PairTermsF& pt) {
     const float inv_dist = rsqrtf(d2);
     const float dist = d2 * inv_dist;
     const float F_mag = __fmaf_rn(-rsum, inv_dist, 1.0f);  // -(r/dist - 1)
 RCPG_UNROLL
     for (int d = 0; d < ND; ++d) fi[d] = __fmaf_rn(F_mag, dxf[d], fi[d]);
-    pt.U = static_cast<double>(1.0f - __fdividef(dist, rsum));
-    pt.Lc = static_cast<double>(rsum);
-    pt.dk = static_cast<double>(rsum * (dist - rsum));
-    pt.Fm = static_cast<double>(F_mag);
+    pt.U = 1.0f - __fdividef(dist, rsum);
+    pt.Lc = rsum;
+    pt.dk = rsum * (dist - rsum);
+    pt.Fm = F_mag;
+}
+
+template <int ND>
+__device__ __forceinline__ void pair_terms_mixed(const float* dxf, float d2, float rsum, float* fi,
+                                                 PairTerms& pt) {
+    PairTermsF f;
+    pair_terms_mixed_f<ND>(dxf, d2, rsum, fi, f);
+    pt.U = static_cast<double>(f.U);
+    pt.Lc = static_cast<double>(f.Lc);
+    pt.dk = static_cast<double>(f.dk);
+    pt.Fm = static_cast<double>(f.Fm);
 }
 #endif
 

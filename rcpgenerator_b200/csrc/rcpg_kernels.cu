@@ -136,7 +136,7 @@ struct UnitShape {
     static constexpr int maxw = ndc == 2 ? 256 : 128;    // cells per unit at most
     static constexpr int slice = maxw + 3;               // cell_start entries per row (build)
     static constexpr int windows = 3 * rows;             // main, wrapped x-1, wrapped x+1 per row
-    static constexpr int min_blocks = 6;                 // resident blocks per SM (register budget)
+    static constexpr int min_blocks = 5;                 // resident blocks per SM (register budget)
 };
 
 // Cells per unit for a build with `cells` cells in a grid of nc0 cells per row:
@@ -1114,42 +1114,47 @@ struct UnitPair {
         scount = 0;
     }
 
-    __device__ __forceinline__ void add_scalars(const PairTerms& pt) {
-        if constexpr (MX) {
-            sU += static_cast<float>(pt.U);
-            sLc += static_cast<float>(pt.Lc);
-            sdk += static_cast<float>(pt.dk);
-            sFm += static_cast<float>(pt.Fm);
-            smax = fmaxf(smax, static_cast<float>(pt.U));
-        } else {
+    // Pair terms of an overlapping pair (FP32 terms summed in FP32, or FP64);
+    // the scalars once per pair, from the lower index.
+    __device__ __forceinline__ void overlap_f32(bool upper, const float* dxf, float d2f, float rsum) {
+        PairTermsF pf;
+        pair_terms_mixed_f<ND>(dxf, d2f, rsum, fif, pf);
+        if (upper) {
+            sU += pf.U;
+            sLc += pf.Lc;
+            sdk += pf.dk;
+            sFm += pf.Fm;
+            smax = fmaxf(smax, pf.U);
+            ++scount;
+        }
+    }
+    __device__ __forceinline__ void overlap_f64(bool upper, const double* dx, double d2, double r_ij) {
+        PairTerms pt;
+        pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
+        if (upper) {
             sU = xadd(sU, pt.U);
             sLc = xadd(sLc, pt.Lc);
             sdk = xadd(sdk, pt.dk);
             sFm = xadd(sFm, pt.Fm);
             smax = fmax(smax, pt.U);
+            ++scount;
         }
-        ++scount;
     }
 
-    // Partner with record (xj, D0j) of a row (as k_forces): pair terms of an
-    // overlapping pair; scalars once per pair, from the lower index.
+    // Partner with record (xj, D0j) of a row (as k_forces).
     __device__ __forceinline__ void row_partner(bool upper, const double* xj, double D0j, const double* bx,
                                                 const double* ibx, const float* hbf) {
-        PairTerms pt;
         if constexpr (MX) {
             float dxf[ND];
             const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
             const float rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
-            if (!(d2f < rsum * rsum)) return;
-            pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
+            if (d2f < rsum * rsum) overlap_f32(upper, dxf, d2f, rsum);
         } else {
             const double r_ij = xmul(0.5, xadd(Di, xmul(D0j, kap)));
             double dx[ND];
             const double d2 = pair_disp<ND>(xi, xj, bx, ibx, dx);
-            if (!(d2 < xmul(r_ij, r_ij))) return;
-            pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
+            if (d2 < xmul(r_ij, r_ij)) overlap_f64(upper, dx, d2, r_ij);
         }
-        if (upper) add_scalars(pt);
     }
 
     // Candidate of a build: the shell test; on a pass the pair terms when
@@ -1157,15 +1162,13 @@ struct UnitPair {
     __device__ __forceinline__ bool candidate(bool upper, const double* xj, double D0j, const double* bx,
                                               const double* ibx, const float* hbf, double t_shell, float tf,
                                               bool fuse) {
-        PairTerms pt;
         if constexpr (MX) {
             float dxf[ND];
             const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
             const float rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
             const float rc = rsum + tf;
             if (!(d2f < rc * rc * kShellMarginF)) return false;
-            if (!(fuse && d2f < rsum * rsum)) return true;
-            pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
+            if (fuse && d2f < rsum * rsum) overlap_f32(upper, dxf, d2f, rsum);
         } else {
             const double Dj = xmul(D0j, kap);
             double dx[ND];
@@ -1173,10 +1176,8 @@ struct UnitPair {
             const double r_c = shell_cut<ND>(Di, Dj, t_shell);  // ndim <= 3: symmetric
             if (!(d2 < xmul(r_c, r_c))) return false;
             const double r_ij = xmul(0.5, xadd(Di, Dj));
-            if (!(fuse && d2 < xmul(r_ij, r_ij))) return true;
-            pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
+            if (fuse && d2 < xmul(r_ij, r_ij)) overlap_f64(upper, dx, d2, r_ij);
         }
-        if (upper) add_scalars(pt);
         return true;
     }
 
@@ -1266,9 +1267,9 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
         __syncthreads();  // the previous unit is finished with the shared arrays
         // 1. cell_start entries
         if constexpr (BUILD) {
-            for (int t = threadIdx.x; t < R * cnt; t += T) {
-                const int r = t / cnt, c = t - r * cnt;
-                s_cs[r * US::slice + c] = a.cell_start[rowbase(r) + static_cast<std::uint64_t>(cl + c)];
+            for (int r = 0; r < R; ++r) {
+                const std::uint32_t* cs = a.cell_start + rowbase(r) + cl;
+                for (int c = threadIdx.x; c < cnt; c += T) s_cs[r * US::slice + c] = cs[c];
             }
         }
         if (threadIdx.x < R) {
@@ -1354,114 +1355,144 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
             }
         }
         __syncthreads();
-        const double* recs = staged ? u_stage : a.pos;  // record s at recs + 4 s
-        auto record = [&](std::uint32_t s, double* x, double& D0) {
-            const double2* r2 = reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(s));
-            unpack_record<ND>(r2[0], r2[1], x, D0);
-        };
         const std::uint32_t own_b = s_wb[3 * CR], own_s = s_ws[3 * CR];
-        // 3. the unit's particles
-        for (std::uint32_t q = s_qa + threadIdx.x; q < s_qb; q += T) {
-            double xq[ND], D0q;
-            record(own_s + (q - own_b), xq, D0q);
-            UnitPair<ND, MX> up;
-            up.begin(xq, D0q, kap);
-            std::uint32_t n = 0;
-            if constexpr (BUILD) {
-                // the binning's cell (same arithmetic and positions), held
-                // inside the unit so that every slice index stays in range
-                const int cx = min(max(cell_coord(xq[0], scale0, nc[0]), cx0), cx1 - 1);
-                const int lo = cx == 0 ? 0 : (cx == nc[0] - 1 ? nc[0] - 2 : cx - 1);
-                const int hi = cx == 0 ? 2 : (cx == nc[0] - 1 ? nc[0] : cx + 2);
-                auto scan = [&](std::uint32_t pb, std::uint32_t pe, std::uint32_t s0) {
-                    for (std::uint32_t p = pb; p < pe; ++p) {
-                        if (p == q) continue;
-                        double xj[ND], D0j;
-                        record(s0 + (p - pb), xj, D0j);
-                        if (up.candidate(p > q, xj, D0j, bx, ibx, hbf, t_shell, tf, fuse)) {
-                            if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = p;
-                            ++n;
-                        }
-                    }
-                };
-                for (int r = 0; r < R; ++r) {
-                    const std::uint32_t* sl = s_cs + r * US::slice;
-                    const std::uint32_t mb = s_wb[3 * r], ms = s_ws[3 * r];
-                    if (cx == 0) scan(s_wb[3 * r + 1], s_wb[3 * r + 1] + s_wl[3 * r + 1], s_ws[3 * r + 1]);
-                    const std::uint32_t pb = sl[lo - cl], pe = sl[hi - cl];
-                    scan(pb, pe, ms + (pb - mb));
-                    if (cx == nc[0] - 1) scan(s_wb[3 * r + 2], s_wb[3 * r + 2] + s_wl[3 * r + 2], s_ws[3 * r + 2]);
+        // 3. the unit's particles; records from the stage (shared memory) or,
+        // for a unit whose windows did not fit, from pos
+        auto particles = [&](auto staged_tag) {
+            constexpr bool STG = decltype(staged_tag)::value;
+            const double* recs = STG ? static_cast<const double*>(u_stage) : a.pos;  // record s at recs + 4 s
+            for (std::uint32_t q = s_qa + threadIdx.x; q < s_qb; q += T) {
+                double xq[ND], D0q;
+                {
+                    const double2* r2 = reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(own_s + (q - own_b)));
+                    unpack_record<ND>(r2[0], r2[1], xq, D0q);
                 }
-                // the reference's capacity check counts the partners after q in
-                // its own order; a row that fits the capacity in full needs no count
-                const std::uint32_t cap = a.caps[q];
-                if (n > cap && n <= S) {
-                    const std::uint32_t rq = a.ref_rank[q];
-                    std::uint32_t n_half = 0;
-                    for (std::uint32_t k = 0; k < n; ++k)
-                        n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
-                    if (n_half > cap) report_cap_error(ctl, rq, cap);
-                }
-                need = max(need, n);
-                if (n > S) {
-                    a.nbr_cnt[q] = 0u;  // overflow: empty row, rebuilt after the capacity grows
-                    overflow = true;
-                    continue;
-                }
-                a.nbr_cnt[q] = n;
-                if (!fuse) continue;
-            } else {
-                n = min(a.nbr_cnt[q], S);
-                const std::uint32_t nl = s_nl;
-                constexpr std::uint32_t kChunk = 4;
-                for (std::uint32_t k0 = 0; k0 < n; k0 += kChunk) {
-                    std::uint32_t jj[kChunk];
-                    RCPG_UNROLL
-                    for (std::uint32_t v = 0; v < kChunk; ++v)
-                        jj[v] = (k0 + v < n) ? __ldg(a.nbr + static_cast<std::uint64_t>(k0 + v) * N + q) : 0u;
-                    RCPG_UNROLL
-                    for (std::uint32_t v = 0; v < kChunk; ++v) {
-                        if (k0 + v >= n) break;
-                        const std::uint32_t j = jj[v];
-                        if (j >= N) continue;
-                        // last window starting at or before j
-                        std::uint32_t lo = 0, len = nl;
-                        while (len > 1) {
-                            const std::uint32_t h = len >> 1;
-                            if (s_lb[lo + h] <= j) lo += h;
-                            len -= h;
-                        }
-                        double xj[ND], D0j;
-                        if (nl && j - s_lb[lo] < s_ll[lo]) {
-                            record(s_ls[lo] + (j - s_lb[lo]), xj, D0j);
+                UnitPair<ND, MX> up;
+                up.begin(xq, D0q, kap);
+                std::uint32_t n = 0;
+                if constexpr (BUILD) {
+                    // the binning's cell (same arithmetic and positions), held
+                    // inside the unit so that every slice index stays in range
+                    const int cx = min(max(cell_coord(xq[0], scale0, nc[0]), cx0), cx1 - 1);
+                    const int lo = cx == 0 ? 0 : (cx == nc[0] - 1 ? nc[0] - 2 : cx - 1);
+                    const int hi = cx == 0 ? 2 : (cx == nc[0] - 1 ? nc[0] : cx + 2);
+                    for (int r = 0; r < R; ++r) {
+                        // up to two contiguous segments of the row in scan order:
+                        // [wrapped x-1 cell] cells lo..hi-1 [wrapped x+1 cell]
+                        const std::uint32_t* sl = s_cs + r * US::slice;
+                        const std::uint32_t pb = sl[lo - cl], pe = sl[hi - cl];
+                        std::uint32_t seg_p[2], seg_n[2], seg_s[2];
+                        const int wk = cx == 0 ? 1 : 2;  // wrapped window used, if any
+                        const std::uint32_t wb = s_wb[3 * r + wk], wl = s_wl[3 * r + wk], ws = s_ws[3 * r + wk];
+                        const std::uint32_t mp = pb, mn = pe - pb, ms = s_ws[3 * r] + (pb - s_wb[3 * r]);
+                        const bool wrap = (cx == 0) | (cx == nc[0] - 1);
+                        if (cx == 0) {
+                            seg_p[0] = wb; seg_n[0] = wl; seg_s[0] = ws;
+                            seg_p[1] = mp; seg_n[1] = mn; seg_s[1] = ms;
                         } else {
-                            double2 rl, rh;
-                            ld_record(a.pos + 4 * static_cast<std::uint64_t>(j), rl, rh);
-                            unpack_record<ND>(rl, rh, xj, D0j);
+                            seg_p[0] = mp; seg_n[0] = mn; seg_s[0] = ms;
+                            seg_p[1] = wb; seg_n[1] = wrap ? wl : 0u; seg_s[1] = ws;
                         }
-                        up.row_partner(j > q, xj, D0j, bx, ibx, hbf);
+                        const std::uint32_t tot = seg_n[0] + seg_n[1];
+                        for (std::uint32_t k = 0; k < tot; ++k) {
+                            const bool first = k < seg_n[0];
+                            const std::uint32_t o = first ? k : k - seg_n[0];
+                            const std::uint32_t p = (first ? seg_p[0] : seg_p[1]) + o;
+                            const std::uint32_t sidx = (first ? seg_s[0] : seg_s[1]) + o;
+                            if (p == q) continue;
+                            const double2* r2 = reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(sidx));
+                            double xj[ND], D0j;
+                            unpack_record<ND>(r2[0], r2[1], xj, D0j);
+                            if (up.candidate(p > q, xj, D0j, bx, ibx, hbf, t_shell, tf, fuse)) {
+                                if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = p;
+                                ++n;
+                            }
+                        }
+                    }
+                    // the reference's capacity check counts the partners after q in
+                    // its own order; a row that fits the capacity in full needs no count
+                    const std::uint32_t cap = a.caps[q];
+                    if (n > cap && n <= S) {
+                        const std::uint32_t rq = a.ref_rank[q];
+                        std::uint32_t n_half = 0;
+                        for (std::uint32_t k = 0; k < n; ++k)
+                            n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
+                        if (n_half > cap) report_cap_error(ctl, rq, cap);
+                    }
+                    need = max(need, n);
+                    if (n > S) {
+                        a.nbr_cnt[q] = 0u;  // overflow: empty row, rebuilt after the capacity grows
+                        overflow = true;
+                        continue;
+                    }
+                    a.nbr_cnt[q] = n;
+                    if (!fuse) continue;
+                } else {
+                    n = min(a.nbr_cnt[q], S);
+                    const std::uint32_t nl = STG ? s_nl : 0u;
+                    // chunks of kChunk entries: the row ids, then the windows and
+                    // records of all of them, before any pair arithmetic (the
+                    // pairs are still summed in row order); staged records are a
+                    // shared-memory read away, so two in flight cover them
+                    constexpr std::uint32_t kChunk = STG ? 2 : 4;
+                    for (std::uint32_t k0 = 0; k0 < n; k0 += kChunk) {
+                        std::uint32_t jj[kChunk];
+                        RCPG_UNROLL
+                        for (std::uint32_t v = 0; v < kChunk; ++v)
+                            jj[v] = (k0 + v < n) ? __ldg(a.nbr + static_cast<std::uint64_t>(k0 + v) * N + q)
+                                                 : 0xFFFFFFFFu;
+                        double xj[kChunk][ND], D0j[kChunk];
+                        RCPG_UNROLL
+                        for (std::uint32_t v = 0; v < kChunk; ++v) {
+                            const std::uint32_t j = jj[v];
+                            if (j >= N) continue;  // past the row's end
+                            double2 rl, rh;
+                            if constexpr (STG) {
+                                // the last window starting at or before j: windows
+                                // below it, counted without branches
+                                std::uint32_t w = 0;
+                                for (std::uint32_t k = 1; k < nl; ++k) w += j >= s_lb[k] ? 1u : 0u;
+                                const std::uint32_t off = j - s_lb[w];
+                                if (nl && off < s_ll[w]) {
+                                    const double2* r2 = reinterpret_cast<const double2*>(
+                                        recs + 4 * static_cast<std::size_t>(s_ls[w] + off));
+                                    rl = r2[0];
+                                    rh = r2[1];
+                                } else {
+                                    ld_record(a.pos + 4 * static_cast<std::uint64_t>(j), rl, rh);
+                                }
+                            } else {
+                                ld_record(a.pos + 4 * static_cast<std::uint64_t>(j), rl, rh);
+                            }
+                            unpack_record<ND>(rl, rh, xj[v], D0j[v]);
+                        }
+                        RCPG_UNROLL
+                        for (std::uint32_t v = 0; v < kChunk; ++v)
+                            if (jj[v] < N) up.row_partner(jj[v] > q, xj[v], D0j[v], bx, ibx, hbf);
                     }
                 }
+                double f[ND];
+                up.force(f);
+                s_acc[0][col] = xadd(s_acc[0][col], static_cast<double>(up.sU));
+                s_acc[1][col] = xadd(s_acc[1][col], static_cast<double>(up.sLc));
+                s_acc[2][col] = xadd(s_acc[2][col], static_cast<double>(up.sdk));
+                s_acc[3][col] = xadd(s_acc[3][col], static_cast<double>(up.sFm));
+                s_acc[4][col] = fmax(s_acc[4][col], static_cast<double>(up.smax));
+                std::uint32_t wc = 0;
+                wall_forces<ND>(xq, up.Di, g, f, s_acc[0][col], s_acc[2][col], s_acc[3][col], wc);
+                s_accn[0][col] += up.scount + wc;
+                const double f2 = force_norm2<ND>(f);
+                if (f2 > 1.0E-16) {
+                    s_acc[5][col] = xadd(s_acc[5][col], xsqrt(f2));
+                    ++s_accn[1][col];
+                }
+                s_acc[6][col] = xadd(s_acc[6][col], up.Di);
+                RCPG_UNROLL
+                for (int d = 0; d < ND; ++d) a.F[static_cast<std::uint64_t>(q) * ND + d] = f[d];
             }
-            double f[ND];
-            up.force(f);
-            s_acc[0][col] = xadd(s_acc[0][col], static_cast<double>(up.sU));
-            s_acc[1][col] = xadd(s_acc[1][col], static_cast<double>(up.sLc));
-            s_acc[2][col] = xadd(s_acc[2][col], static_cast<double>(up.sdk));
-            s_acc[3][col] = xadd(s_acc[3][col], static_cast<double>(up.sFm));
-            s_acc[4][col] = fmax(s_acc[4][col], static_cast<double>(up.smax));
-            std::uint32_t wc = 0;
-            wall_forces<ND>(xq, up.Di, g, f, s_acc[0][col], s_acc[2][col], s_acc[3][col], wc);
-            s_accn[0][col] += up.scount + wc;
-            const double f2 = force_norm2<ND>(f);
-            if (f2 > 1.0E-16) {
-                s_acc[5][col] = xadd(s_acc[5][col], xsqrt(f2));
-                ++s_accn[1][col];
-            }
-            s_acc[6][col] = xadd(s_acc[6][col], up.Di);
-            RCPG_UNROLL
-            for (int d = 0; d < ND; ++d) a.F[static_cast<std::uint64_t>(q) * ND + d] = f[d];
-        }
+        };
+        if (staged) particles(std::true_type{});
+        else particles(std::false_type{});
     }
     if constexpr (BUILD) {
         if (overflow && fuse) ctl->forces_done = 0u;
@@ -1589,14 +1620,26 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
                     if (k0 + u >= n) break;
                     const std::uint32_t j = jj[u];
                     if (j >= N) continue;
-                    PairTerms pt;
                     if constexpr (MX) {
+                        // FP32 terms summed in FP32 (EXACT never takes FP32 terms)
                         float dxf[ND];
                         const float d2f = mixed_disp<ND>(xi, xj[u], bx, hbf, dxf);
                         const float rsum = 0.5f * (Dif + static_cast<float>(D0j[u]) * kapf);
                         if (!(d2f < rsum * rsum)) continue;
-                        pair_terms_mixed<ND>(dxf, d2f, rsum, fif, pt);
-                    } else {
+                        PairTermsF pf;
+                        pair_terms_mixed_f<ND>(dxf, d2f, rsum, fif, pf);
+                        if (j > i) {
+                            sU += pf.U;
+                            sLc += pf.Lc;
+                            sdk += pf.dk;
+                            sFm += pf.Fm;
+                            smax = fmaxf(smax, pf.U);
+                            ++scount;
+                        }
+                        continue;
+                    }
+                    PairTerms pt;
+                    {
                         const double r_ij = xmul(0.5, xadd(Di, xmul(D0j[u], kap)));
                         double dx[ND];
                         const double d2 = pair_disp<ND>(xi, xj[u], bx, ibx, dx);
@@ -1607,13 +1650,6 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
                         if constexpr (EXACT) {
                             a.pterm[static_cast<std::uint64_t>(nterm) * N + i] = pt;
                             ++nterm;
-                        } else if constexpr (MX) {
-                            sU += static_cast<float>(pt.U);
-                            sLc += static_cast<float>(pt.Lc);
-                            sdk += static_cast<float>(pt.dk);
-                            sFm += static_cast<float>(pt.Fm);
-                            smax = fmaxf(smax, static_cast<float>(pt.U));
-                            ++scount;
                         } else {
                             sU = xadd(sU, pt.U);
                             sLc = xadd(sLc, pt.Lc);
