@@ -273,10 +273,9 @@ int32_t rcpg_pairs_full_noalloc(uint64_t N, int32_t ndim, const double* x_dev, c
  * pair_precision 1 = the graph engine's mixed precision (FP32 pair terms on
  * FP64 differences; the row test is widened by 1e-5 relative, so rows hold
  * every pair of the FP64 shell and a few just outside it), 0 = FP64; plus 2:
- * F_dev and scalars from the step's pair kernel on the new rows (the cell-unit
- * pair kernel where the build ran on cell units), also when the build fused
- * the forces. Diagnostic entry point for parity tests; no counterpart in the
- * reference. */
+ * F_dev and scalars from the pair kernel on the new rows, also when the build
+ * fused the forces. Diagnostic entry point for parity tests; no counterpart in
+ * the reference. */
 int32_t rcpg_pairs_forces_scan(uint64_t N, int32_t ndim, const double* x_dev, const double* D_dev,
                                const double* box, const int8_t* walls, double t_shell, double mu,
                                int32_t pair_precision, uint32_t row_capacity, uint32_t* nbr_dev,

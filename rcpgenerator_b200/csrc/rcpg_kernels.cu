@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(256) k_adam_refresh(DevArrays a, int do_adam, 
 constexpr int kTileRowsMin = 4, kTileRowsMax = 12, kTileRowsPref = 8;
 constexpr int kTileStage2 = 1024;  // staged particles per 2-D tile (TileShape<2>::stage)
 
-// Shape of the cell units of the cell-order kernels (k_cells, below).
+// Shape of the cell units of the cell-order search (k_cells, below).
 template <int ND>
 struct UnitShape {
     static constexpr int ndc = ND <= 3 ? ND : 3;
@@ -136,7 +136,7 @@ struct UnitShape {
     static constexpr int maxw = ndc == 2 ? 256 : 128;    // cells per unit at most
     static constexpr int slice = maxw + 3;               // cell_start entries per row (build)
     static constexpr int windows = 3 * rows;             // main, wrapped x-1, wrapped x+1 per row
-    static constexpr int min_blocks = 5;                 // resident blocks per SM (register budget)
+    static constexpr int min_blocks = 6;                 // resident blocks per SM (register budget)
 };
 
 // Cells per unit for a build with `cells` cells in a grid of nc0 cells per row:
@@ -1035,7 +1035,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
     if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
 }
 
-// ---- cell units: the cell-order search and pair kernel (graph mode) -------
+// ---- cell units: the cell-order search (graph mode) -------------------------
 // With cell-order storage the members of consecutive cells of one grid row
 // are one contiguous range of particles. A unit is a chunk of unit_w
 // consecutive cells of one grid row (2-D: row y; 3-D: row (y, z)), sized by
@@ -1046,27 +1046,23 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
 //      the end of the grid row, the cell at the row's other end (the wrapped
 //      x-1 / x+1 cell);
 //   2. the FP64 records of those windows -- contiguous ranges of pos -- into
-//      shared memory, with coalesced 256-bit loads by the whole block;
-//   3. one thread per particle of the unit, every partner read from shared
+//      shared memory, with coalesced 256-bit loads by the whole block (2-D:
+//      the record's spare slot takes the FP32 diameter of the mixed test);
+//   3. one thread per particle of the unit tests its candidates from shared
 //      memory (windows that do not fit the stage are read from pos instead:
-//      same code, other pointer).
-// k_cells<ND, MX, BUILD>:
-//   BUILD  the neighbour search of a build. A particle's candidates in scan
-//          order -- rows of the grid in order (row offset r = (dy+1) +
-//          3 (dz+1)), cells x-1, x, x+1 within a row (a wrapped cell in its
-//          place) -- go through the reference's predicate in FP64, or (MX) the
-//          mixed-precision shell test (FP32 on FP64 differences, widened by
-//          kShellMarginF so that the rows hold every pair of the FP64 shell);
-//          rows hold the partners in that order, and the step's forces are
-//          computed in the same pass.
-//   !BUILD the pair kernel of a step without a build: each particle's row
-//          entries (coalesced reads of nbr) are found in the staged windows by
-//          a binary search over the windows' first particles (every partner
-//          lies in one: the build took the rows from the same windows) and
-//          summed in row order with the arithmetic of k_forces, so the build
-//          and the pair kernel give the same forces bit for bit.
-// MX: FP32 pair terms; each variant returns at once when the step's pair
-// precision is the other one.
+//      the same code instantiated for global records).
+// A particle's candidates in scan order: the cells x-1, x, x+1 of each
+// neighbour row, rows in order (row offset r = (dy+1) + 3 (dz+1)), then the
+// wrapped cell of each row where the particle sits at the row's end (2-D: the
+// three rows' ranges are walked as one sequence, so the lanes of a warp run
+// about as many rounds as their longest candidate list). Each goes through
+// the reference's predicate in FP64, or (MX) the mixed-precision shell test
+// (FP32 on FP64 differences, widened by kShellMarginF so that the rows hold
+// every pair of the FP64 shell); rows hold the partners in that order and the
+// step's forces are computed in the same pass, summed in row order with the
+// arithmetic of k_forces (which gives the same forces on these rows bit for
+// bit). MX: each variant returns at once when the step's pair precision is
+// the other one.
 
 // 32-byte particle record (ndim <= 3) from global memory, one 256-bit load
 __device__ __forceinline__ void ld_record(const double* p, double2& lo, double2& hi) {
@@ -1087,8 +1083,17 @@ __device__ __forceinline__ void unpack_record(const double2& lo, const double2& 
     }
 }
 
-// Per-particle pair sums in the arithmetic of k_forces: FP32 (MX) or FP64
-// accumulators for the pair scalars, the force in FP32 (MX) or FP64.
+// FP32 diameter kept in the spare slot of a staged 2-D record
+__device__ __forceinline__ double pack_f32(float f) {
+    return __longlong_as_double(static_cast<long long>(__float_as_uint(f)));
+}
+__device__ __forceinline__ float unpack_f32(double d) {
+    return __uint_as_float(static_cast<unsigned>(__double_as_longlong(d)));
+}
+
+// One particle's candidate tests and its pair sums in the arithmetic of
+// k_forces: FP32 (MX) or FP64 accumulators for the pair scalars, the force in
+// FP32 (MX) or FP64.
 template <int ND, bool MX>
 struct UnitPair {
     using Acc = std::conditional_t<MX, float, double>;
@@ -1114,61 +1119,30 @@ struct UnitPair {
         scount = 0;
     }
 
-    // Pair terms of an overlapping pair (FP32 terms summed in FP32, or FP64);
-    // the scalars once per pair, from the lower index.
-    __device__ __forceinline__ void overlap_f32(bool upper, const float* dxf, float d2f, float rsum) {
-        PairTermsF pf;
-        pair_terms_mixed_f<ND>(dxf, d2f, rsum, fif, pf);
-        if (upper) {
-            sU += pf.U;
-            sLc += pf.Lc;
-            sdk += pf.dk;
-            sFm += pf.Fm;
-            smax = fmaxf(smax, pf.U);
-            ++scount;
-        }
-    }
-    __device__ __forceinline__ void overlap_f64(bool upper, const double* dx, double d2, double r_ij) {
-        PairTerms pt;
-        pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
-        if (upper) {
-            sU = xadd(sU, pt.U);
-            sLc = xadd(sLc, pt.Lc);
-            sdk = xadd(sdk, pt.dk);
-            sFm = xadd(sFm, pt.Fm);
-            smax = fmax(smax, pt.U);
-            ++scount;
-        }
-    }
-
-    // Partner with record (xj, D0j) of a row (as k_forces).
-    __device__ __forceinline__ void row_partner(bool upper, const double* xj, double D0j, const double* bx,
-                                                const double* ibx, const float* hbf) {
+    // Candidate (xj, D0j; D0jf = its FP32 diameter): the shell test; on a pass
+    // the pair terms when `fuse` and the pair overlaps, the scalars once per
+    // pair (from the lower index). Returns whether the candidate is a partner.
+    __device__ __forceinline__ bool candidate(bool upper, const double* xj, double D0j, float D0jf,
+                                              const double* bx, const double* ibx, const float* hbf,
+                                              double t_shell, float tf, bool fuse) {
         if constexpr (MX) {
             float dxf[ND];
             const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
-            const float rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
-            if (d2f < rsum * rsum) overlap_f32(upper, dxf, d2f, rsum);
-        } else {
-            const double r_ij = xmul(0.5, xadd(Di, xmul(D0j, kap)));
-            double dx[ND];
-            const double d2 = pair_disp<ND>(xi, xj, bx, ibx, dx);
-            if (d2 < xmul(r_ij, r_ij)) overlap_f64(upper, dx, d2, r_ij);
-        }
-    }
-
-    // Candidate of a build: the shell test; on a pass the pair terms when
-    // `fuse` and the pair overlaps. Returns whether the candidate is a partner.
-    __device__ __forceinline__ bool candidate(bool upper, const double* xj, double D0j, const double* bx,
-                                              const double* ibx, const float* hbf, double t_shell, float tf,
-                                              bool fuse) {
-        if constexpr (MX) {
-            float dxf[ND];
-            const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
-            const float rsum = 0.5f * (Dif + static_cast<float>(D0j) * kapf);
+            const float rsum = 0.5f * (Dif + D0jf * kapf);
             const float rc = rsum + tf;
             if (!(d2f < rc * rc * kShellMarginF)) return false;
-            if (fuse && d2f < rsum * rsum) overlap_f32(upper, dxf, d2f, rsum);
+            if (fuse && d2f < rsum * rsum) {
+                PairTermsF pf;
+                pair_terms_mixed_f<ND>(dxf, d2f, rsum, fif, pf);
+                if (upper) {
+                    sU += pf.U;
+                    sLc += pf.Lc;
+                    sdk += pf.dk;
+                    sFm += pf.Fm;
+                    smax = fmaxf(smax, pf.U);
+                    ++scount;
+                }
+            }
         } else {
             const double Dj = xmul(D0j, kap);
             double dx[ND];
@@ -1176,7 +1150,18 @@ struct UnitPair {
             const double r_c = shell_cut<ND>(Di, Dj, t_shell);  // ndim <= 3: symmetric
             if (!(d2 < xmul(r_c, r_c))) return false;
             const double r_ij = xmul(0.5, xadd(Di, Dj));
-            if (fuse && d2 < xmul(r_ij, r_ij)) overlap_f64(upper, dx, d2, r_ij);
+            if (fuse && d2 < xmul(r_ij, r_ij)) {
+                PairTerms pt;
+                pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
+                if (upper) {
+                    sU = xadd(sU, pt.U);
+                    sLc = xadd(sLc, pt.Lc);
+                    sdk = xadd(sdk, pt.dk);
+                    sFm = xadd(sFm, pt.Fm);
+                    smax = fmax(smax, pt.U);
+                    ++scount;
+                }
+            }
         }
         return true;
     }
@@ -1187,27 +1172,21 @@ struct UnitPair {
     }
 };
 
-template <int ND, bool MX, bool BUILD>
+template <int ND, bool MX>
 __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blocks) k_cells(DevArrays a) {
     using US = UnitShape<ND>;
     constexpr int NDC = US::ndc, R = US::rows, T = US::threads, NW = US::windows;
     constexpr int CR = NDC == 2 ? 1 : 4;  // row offset of the unit's own row
     DevCtl* ctl = a.ctl;
-    if constexpr (BUILD) {
-        if (build_off(ctl) || !use_cells<ND>(a) || MX != (ctl->pair_fp32 != 0u)) return;
-    } else {
-        const std::uint32_t st = ctl->stopped, ha = ctl->halted, fd = ctl->forces_done, p32 = ctl->pair_fp32;
-        if ((st | ha | fd) != 0u || MX != (p32 != 0u) || !use_cells<ND>(a)) return;
-    }
+    if (build_off(ctl) || !use_cells<ND>(a) || MX != (ctl->pair_fp32 != 0u)) return;
     bind_buffers(a);
     extern __shared__ __align__(16) double u_stage[];  // [US::stage][4]: the staged records
-    std::uint32_t* s_cs = reinterpret_cast<std::uint32_t*>(u_stage + 4 * US::stage);  // [R][US::slice] (build)
+    std::uint32_t* s_cs = reinterpret_cast<std::uint32_t*>(u_stage + 4 * US::stage);  // [R][US::slice]
     // windows, flat index w = 3 r + kind (0 main, 1 wrapped x-1, 2 wrapped x+1):
-    // first particle, length, index of the first record in `recs`
+    // first particle, length, index of the first record in the stage (or in
+    // pos, for a unit that is not staged)
     __shared__ std::uint32_t s_wb[NW], s_wl[NW], s_ws[NW];
-    // the pair kernel's lookup: the non-empty windows sorted by first particle
-    __shared__ std::uint32_t s_lb[NW], s_ll[NW], s_ls[NW];
-    __shared__ std::uint32_t s_qa, s_qb, s_total, s_nl, s_need;
+    __shared__ std::uint32_t s_qa, s_qb, s_total, s_need;
     __shared__ ForceSums s_red[T / 32];
     // the thread's column of the block sums (its particles in order), in
     // shared memory: they change once per particle
@@ -1229,14 +1208,11 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
     for (int d = 0; d < NDC; ++d) nc[d] = ctl->ncell[d];
     const double scale0 = ctl->cell_scale[0];
     const std::uint32_t W = ctl->unit_w, chunks = ctl->unit_chunks, units = ctl->unit_count;
-    const double kap = BUILD ? ctl->build_kappa : ctl->force_kappa;
+    const double kap = ctl->build_kappa;
     const double t_shell = ctl->build_t_shell;
     const float tf = static_cast<float>(t_shell);
-    const bool fuse = BUILD ? (ctl->forces_done != 0u) : true;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) {
-        ctl->nsum_blocks = gridDim.x;
-        if constexpr (!BUILD) ctl->pair_kernel_runs += 1ull;
-    }
+    const bool fuse = ctl->forces_done != 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && fuse) ctl->nsum_blocks = gridDim.x;
     if (threadIdx.x == 0) s_need = 0u;
     const int col = threadIdx.x;
     RCPG_UNROLL
@@ -1265,12 +1241,10 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
             return row * static_cast<std::uint64_t>(nc[0]);
         };
         __syncthreads();  // the previous unit is finished with the shared arrays
-        // 1. cell_start entries
-        if constexpr (BUILD) {
-            for (int r = 0; r < R; ++r) {
-                const std::uint32_t* cs = a.cell_start + rowbase(r) + cl;
-                for (int c = threadIdx.x; c < cnt; c += T) s_cs[r * US::slice + c] = cs[c];
-            }
+        // 1. cell_start entries: the rows' slices and windows
+        for (int r = 0; r < R; ++r) {
+            const std::uint32_t* cs = a.cell_start + rowbase(r) + cl;
+            for (int c = threadIdx.x; c < cnt; c += T) s_cs[r * US::slice + c] = cs[c];
         }
         if (threadIdx.x < R) {
             const int r = threadIdx.x;
@@ -1306,24 +1280,6 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
             s_total = tot;
             if (tot > static_cast<std::uint32_t>(US::stage))  // not staged: records read from pos
                 for (int w = 0; w < NW; ++w) s_ws[w] = s_wb[w];
-            if constexpr (!BUILD) {
-                // non-empty windows sorted by first particle (insertion sort)
-                std::uint32_t n = 0;
-                for (int w = 0; w < NW; ++w) {
-                    if (s_wl[w] == 0u) continue;
-                    std::uint32_t p = n++;
-                    while (p > 0 && s_lb[p - 1] > s_wb[w]) {
-                        s_lb[p] = s_lb[p - 1];
-                        s_ll[p] = s_ll[p - 1];
-                        s_ls[p] = s_ls[p - 1];
-                        --p;
-                    }
-                    s_lb[p] = s_wb[w];
-                    s_ll[p] = s_wl[w];
-                    s_ls[p] = s_ws[w];
-                }
-                s_nl = n;
-            }
         }
         __syncthreads();
         const std::uint32_t total = s_total;
@@ -1347,6 +1303,7 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
                 for (int k = 0; k < 4; ++k) {
                     const std::uint32_t e = e0 + static_cast<std::uint32_t>(k * T);
                     if (e < total) {
+                        if constexpr (NDC == 2) hi[k].y = pack_f32(static_cast<float>(hi[k].x));
                         double2* dst = reinterpret_cast<double2*>(u_stage + 4 * static_cast<std::size_t>(e));
                         dst[0] = lo[k];
                         dst[1] = hi[k];
@@ -1356,121 +1313,93 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
         }
         __syncthreads();
         const std::uint32_t own_b = s_wb[3 * CR], own_s = s_ws[3 * CR];
-        // 3. the unit's particles; records from the stage (shared memory) or,
-        // for a unit whose windows did not fit, from pos
+        // 3. the unit's particles; records from the stage or, for a unit whose
+        // windows did not fit, from pos
         auto particles = [&](auto staged_tag) {
             constexpr bool STG = decltype(staged_tag)::value;
             const double* recs = STG ? static_cast<const double*>(u_stage) : a.pos;  // record s at recs + 4 s
             for (std::uint32_t q = s_qa + threadIdx.x; q < s_qb; q += T) {
                 double xq[ND], D0q;
                 {
-                    const double2* r2 = reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(own_s + (q - own_b)));
+                    const double2* r2 =
+                        reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(own_s + (q - own_b)));
                     unpack_record<ND>(r2[0], r2[1], xq, D0q);
                 }
                 UnitPair<ND, MX> up;
                 up.begin(xq, D0q, kap);
                 std::uint32_t n = 0;
-                if constexpr (BUILD) {
-                    // the binning's cell (same arithmetic and positions), held
-                    // inside the unit so that every slice index stays in range
-                    const int cx = min(max(cell_coord(xq[0], scale0, nc[0]), cx0), cx1 - 1);
-                    const int lo = cx == 0 ? 0 : (cx == nc[0] - 1 ? nc[0] - 2 : cx - 1);
-                    const int hi = cx == 0 ? 2 : (cx == nc[0] - 1 ? nc[0] : cx + 2);
+                // candidate p, record s of `recs`
+                auto test = [&](std::uint32_t p, std::uint32_t s) {
+                    const double2* r2 = reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(s));
+                    const double2 lo = r2[0], hi = r2[1];
+                    double xj[ND], D0j;
+                    unpack_record<ND>(lo, hi, xj, D0j);
+                    float D0jf = 0.0f;
+                    if constexpr (MX) D0jf = (STG && NDC == 2) ? unpack_f32(hi.y) : static_cast<float>(D0j);
+                    if (up.candidate(p > q, xj, D0j, D0jf, bx, ibx, hbf, t_shell, tf, fuse)) {
+                        if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = p;
+                        ++n;
+                    }
+                };
+                // the binning's cell (same arithmetic and positions), held
+                // inside the unit so that every slice index stays in range
+                const int cx = min(max(cell_coord(xq[0], scale0, nc[0]), cx0), cx1 - 1);
+                const int lo = cx == 0 ? 0 : cx - 1, hi = cx == nc[0] - 1 ? nc[0] : cx + 2;
+                // the main ranges: cells lo .. hi-1 of each row
+                if constexpr (NDC == 2) {
+                    std::uint32_t pb[3], ns[3], sb[3];
+                    RCPG_UNROLL
+                    for (int r = 0; r < 3; ++r) {
+                        const std::uint32_t* sl = s_cs + r * US::slice;
+                        pb[r] = sl[lo - cl];
+                        ns[r] = sl[hi - cl] - pb[r];
+                        sb[r] = s_ws[3 * r] + (pb[r] - s_wb[3 * r]);
+                    }
+                    const std::uint32_t c1 = ns[0], c2 = ns[0] + ns[1], tot = c2 + ns[2];
+                    for (std::uint32_t k = 0; k < tot; ++k) {
+                        const bool r0 = k < c1, r1 = k < c2;
+                        const std::uint32_t o = r0 ? k : (r1 ? k - c1 : k - c2);
+                        const std::uint32_t p = (r0 ? pb[0] : (r1 ? pb[1] : pb[2])) + o;
+                        const std::uint32_t s = (r0 ? sb[0] : (r1 ? sb[1] : sb[2])) + o;
+                        if (p != q) test(p, s);
+                    }
+                } else {
                     for (int r = 0; r < R; ++r) {
-                        // up to two contiguous segments of the row in scan order:
-                        // [wrapped x-1 cell] cells lo..hi-1 [wrapped x+1 cell]
                         const std::uint32_t* sl = s_cs + r * US::slice;
                         const std::uint32_t pb = sl[lo - cl], pe = sl[hi - cl];
-                        std::uint32_t seg_p[2], seg_n[2], seg_s[2];
-                        const int wk = cx == 0 ? 1 : 2;  // wrapped window used, if any
-                        const std::uint32_t wb = s_wb[3 * r + wk], wl = s_wl[3 * r + wk], ws = s_ws[3 * r + wk];
-                        const std::uint32_t mp = pb, mn = pe - pb, ms = s_ws[3 * r] + (pb - s_wb[3 * r]);
-                        const bool wrap = (cx == 0) | (cx == nc[0] - 1);
-                        if (cx == 0) {
-                            seg_p[0] = wb; seg_n[0] = wl; seg_s[0] = ws;
-                            seg_p[1] = mp; seg_n[1] = mn; seg_s[1] = ms;
-                        } else {
-                            seg_p[0] = mp; seg_n[0] = mn; seg_s[0] = ms;
-                            seg_p[1] = wb; seg_n[1] = wrap ? wl : 0u; seg_s[1] = ws;
-                        }
-                        const std::uint32_t tot = seg_n[0] + seg_n[1];
-                        for (std::uint32_t k = 0; k < tot; ++k) {
-                            const bool first = k < seg_n[0];
-                            const std::uint32_t o = first ? k : k - seg_n[0];
-                            const std::uint32_t p = (first ? seg_p[0] : seg_p[1]) + o;
-                            const std::uint32_t sidx = (first ? seg_s[0] : seg_s[1]) + o;
-                            if (p == q) continue;
-                            const double2* r2 = reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(sidx));
-                            double xj[ND], D0j;
-                            unpack_record<ND>(r2[0], r2[1], xj, D0j);
-                            if (up.candidate(p > q, xj, D0j, bx, ibx, hbf, t_shell, tf, fuse)) {
-                                if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = p;
-                                ++n;
-                            }
-                        }
-                    }
-                    // the reference's capacity check counts the partners after q in
-                    // its own order; a row that fits the capacity in full needs no count
-                    const std::uint32_t cap = a.caps[q];
-                    if (n > cap && n <= S) {
-                        const std::uint32_t rq = a.ref_rank[q];
-                        std::uint32_t n_half = 0;
-                        for (std::uint32_t k = 0; k < n; ++k)
-                            n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
-                        if (n_half > cap) report_cap_error(ctl, rq, cap);
-                    }
-                    need = max(need, n);
-                    if (n > S) {
-                        a.nbr_cnt[q] = 0u;  // overflow: empty row, rebuilt after the capacity grows
-                        overflow = true;
-                        continue;
-                    }
-                    a.nbr_cnt[q] = n;
-                    if (!fuse) continue;
-                } else {
-                    n = min(a.nbr_cnt[q], S);
-                    const std::uint32_t nl = STG ? s_nl : 0u;
-                    // chunks of kChunk entries: the row ids, then the windows and
-                    // records of all of them, before any pair arithmetic (the
-                    // pairs are still summed in row order); staged records are a
-                    // shared-memory read away, so two in flight cover them
-                    constexpr std::uint32_t kChunk = STG ? 2 : 4;
-                    for (std::uint32_t k0 = 0; k0 < n; k0 += kChunk) {
-                        std::uint32_t jj[kChunk];
-                        RCPG_UNROLL
-                        for (std::uint32_t v = 0; v < kChunk; ++v)
-                            jj[v] = (k0 + v < n) ? __ldg(a.nbr + static_cast<std::uint64_t>(k0 + v) * N + q)
-                                                 : 0xFFFFFFFFu;
-                        double xj[kChunk][ND], D0j[kChunk];
-                        RCPG_UNROLL
-                        for (std::uint32_t v = 0; v < kChunk; ++v) {
-                            const std::uint32_t j = jj[v];
-                            if (j >= N) continue;  // past the row's end
-                            double2 rl, rh;
-                            if constexpr (STG) {
-                                // the last window starting at or before j: windows
-                                // below it, counted without branches
-                                std::uint32_t w = 0;
-                                for (std::uint32_t k = 1; k < nl; ++k) w += j >= s_lb[k] ? 1u : 0u;
-                                const std::uint32_t off = j - s_lb[w];
-                                if (nl && off < s_ll[w]) {
-                                    const double2* r2 = reinterpret_cast<const double2*>(
-                                        recs + 4 * static_cast<std::size_t>(s_ls[w] + off));
-                                    rl = r2[0];
-                                    rh = r2[1];
-                                } else {
-                                    ld_record(a.pos + 4 * static_cast<std::uint64_t>(j), rl, rh);
-                                }
-                            } else {
-                                ld_record(a.pos + 4 * static_cast<std::uint64_t>(j), rl, rh);
-                            }
-                            unpack_record<ND>(rl, rh, xj[v], D0j[v]);
-                        }
-                        RCPG_UNROLL
-                        for (std::uint32_t v = 0; v < kChunk; ++v)
-                            if (jj[v] < N) up.row_partner(jj[v] > q, xj[v], D0j[v], bx, ibx, hbf);
+                        const std::uint32_t sb = s_ws[3 * r] + (pb - s_wb[3 * r]);
+                        for (std::uint32_t p = pb; p < pe; ++p)
+                            if (p != q) test(p, sb + (p - pb));
                     }
                 }
+                // the wrapped cells: the x-1 cell of a particle at x = 0, the
+                // x+1 cell of one at x = nc0-1
+                if (cx == 0 || cx == nc[0] - 1) {
+                    const int wk = cx == 0 ? 1 : 2;
+                    for (int r = 0; r < R; ++r) {
+                        const std::uint32_t wb = s_wb[3 * r + wk], wl = s_wl[3 * r + wk], ws = s_ws[3 * r + wk];
+                        for (std::uint32_t o = 0; o < wl; ++o)
+                            if (wb + o != q) test(wb + o, ws + o);
+                    }
+                }
+                // the reference's capacity check counts the partners after q in
+                // its own order; a row that fits the capacity in full needs no count
+                const std::uint32_t cap = a.caps[q];
+                if (n > cap && n <= S) {
+                    const std::uint32_t rq = a.ref_rank[q];
+                    std::uint32_t n_half = 0;
+                    for (std::uint32_t k = 0; k < n; ++k)
+                        n_half += a.ref_rank[a.nbr[static_cast<std::uint64_t>(k) * N + q]] > rq;
+                    if (n_half > cap) report_cap_error(ctl, rq, cap);
+                }
+                need = max(need, n);
+                if (n > S) {
+                    a.nbr_cnt[q] = 0u;  // overflow: empty row, rebuilt after the capacity grows
+                    overflow = true;
+                    continue;
+                }
+                a.nbr_cnt[q] = n;
+                if (!fuse) continue;
                 double f[ND];
                 up.force(f);
                 s_acc[0][col] = xadd(s_acc[0][col], static_cast<double>(up.sU));
@@ -1494,14 +1423,12 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
         if (staged) particles(std::true_type{});
         else particles(std::false_type{});
     }
-    if constexpr (BUILD) {
-        if (overflow && fuse) ctl->forces_done = 0u;
-        // block maximum of the row lengths, one atomic per block
-        RCPG_UNROLL
-        for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_xor_sync(0xffffffffu, need, o));
-        __syncthreads();
-        if ((threadIdx.x & 31) == 0 && need) atomicMax(&s_need, need);
-    }
+    if (overflow && fuse) ctl->forces_done = 0u;
+    // block maximum of the row lengths, one atomic per block
+    RCPG_UNROLL
+    for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_xor_sync(0xffffffffu, need, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && need) atomicMax(&s_need, need);
     if (fuse) {
         ForceSums fs;
         sums_zero(fs);
@@ -1519,18 +1446,15 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
     } else {
         __syncthreads();
     }
-    if constexpr (BUILD) {
-        if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
-    }
+    if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
 }
 
-// dynamic shared memory of k_cells<ND, *, BUILD>: the stage, and the build's
-// cell_start slices
-template <int ND, bool BUILD>
+// dynamic shared memory of k_cells<ND, *>: the stage and the rows' cell_start slices
+template <int ND>
 constexpr std::size_t cells_smem_bytes() {
     using US = UnitShape<ND>;
     return static_cast<std::size_t>(US::stage) * 4 * sizeof(double) +
-           (BUILD ? static_cast<std::size_t>(US::rows) * US::slice * sizeof(std::uint32_t) : 0);
+           static_cast<std::size_t>(US::rows) * US::slice * sizeof(std::uint32_t);
 }
 
 // ===========================================================================
@@ -1550,9 +1474,6 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
         // one round trip for every flag of the early exit
         const std::uint32_t st = ctl->stopped, ha = ctl->halted, fd = ctl->forces_done, p32 = ctl->pair_fp32;
         if ((st | ha | fd) != 0u || MIXED != (!EXACT && p32 != 0u)) return;
-    }
-    if constexpr (!EXACT) {
-        if (a.permute && use_cells<ND>(a)) return;  // the cell-unit pair kernel takes the step
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.ctl->nsum_blocks = gridDim.x;
@@ -2275,36 +2196,33 @@ void adam_nd(const DevArrays& a, int do_adam, int do_refresh, cudaStream_t st) {
 
 // persistent force grid: at most the blocks resident at once (the block-sum
 // buffers hold at least force_blocks(N) entries)
-// persistent grid of the cell-unit kernels: the blocks resident at once (at
+// persistent grid of the cell-unit search: the blocks resident at once (at
 // most 4096, the engine's block-sum entries)
-template <int ND, bool MX, bool BUILD>
+template <int ND, bool MX>
 void launch_cells_variant(const DevArrays& a, cudaStream_t st) {
     if constexpr (ND <= 3) {
         int dev = 0;
         cudaGetDevice(&dev);
-        constexpr std::size_t smem = cells_smem_bytes<ND, BUILD>();
+        constexpr std::size_t smem = cells_smem_bytes<ND>();
         constexpr int T = UnitShape<ND>::threads;
         static int grid[64] = {};
         if (dev >= 0 && dev < 64 && grid[dev] == 0) {
-            cudaFuncSetAttribute(k_cells<ND, MX, BUILD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem));
+            cudaFuncSetAttribute(k_cells<ND, MX>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
             int sms = 148, per_sm = 1;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cells<ND, MX, BUILD>, T, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cells<ND, MX>, T, smem);
             const int gr = sms * (per_sm > 0 ? per_sm : 1);
             grid[dev] = gr < 4096 ? gr : 4096;
         }
         const unsigned g = (dev >= 0 && dev < 64) ? static_cast<unsigned>(grid[dev]) : 148u;
-        k_cells<ND, MX, BUILD><<<g, T, smem, st>>>(a);
+        k_cells<ND, MX><<<g, T, smem, st>>>(a);
     }
 }
 
-// The pair kernel: k_forces over the rows and, with cell-order storage (graph
-// mode, ndim <= 3), the cell-unit pair kernel; the one that does not apply to
-// the step returns at once.
+// persistent force grid: at most the blocks resident at once (the block-sum
+// buffers hold at least force_blocks(N) entries)
 template <int ND, bool EXACT, bool MIXED>
 void forces_nd(const DevArrays& a, cudaStream_t st) {
-    if (!EXACT && a.permute && ND <= 3 && a.N >= kTiledMinN) launch_cells_variant<ND, MIXED, false>(a, st);
     const unsigned need = force_blocks(a.N), g = resident_grid<k_forces<ND, EXACT, MIXED>>(kForceBlock);
     k_forces<ND, EXACT, MIXED><<<need < g ? need : g, kForceBlock, 0, st>>>(a);
 }
@@ -2332,8 +2250,8 @@ void launch_tiled(const DevArrays& a, cudaStream_t st) {
 // not match the step returns at once)
 template <int ND>
 void launch_cells(const DevArrays& a, cudaStream_t st) {
-    launch_cells_variant<ND, false, true>(a, st);
-    if (a.mixed) launch_cells_variant<ND, true, true>(a, st);
+    launch_cells_variant<ND, false>(a, st);
+    if (a.mixed) launch_cells_variant<ND, true>(a, st);
 }
 
 // e0 / e1 (optional): events recorded around the search kernels only

@@ -16,8 +16,8 @@ tests/golden/make_large_golden.py from the compiled reference):
   precision its rows are a superset of the FP64 shell (every extra pair lies
   within the 1e-5 relative widening) and its forces are within 1e-4 of the
   largest FP64 force;
-* the cell-unit pair kernel of the steps without a build gives the fused
-  build's forces on the same rows bit for bit.
+* the pair kernel of the steps without a build gives the fused build's forces
+  on the same rows bit for bit, FP64 and mixed.
 
 The power-law case (size ratio 10) has several size classes and takes the warp
 search at this N; it pins that path at large N the same way.
@@ -197,10 +197,10 @@ def test_scan_build_fp64_fused_forces(cuda_device, native, golden, case):
 
 @pytest.mark.parametrize("case", [c for c in CASES if FUSED[c]])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_cell_pair_kernel_equals_fused_build(cuda_device, native, golden, case, precision):
-    """The pair kernel of the steps without a build (cell units: row entries
-    looked up in the staged windows) sums the same rows in the same order as
-    the build that fused the forces: identical forces, FP64 and mixed."""
+def test_pair_kernel_equals_fused_build(cuda_device, native, golden, case, precision):
+    """The pair kernel of the steps without a build (k_forces on the cell-order
+    rows) sums the same rows in the same order as the cell-unit build that
+    fused the forces: identical forces, FP64 and mixed."""
     g = golden(f"large_{case}.npz")
     _, cnt, _, F, sc, fused = _scan_build(native, g, precision)
     _, cnt2, _, F2, sc2, fused2 = _scan_build(native, g, precision + 2)
