@@ -131,13 +131,12 @@ struct UnitShape {
     static constexpr int ndc = ND <= 3 ? ND : 3;
     static constexpr int rows = ndc == 2 ? 3 : 9;        // neighbour rows of a unit
     static constexpr int threads = ndc == 2 ? 128 : 64;  // block size
-    static constexpr int target = ndc == 2 ? 96 : 48;    // particles per unit
-    static constexpr int stage = ndc == 2 ? 512 : 640;   // staged records (32 + 16 bytes each)
+    static constexpr int target = ndc == 2 ? 112 : 56;   // particles per unit
+    static constexpr int stage = ndc == 2 ? 640 : 768;   // staged records (32 bytes each)
     static constexpr int maxw = ndc == 2 ? 256 : 128;    // cells per unit at most
-    static constexpr int slice = maxw + 3;               // cell_start entries per row
+    static constexpr int slice = maxw + 3;               // cell_start entries per row (build)
     static constexpr int windows = 3 * rows;             // main, wrapped x-1, wrapped x+1 per row
-    static constexpr int queue = 32;                     // prefilter passes queued per thread
-    static constexpr int min_blocks = 5;                 // resident blocks per SM (register budget)
+    static constexpr int min_blocks = 6;                 // resident blocks per SM (register budget)
 };
 
 // Cells per unit for a build with `cells` cells in a grid of nc0 cells per row:
@@ -1108,6 +1107,14 @@ __device__ __forceinline__ void unpack_record(const double2& lo, const double2& 
     }
 }
 
+// FP32 diameter kept in the spare slot of a staged 2-D record
+__device__ __forceinline__ double pack_f32(float f) {
+    return __longlong_as_double(static_cast<long long>(__float_as_uint(f)));
+}
+__device__ __forceinline__ float unpack_f32(double d) {
+    return __uint_as_float(static_cast<unsigned>(__double_as_longlong(d)));
+}
+
 // One particle's candidate tests and its pair sums in the arithmetic of
 // k_forces: FP32 (MX) or FP64 accumulators for the pair scalars, the force in
 // FP32 (MX) or FP64.
@@ -1197,13 +1204,8 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
     DevCtl* ctl = a.ctl;
     if (build_off(ctl) || !use_cells<ND>(a) || MX != (ctl->pair_fp32 != 0u)) return;
     bind_buffers(a);
-    // dynamic shared memory: the staged FP64 records [US::stage][4], their FP32
-    // copies (x, y, [z,] D0) for the prefilter, the rows' cell_start slices
-    // [R][US::slice] and the per-thread queues of prefilter passes [queue][T]
-    extern __shared__ __align__(16) double u_stage[];
-    float4* u_stagef = reinterpret_cast<float4*>(u_stage + 4 * US::stage);
-    std::uint32_t* s_cs = reinterpret_cast<std::uint32_t*>(u_stagef + US::stage);
-    std::uint16_t* s_q = reinterpret_cast<std::uint16_t*>(s_cs + R * US::slice);
+    extern __shared__ __align__(16) double u_stage[];  // [US::stage][4]: the staged records
+    std::uint32_t* s_cs = reinterpret_cast<std::uint32_t*>(u_stage + 4 * US::stage);  // [R][US::slice]
     // windows, flat index w = 3 r + kind (0 main, 1 wrapped x-1, 2 wrapped x+1):
     // first particle, length, index of the first record in the stage (or in
     // pos, for a unit that is not staged)
@@ -1225,19 +1227,6 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
         ibx[d] = g.inv_box[d];
         hbf[d] = static_cast<float>(0.5 * g.box[d]);
     }
-    // the prefilter's box in FP32 and its absolute widening: FP32 coordinates
-    // of positions within the box are within 2^-24 box of the FP64 ones, so a
-    // distance formed from them (minimum image included) is within 2^-21 of
-    // the largest box side of the FP64 one; 2^-19 leaves a factor 4 (positions
-    // somewhat outside the box)
-    float bxf[NDC];
-    float bmax = 0.0f;
-    RCPG_UNROLL
-    for (int d = 0; d < NDC; ++d) {
-        bxf[d] = static_cast<float>(g.box[d]);
-        bmax = fmaxf(bmax, bxf[d]);
-    }
-    const float eabs = ldexpf(bmax, -19);
     int nc[NDC];
     RCPG_UNROLL
     for (int d = 0; d < NDC; ++d) nc[d] = ctl->ncell[d];
@@ -1338,13 +1327,10 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
                 for (int k = 0; k < 4; ++k) {
                     const std::uint32_t e = e0 + static_cast<std::uint32_t>(k * T);
                     if (e < total) {
+                        if constexpr (NDC == 2) hi[k].y = pack_f32(static_cast<float>(hi[k].x));
                         double2* dst = reinterpret_cast<double2*>(u_stage + 4 * static_cast<std::size_t>(e));
                         dst[0] = lo[k];
                         dst[1] = hi[k];
-                        u_stagef[e] = NDC == 2 ? make_float4(static_cast<float>(lo[k].x), static_cast<float>(lo[k].y),
-                                                             static_cast<float>(hi[k].x), 0.0f)
-                                               : make_float4(static_cast<float>(lo[k].x), static_cast<float>(lo[k].y),
-                                                             static_cast<float>(hi[k].x), static_cast<float>(hi[k].y));
                     }
                 }
             }
@@ -1366,16 +1352,14 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
                 UnitPair<ND, MX> up;
                 up.begin(xq, D0q, kap);
                 std::uint32_t n = 0;
-                // the exact test of candidate p (record s of `recs`)
+                // candidate p, record s of `recs`
                 auto test = [&](std::uint32_t p, std::uint32_t s) {
                     const double2* r2 = reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(s));
+                    const double2 lo = r2[0], hi = r2[1];
                     double xj[ND], D0j;
-                    unpack_record<ND>(r2[0], r2[1], xj, D0j);
+                    unpack_record<ND>(lo, hi, xj, D0j);
                     float D0jf = 0.0f;
-                    if constexpr (MX) {
-                        if constexpr (STG) D0jf = NDC == 2 ? u_stagef[s].z : u_stagef[s].w;
-                        else D0jf = static_cast<float>(D0j);
-                    }
+                    if constexpr (MX) D0jf = (STG && NDC == 2) ? unpack_f32(hi.y) : static_cast<float>(D0j);
                     if (up.candidate(p > q, xj, D0j, D0jf, bx, ibx, hbf, t_shell, tf, fuse)) {
                         if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = p;
                         ++n;
@@ -1385,94 +1369,35 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
                 // inside the unit so that every slice index stays in range
                 const int cx = min(max(cell_coord(xq[0], scale0, nc[0]), cx0), cx1 - 1);
                 const int lo = cx == 0 ? 0 : cx - 1, hi = cx == nc[0] - 1 ? nc[0] : cx + 2;
-                if constexpr (STG) {
-                    // FP32 prefilter over the staged copies: a candidate whose
-                    // FP32 distance is within the widened cutoff joins this
-                    // thread's queue (stage indices in scan order); the exact
-                    // test runs over the queue when it is full and at the end
-                    float xif[NDC];
+                // the main ranges: cells lo .. hi-1 of each row
+                if constexpr (NDC == 2) {
+                    std::uint32_t pb[3], ns[3], sb[3];
                     RCPG_UNROLL
-                    for (int d = 0; d < NDC; ++d) xif[d] = static_cast<float>(xq[d]);
-                    const float rc_a = 0.5f * up.kapf * 1.00002f;
-                    const float rc_b = __fmaf_rn(0.5f * up.Dif + tf, 1.00002f, eabs);
-                    const std::uint32_t sq = own_s + (q - own_b);
-                    std::uint16_t* myq = s_q + col;
-                    std::uint32_t nq = 0;
-                    auto pre = [&](std::uint32_t s) -> bool {
-                        const float4 c = u_stagef[s];
-                        float d2 = 0.0f;
-                        RCPG_UNROLL
-                        for (int d = 0; d < NDC; ++d) {
-                            float v = (d == 0 ? c.x : (d == 1 ? c.y : c.z)) - xif[d];
-                            v = v > hbf[d] ? v - bxf[d] : (v < -hbf[d] ? v + bxf[d] : v);
-                            d2 = __fmaf_rn(v, v, d2);
-                        }
-                        const float rc = __fmaf_rn(NDC == 2 ? c.z : c.w, rc_a, rc_b);
-                        return d2 < rc * rc;
-                    };
-                    if constexpr (NDC == 2) {
-                        // the three rows' main ranges as one sequence
-                        std::uint32_t pb[3], sb[3], ns[3];
-                        RCPG_UNROLL
-                        for (int r = 0; r < 3; ++r) {
-                            const std::uint32_t* sl = s_cs + r * US::slice;
-                            pb[r] = sl[lo - cl];
-                            ns[r] = sl[hi - cl] - pb[r];
-                            sb[r] = s_ws[3 * r] + (pb[r] - s_wb[3 * r]);
-                        }
-                        // stage index -> particle: the rows' stage ranges ascend
-                        auto drain = [&]() {
-                            for (std::uint32_t k = 0; k < nq; ++k) {
-                                const std::uint32_t st = myq[k * T];
-                                const bool in0 = st < sb[1], in1 = st < sb[2];
-                                const std::uint32_t p = (in0 ? pb[0] : (in1 ? pb[1] : pb[2])) +
-                                                        (st - (in0 ? sb[0] : (in1 ? sb[1] : sb[2])));
-                                test(p, st);
-                            }
-                            nq = 0;
-                        };
-                        const std::uint32_t c1 = ns[0], c2 = ns[0] + ns[1], tot = c2 + ns[2];
-                        for (std::uint32_t k = 0; k < tot; ++k) {
-                            const bool r0 = k < c1, r1 = k < c2;
-                            const std::uint32_t st = (r0 ? sb[0] : (r1 ? sb[1] - c1 : sb[2] - c2)) + k;
-                            if (st != sq && pre(st)) {
-                                myq[nq * T] = static_cast<std::uint16_t>(st);
-                                if (++nq == static_cast<std::uint32_t>(US::queue)) drain();
-                            }
-                        }
-                        drain();
-                    } else {
-                        for (int r = 0; r < R; ++r) {
-                            const std::uint32_t* sl = s_cs + r * US::slice;
-                            const std::uint32_t pb = sl[lo - cl], pe = sl[hi - cl];
-                            const std::uint32_t sb = s_ws[3 * r] + (pb - s_wb[3 * r]);
-                            auto drain = [&]() {
-                                for (std::uint32_t k = 0; k < nq; ++k) {
-                                    const std::uint32_t st = myq[k * T];
-                                    test(pb + (st - sb), st);
-                                }
-                                nq = 0;
-                            };
-                            for (std::uint32_t st = sb; st < sb + (pe - pb); ++st) {
-                                if (st != sq && pre(st)) {
-                                    myq[nq * T] = static_cast<std::uint16_t>(st);
-                                    if (++nq == static_cast<std::uint32_t>(US::queue)) drain();
-                                }
-                            }
-                            drain();
-                        }
+                    for (int r = 0; r < 3; ++r) {
+                        const std::uint32_t* sl = s_cs + r * US::slice;
+                        pb[r] = sl[lo - cl];
+                        ns[r] = sl[hi - cl] - pb[r];
+                        sb[r] = s_ws[3 * r] + (pb[r] - s_wb[3 * r]);
+                    }
+                    const std::uint32_t c1 = ns[0], c2 = ns[0] + ns[1], tot = c2 + ns[2];
+                    for (std::uint32_t k = 0; k < tot; ++k) {
+                        const bool r0 = k < c1, r1 = k < c2;
+                        const std::uint32_t o = r0 ? k : (r1 ? k - c1 : k - c2);
+                        const std::uint32_t p = (r0 ? pb[0] : (r1 ? pb[1] : pb[2])) + o;
+                        const std::uint32_t s = (r0 ? sb[0] : (r1 ? sb[1] : sb[2])) + o;
+                        if (p != q) test(p, s);
                     }
                 } else {
-                    // records in pos: every candidate takes the exact test
                     for (int r = 0; r < R; ++r) {
                         const std::uint32_t* sl = s_cs + r * US::slice;
                         const std::uint32_t pb = sl[lo - cl], pe = sl[hi - cl];
+                        const std::uint32_t sb = s_ws[3 * r] + (pb - s_wb[3 * r]);
                         for (std::uint32_t p = pb; p < pe; ++p)
-                            if (p != q) test(p, p);
+                            if (p != q) test(p, sb + (p - pb));
                     }
                 }
                 // the wrapped cells: the x-1 cell of a particle at x = 0, the
-                // x+1 cell of one at x = nc0-1 (exact tests)
+                // x+1 cell of one at x = nc0-1
                 if (cx == 0 || cx == nc[0] - 1) {
                     const int wk = cx == 0 ? 1 : 2;
                     for (int r = 0; r < R; ++r) {
@@ -1548,14 +1473,12 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
     if (threadIdx.x == 0 && s_need) atomicMax(&ctl->row_need, s_need);
 }
 
-// dynamic shared memory of k_cells<ND, *>: the stage (FP64 records and FP32
-// copies), the rows' cell_start slices and the prefilter queues
+// dynamic shared memory of k_cells<ND, *>: the stage and the rows' cell_start slices
 template <int ND>
 constexpr std::size_t cells_smem_bytes() {
     using US = UnitShape<ND>;
-    return static_cast<std::size_t>(US::stage) * (4 * sizeof(double) + sizeof(float4)) +
-           static_cast<std::size_t>(US::rows) * US::slice * sizeof(std::uint32_t) +
-           static_cast<std::size_t>(US::queue) * US::threads * sizeof(std::uint16_t);
+    return static_cast<std::size_t>(US::stage) * 4 * sizeof(double) +
+           static_cast<std::size_t>(US::rows) * US::slice * sizeof(std::uint32_t);
 }
 
 // ===========================================================================
