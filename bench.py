@@ -41,10 +41,10 @@ PEAKS = REPO / "MEASURED_PEAKS.json"
 # (profiles/k_forces_bidisperse2d_n3e5_mixed.md: 24.2 MB for 20.1 MB at N = 300k);
 # the N = 1M launch is too large to capture with the full metric set
 FORCES_TRAFFIC_PER_ALG_BYTE = 24.2 / 20.1
-# the same for the tiled build with fused forces
-# (profiles/k_build_search_tiled_bidisperse2d_n3e5_mixed.md: 14.9 MB for 24.8 MB at N = 300k; its
-# inputs were just written by the binning kernels and are partly still in L2)
-BUILD_TRAFFIC_PER_ALG_BYTE = 14.9 / 24.8
+# the same for the cell-unit build with fused forces, k_cells<2, mixed>
+# (profiles/k_cells_bidisperse2d_n3e5_mixed.md: 12.3 MB for 22.7 MB at N = 300k; the rows and
+# forces it writes are still in L2 when the launch ends)
+BUILD_TRAFFIC_PER_ALG_BYTE = 12.3 / 22.7
 
 
 def workload_name(n: int) -> str:
@@ -553,7 +553,7 @@ def run_single(args) -> int:
         "late_phase": late or None,
         # the step's dominant kernel in this window: every step rebuilds its
         # rows, and the tiled build computes that step's forces in the same pass
-        "roofline": roofline_of(bprof, peak, peak_kind, "k_build_search_tiled (neighbour build + fused forces)",
+        "roofline": roofline_of(bprof, peak, peak_kind, "k_cells (cell-unit neighbour build + fused forces)",
                                 BUILD_TRAFFIC_PER_ALG_BYTE),
         # the pair kernel of the steps without a rebuild (the reference's 81 % kernel),
         # on the state after the growth rung
