@@ -217,6 +217,13 @@ def run_batch_workload(args) -> int:
     t2 = time.perf_counter()
     ps = sum(len(i["positions"]) * r["steps"] for (i, _), r in zip(items, res))
     steps = [r["steps"] for r in res]
+    if args.save_training:
+        # the plain runs as warm-start training data (descriptors with log N, targets, seeds)
+        from rcpgenerator_b200 import warmstart as W
+        X = np.stack([W.descriptors(i["diameters"], np.asarray(i["positions"]).shape[1], c["walls"], True)
+                      for i, c in items])
+        Y = np.stack([W.targets(r) for r in res])
+        np.savez_compressed(args.save_training, X=X, Y=Y, seeds=np.asarray(seeds, dtype=np.int64))
     value = len(items) / (t2 - t1) * 3600.0
     single_value = len(single) / (t1 - t0) * 3600.0
     warm = None
@@ -656,6 +663,8 @@ def main() -> int:
                     help="batch: generator seeds k * stride (0: 4096 // count, a stratified sample of "
                          "seeds 0..4095)")
     ap.add_argument("--batch-single", type=int, default=8, help="packings timed one at a time")
+    ap.add_argument("--save-training", default=None,
+                    help="batch workload: write the plain runs' warm-start descriptors, targets and seeds (.npz)")
     ap.add_argument("--concurrency", type=int, default=0,
                     help="-1: persistent batch kernel; 0: persistent for small packings + 32 streams; k: k streams")
     ap.add_argument("--cpu-cap-steps", type=int, default=300)

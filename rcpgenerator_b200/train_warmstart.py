@@ -4,7 +4,9 @@
 
 Generates ``count`` plain packings with the batch engine (draw_packing: N
 log-uniform on [--n-min, --n-max], Ndim in {2, 3, 4}, mono / bidisperse /
-log-normal diameters), trains the network with the project's BF16 kernels,
+log-normal diameters) or takes them from ``--data`` (for instance the plain
+runs of ``bench.py --workload batch --save-training``, leaving out every
+``--exclude-stride``-th seed), trains the network with the project's BF16 kernels,
 evaluates it on held-out packings (draw_evaluation_packing: 3-D, N = --eval-n)
 plain against warm-started, and prints one JSON line with the figures.
 """
@@ -39,20 +41,31 @@ def main(argv=None) -> dict:
     ap.add_argument("--eval-n", type=int, default=100_000)
     ap.add_argument("--eval-concurrency", type=int, default=8)
     ap.add_argument("--eval-margins", default="", help="extra comma-separated margins to evaluate")
+    ap.add_argument("--eval-plain-precision", default=None, choices=("f64", "mixed"),
+                    help="pair precision of the evaluation's plain runs (default: --pair-precision)")
+    ap.add_argument("--exclude-stride", type=int, default=0,
+                    help="with --data holding seeds: leave out of training every packing whose seed is a "
+                         "multiple of this stride (held out for the batch benchmark's sample)")
     ap.add_argument("--eval-only", action="store_true", help="evaluate the model file --out without training")
     a = ap.parse_args(argv)
     opts = {"pair_precision": a.pair_precision}
+    plain_opts = {"pair_precision": a.eval_plain_precision or a.pair_precision}
     if a.eval_only:
         ws = W.WarmStart.load(a.out)
         items = [W.draw_evaluation_packing(s, a.eval_n) for s in range(a.eval_count)]
-        out = {"model": str(a.out), "eval": W.evaluate(ws, items, opts, a.eval_concurrency)}
+        out = {"model": str(a.out), "eval": W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)}
         out["eval"]["N"] = a.eval_n
         print(json.dumps(out))
         return out
     t0 = time.perf_counter()
+    held = 0
     if a.data:
         z = np.load(a.data)
         X, Y = z["X"], z["Y"]
+        if a.exclude_stride > 0 and "seeds" in z.files:
+            keep = (z["seeds"] % a.exclude_stride) != 0
+            held = int((~keep).sum())
+            X, Y = X[keep], Y[keep]
     else:
         X, Y = W.generate_training_set(a.count, a.seed0, (a.n_min, a.n_max), opts)
         if a.save_data:
@@ -60,22 +73,23 @@ def main(argv=None) -> dict:
     t1 = time.perf_counter()
     ws = W.WarmStart.fit(X, Y, epochs=a.epochs, batch=a.batch, lr=a.lr, eps=a.eps, margin=a.margin)
     t2 = time.perf_counter()
-    ws.meta.update(data=f"{len(X)} plain packings, N log-uniform [{a.n_min}, {a.n_max}], seeds {a.seed0}..",
+    ws.meta.update(data=(f"{len(X)} plain packings of {a.data}" if a.data else
+                         f"{len(X)} plain packings, N log-uniform [{a.n_min}, {a.n_max}], seeds {a.seed0}.."),
                    pair_precision=a.pair_precision)
     ws.save(a.out)
     # fit on the training set (phi_J)
     P = ws.predict(X)
-    out = {"train_packings": int(len(X)), "generate_s": t1 - t0, "train_s": t2 - t1,
+    out = {"train_packings": int(len(X)), "held_out_of_data": held, "generate_s": t1 - t0, "train_s": t2 - t1,
            "train_loss_first": ws.meta["train_loss"][0], "train_loss_last": ws.meta["train_loss"][-1],
            "train_phi_mae": float(np.abs(P[:, 0] - Y[:, 0]).mean()),
            "train_phi_std": float(Y[:, 0].std())}
     if a.eval_count > 0:
         items = [W.draw_evaluation_packing(s, a.eval_n) for s in range(a.eval_count)]
-        out["eval"] = W.evaluate(ws, items, opts, a.eval_concurrency)
+        out["eval"] = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)
         out["eval"]["N"] = a.eval_n
         for m in [float(x) for x in a.eval_margins.split(",") if x]:
             ws.margin = m
-            out[f"eval_margin_{m:g}"] = W.evaluate(ws, items, opts, a.eval_concurrency)
+            out[f"eval_margin_{m:g}"] = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)
         ws.margin = a.margin
     print(json.dumps(out))
     return out

@@ -360,14 +360,19 @@ def generate_training_set(count: int, seed0: int = 0, n_range=(64, 16384), optio
     return np.asarray(X), np.asarray(Y)
 
 
-def evaluate(ws: WarmStart, items: list, options: dict | None = None, concurrency: int = 0) -> dict:
+def evaluate(ws: WarmStart, items: list, options: dict | None = None, concurrency: int = 0,
+             plain_options: dict | None = None) -> dict:
     """Runs ``items`` plain and warm-started (same seeds, same batch call
     shape) and compares: packings/hour of each (host wall clock around the
-    batch call), steps, phi_J per packing, and the network's phi_J error."""
+    batch call), steps, phi_J per packing, and the network's phi_J error.
+    ``plain_options`` (default: ``options``) are the plain runs' options, e.g.
+    FP64 pair arithmetic for the plain method against mixed-precision
+    warm-started runs."""
     import time
 
+    plain_opts = options if plain_options is None else plain_options
     t0 = time.perf_counter()
-    plain = run_packing_batch(items, options, concurrency)
+    plain = run_packing_batch(items, plain_opts, concurrency)
     t1 = time.perf_counter()
     warm, phi_pred = ws.run_batch(items, options, concurrency)
     t2 = time.perf_counter()
@@ -393,6 +398,9 @@ def evaluate(ws: WarmStart, items: list, options: dict | None = None, concurrenc
         "delta_phi_abs_mean": float(np.abs(wj - pj).mean()),
         "phi_pred_mae": float(np.abs(phi_pred - pj).mean()),
         "phi_pred_bias": float((phi_pred - pj).mean()),
+        "delta_phi_abs_max": float(np.abs(wj - pj).max()),
         "max_overlap_warm": float(max(r["max_min_dist"] for r in warm)),
         "max_overlap_plain": float(max(r["max_min_dist"] for r in plain)),
+        "plain_pair_precision": str((plain_opts or {}).get("pair_precision", "f64")),
+        "warm_pair_precision": str((options or {}).get("pair_precision", "f64")),
     }
