@@ -1143,50 +1143,70 @@ struct UnitPair {
         scount = 0;
     }
 
-    // Candidate (xj, D0j; D0jf = its FP32 diameter): the shell test; on a pass
-    // the pair terms when `fuse` and the pair overlaps, the scalars once per
-    // pair (from the lower index). Returns whether the candidate is a partner.
+    // The tests of one candidate (xj, D0j; D0jf = its FP32 diameter), kept
+    // for commit(): the displacement, its square and the pair's r_ij; pass =
+    // the shell test, ov = overlapping (with `fuse`; an overlapping pair also
+    // passes the shell test). Two candidates are probed side by side and
+    // committed in scan order.
+    struct Probe {
+        using T = std::conditional_t<MX, float, double>;
+        T dx[ND], d2, r;
+        bool pass, ov;
+    };
+    __device__ __forceinline__ void probe(Probe& pr, const double* xj, double D0j, float D0jf, const double* bx,
+                                          const double* ibx, const float* hbf, double t_shell, float tf,
+                                          bool fuse) const {
+        if constexpr (MX) {
+            pr.d2 = mixed_disp<ND>(xi, xj, bx, hbf, pr.dx);
+            pr.r = 0.5f * (Dif + D0jf * kapf);
+            const float rc = pr.r + tf;
+            pr.pass = pr.d2 < rc * rc * kShellMarginF;
+            pr.ov = fuse && pr.d2 < pr.r * pr.r;
+        } else {
+            const double Dj = xmul(D0j, kap);
+            pr.d2 = pair_disp<ND>(xi, xj, bx, ibx, pr.dx);
+            const double r_c = shell_cut<ND>(Di, Dj, t_shell);  // ndim <= 3: symmetric
+            pr.pass = pr.d2 < xmul(r_c, r_c);
+            pr.r = xmul(0.5, xadd(Di, Dj));
+            pr.ov = fuse && pr.d2 < xmul(pr.r, pr.r);
+        }
+    }
+    // The pair terms of a probed overlapping pair; the scalars once per pair
+    // (from the lower index).
+    __device__ __forceinline__ void commit(bool upper, const Probe& pr) {
+        if (!pr.ov) return;
+        if constexpr (MX) {
+            PairTermsF pf;
+            pair_terms_mixed_f<ND>(pr.dx, pr.d2, pr.r, fif, pf);
+            if (upper) {
+                sU += pf.U;
+                sLc += pf.Lc;
+                sdk += pf.dk;
+                sFm += pf.Fm;
+                smax = fmaxf(smax, pf.U);
+                ++scount;
+            }
+        } else {
+            PairTerms pt;
+            pair_terms_f64<ND>(pr.dx, pr.d2, pr.r, fi, pt);
+            if (upper) {
+                sU = xadd(sU, pt.U);
+                sLc = xadd(sLc, pt.Lc);
+                sdk = xadd(sdk, pt.dk);
+                sFm = xadd(sFm, pt.Fm);
+                smax = fmax(smax, pt.U);
+                ++scount;
+            }
+        }
+    }
+    // One candidate probed and committed: whether it is a partner.
     __device__ __forceinline__ bool candidate(bool upper, const double* xj, double D0j, float D0jf,
                                               const double* bx, const double* ibx, const float* hbf,
                                               double t_shell, float tf, bool fuse) {
-        if constexpr (MX) {
-            float dxf[ND];
-            const float d2f = mixed_disp<ND>(xi, xj, bx, hbf, dxf);
-            const float rsum = 0.5f * (Dif + D0jf * kapf);
-            const float rc = rsum + tf;
-            if (!(d2f < rc * rc * kShellMarginF)) return false;
-            if (fuse && d2f < rsum * rsum) {
-                PairTermsF pf;
-                pair_terms_mixed_f<ND>(dxf, d2f, rsum, fif, pf);
-                if (upper) {
-                    sU += pf.U;
-                    sLc += pf.Lc;
-                    sdk += pf.dk;
-                    sFm += pf.Fm;
-                    smax = fmaxf(smax, pf.U);
-                    ++scount;
-                }
-            }
-        } else {
-            const double Dj = xmul(D0j, kap);
-            double dx[ND];
-            const double d2 = pair_disp<ND>(xi, xj, bx, ibx, dx);
-            const double r_c = shell_cut<ND>(Di, Dj, t_shell);  // ndim <= 3: symmetric
-            if (!(d2 < xmul(r_c, r_c))) return false;
-            const double r_ij = xmul(0.5, xadd(Di, Dj));
-            if (fuse && d2 < xmul(r_ij, r_ij)) {
-                PairTerms pt;
-                pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
-                if (upper) {
-                    sU = xadd(sU, pt.U);
-                    sLc = xadd(sLc, pt.Lc);
-                    sdk = xadd(sdk, pt.dk);
-                    sFm = xadd(sFm, pt.Fm);
-                    smax = fmax(smax, pt.U);
-                    ++scount;
-                }
-            }
-        }
+        Probe pr;
+        probe(pr, xj, D0j, D0jf, bx, ibx, hbf, t_shell, tf, fuse);
+        if (!pr.pass) return false;
+        commit(upper, pr);
         return true;
     }
 
@@ -1380,12 +1400,34 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
                         sb[r] = s_ws[3 * r] + (pb[r] - s_wb[3 * r]);
                     }
                     const std::uint32_t c1 = ns[0], c2 = ns[0] + ns[1], tot = c2 + ns[2];
-                    for (std::uint32_t k = 0; k < tot; ++k) {
-                        const bool r0 = k < c1, r1 = k < c2;
-                        const std::uint32_t o = r0 ? k : (r1 ? k - c1 : k - c2);
-                        const std::uint32_t p = (r0 ? pb[0] : (r1 ? pb[1] : pb[2])) + o;
-                        const std::uint32_t s = (r0 ? sb[0] : (r1 ? sb[1] : sb[2])) + o;
-                        if (p != q) test(p, s);
+                    // two candidates per round: both probed (independent
+                    // work for the lane), then committed in scan order
+                    for (std::uint32_t k = 0; k < tot; k += 2) {
+                        std::uint32_t pp[2];
+                        typename UnitPair<ND, MX>::Probe pr[2];
+                        RCPG_UNROLL
+                        for (int v = 0; v < 2; ++v) {
+                            const std::uint32_t kk = min(k + static_cast<std::uint32_t>(v), tot - 1);
+                            const bool r0 = kk < c1, r1 = kk < c2;
+                            const std::uint32_t o = r0 ? kk : (r1 ? kk - c1 : kk - c2);
+                            pp[v] = (r0 ? pb[0] : (r1 ? pb[1] : pb[2])) + o;
+                            const std::uint32_t st = (r0 ? sb[0] : (r1 ? sb[1] : sb[2])) + o;
+                            const double2* r2 = reinterpret_cast<const double2*>(recs + 4 * static_cast<std::size_t>(st));
+                            const double2 rl = r2[0], rh = r2[1];
+                            double xj[ND], D0j;
+                            unpack_record<ND>(rl, rh, xj, D0j);
+                            float D0jf = 0.0f;
+                            if constexpr (MX) D0jf = STG ? unpack_f32(rh.y) : static_cast<float>(D0j);
+                            up.probe(pr[v], xj, D0j, D0jf, bx, ibx, hbf, t_shell, tf, fuse);
+                        }
+                        RCPG_UNROLL
+                        for (int v = 0; v < 2; ++v) {
+                            if (k + static_cast<std::uint32_t>(v) < tot && pp[v] != q && pr[v].pass) {
+                                if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = pp[v];
+                                ++n;
+                                up.commit(pp[v] > q, pr[v]);
+                            }
+                        }
                     }
                 } else {
                     for (int r = 0; r < R; ++r) {
