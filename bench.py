@@ -210,8 +210,8 @@ def run_batch_workload(args) -> int:
     rb.run_packing_batch(items[:2], {"max_steps": 50}, concurrency=args.concurrency)
     t0 = time.perf_counter()
     # the one-at-a-time sample: every k-th packing, so that it spans the size range
-    stride = max(1, len(items) // max(1, args.batch_single))
-    single = rb.run_packing_batch(items[::stride][: args.batch_single], run_opts, concurrency=1)
+    single_stride = max(1, len(items) // max(1, args.batch_single))
+    single = rb.run_packing_batch(items[::single_stride][: args.batch_single], run_opts, concurrency=1)
     t1 = time.perf_counter()
     res = rb.run_packing_batch(items, run_opts, concurrency=args.concurrency)
     t2 = time.perf_counter()
@@ -275,7 +275,7 @@ def run_batch_workload(args) -> int:
                    "timing": "host wall clock around run_packing_batch (inputs on the host, results back)"},
         "plain_engine": {"value": single_value, "unit": BATCH_METRIC, "packings": len(single),
                          "note": "the same engine one packing at a time (concurrency 1), every "
-                                 f"{stride}-th packing of the batch"},
+                                 f"{single_stride}-th packing of the batch"},
         "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": BATCH_METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "note": "the timed region is already end to end (host arrays in, result dicts out)"},

@@ -192,13 +192,19 @@ class WarmStart:
     """Trained network + the rule that turns its prediction into a growth-rung
     length: the first knot at which the predicted phi(t)/phi_J reaches
     1 - ``eps``, times ``margin``, kept within [``min_steps``, the reference's
-    deadline]."""
+    deadline]. Inputs are held inside the range of the training set
+    (``x_lo``, ``x_hi``) before the network sees them: a packing larger than
+    any trained on is predicted as the largest trained size, instead of by
+    extrapolating the network in log N."""
 
     def __init__(self, net: Network, x_mean, x_std, y_mean, y_std, eps: float = 2e-3,
-                 margin: float = 1.5, min_steps: int = 1500, meta: dict | None = None):
+                 margin: float = 1.5, min_steps: int = 1500, meta: dict | None = None,
+                 x_lo=None, x_hi=None):
         self.net = net
         self.x_mean = np.asarray(x_mean, dtype=np.float64)
         self.x_std = np.asarray(x_std, dtype=np.float64)
+        self.x_lo = None if x_lo is None else np.asarray(x_lo, dtype=np.float64)
+        self.x_hi = None if x_hi is None else np.asarray(x_hi, dtype=np.float64)
         self.y_mean = np.asarray(y_mean, dtype=np.float64)
         self.y_std = np.asarray(y_std, dtype=np.float64)
         self.eps = float(eps)
@@ -241,7 +247,7 @@ class WarmStart:
                 loss = net.train_step(Xn[idx], Yn[idx], max(lr_t, 1e-6), ow)
                 acc = loss if acc is None else acc + loss
             losses.append(float(acc) / per_epoch)
-        ws = cls(net, xm, xs, ym, ys, **kw)
+        ws = cls(net, xm, xs, ym, ys, x_lo=X.min(0), x_hi=X.max(0), **kw)
         ws.meta.update(train_loss=losses, n_train=int(n), epochs=int(epochs), batch=int(bs), lr=float(lr))
         return ws
 
@@ -249,6 +255,8 @@ class WarmStart:
     def predict(self, X) -> np.ndarray:
         """Raw descriptors [n x 11] -> [n x 17] (phi_J, 16 knot ratios)."""
         X = np.atleast_2d(np.asarray(X, dtype=np.float64))
+        if self.x_lo is not None:
+            X = np.clip(X, self.x_lo, self.x_hi)
         Yn = self.net.forward((X - self.x_mean) / self.x_std)
         return Yn.astype(np.float64) * self.y_std + self.y_mean
 
@@ -288,6 +296,7 @@ class WarmStart:
         np.savez_compressed(
             path, params=self.net.params().astype(np.float32), widths=np.asarray(self.net.widths),
             x_mean=self.x_mean, x_std=self.x_std, y_mean=self.y_mean, y_std=self.y_std,
+            **({} if self.x_lo is None else {"x_lo": self.x_lo, "x_hi": self.x_hi}),
             eps=self.eps, margin=self.margin, min_steps=self.min_steps,
             meta=np.asarray(repr({k: v for k, v in self.meta.items() if k != "train_loss"})))
 
@@ -295,8 +304,9 @@ class WarmStart:
     def load(cls, path=MODEL_PATH, device: int = 0) -> "WarmStart":
         z = np.load(path, allow_pickle=False)
         net = Network(widths=tuple(z["widths"].tolist()), device=device, params=z["params"])
+        lo_hi = {"x_lo": z["x_lo"], "x_hi": z["x_hi"]} if "x_lo" in z.files else {}
         return cls(net, z["x_mean"], z["x_std"], z["y_mean"], z["y_std"], float(z["eps"]),
-                   float(z["margin"]), int(z["min_steps"]), {"saved": str(z["meta"])})
+                   float(z["margin"]), int(z["min_steps"]), {"saved": str(z["meta"])}, **lo_hi)
 
 
 # ---- data --------------------------------------------------------------------------
