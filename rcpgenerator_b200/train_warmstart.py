@@ -53,8 +53,16 @@ def main(argv=None) -> dict:
     if a.eval_only:
         ws = W.WarmStart.load(a.out)
         items = [W.draw_evaluation_packing(s, a.eval_n) for s in range(a.eval_count)]
-        out = {"model": str(a.out), "eval": W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)}
+        ev = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)
+        plain_runs = ev.pop("plain_runs")
+        out = {"model": str(a.out), "eval": ev}
         out["eval"]["N"] = a.eval_n
+        # other rung margins on the same plain runs
+        for m in [float(x) for x in a.eval_margins.split(",") if x]:
+            ws.margin = m
+            e2 = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts, plain=plain_runs)
+            e2.pop("plain_runs")
+            out[f"eval_margin_{m:g}"] = e2
         print(json.dumps(out))
         return out
     t0 = time.perf_counter()
@@ -85,11 +93,15 @@ def main(argv=None) -> dict:
            "train_phi_std": float(Y[:, 0].std())}
     if a.eval_count > 0:
         items = [W.draw_evaluation_packing(s, a.eval_n) for s in range(a.eval_count)]
-        out["eval"] = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)
+        ev = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)
+        plain_runs = ev.pop("plain_runs")
+        out["eval"] = ev
         out["eval"]["N"] = a.eval_n
         for m in [float(x) for x in a.eval_margins.split(",") if x]:
             ws.margin = m
-            out[f"eval_margin_{m:g}"] = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)
+            e2 = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts, plain=plain_runs)
+            e2.pop("plain_runs")
+            out[f"eval_margin_{m:g}"] = e2
         ws.margin = a.margin
     print(json.dumps(out))
     return out

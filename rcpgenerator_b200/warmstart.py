@@ -371,21 +371,28 @@ def generate_training_set(count: int, seed0: int = 0, n_range=(64, 16384), optio
 
 
 def evaluate(ws: WarmStart, items: list, options: dict | None = None, concurrency: int = 0,
-             plain_options: dict | None = None) -> dict:
+             plain_options: dict | None = None, plain: tuple | None = None) -> dict:
     """Runs ``items`` plain and warm-started (same seeds, same batch call
     shape) and compares: packings/hour of each (host wall clock around the
     batch call), steps, phi_J per packing, and the network's phi_J error.
     ``plain_options`` (default: ``options``) are the plain runs' options, e.g.
     FP64 pair arithmetic for the plain method against mixed-precision
-    warm-started runs."""
+    warm-started runs. ``plain``: (results, seconds) of the plain runs of an
+    earlier evaluate() of the same items (its "plain_runs" entry), reused
+    instead of running them again."""
     import time
 
     plain_opts = options if plain_options is None else plain_options
-    t0 = time.perf_counter()
-    plain = run_packing_batch(items, plain_opts, concurrency)
+    if plain is None:
+        t0 = time.perf_counter()
+        plain_res = run_packing_batch(items, plain_opts, concurrency)
+        plain_s = time.perf_counter() - t0
+    else:
+        plain_res, plain_s = plain
     t1 = time.perf_counter()
     warm, phi_pred = ws.run_batch(items, options, concurrency)
-    t2 = time.perf_counter()
+    warm_s = time.perf_counter() - t1
+    plain = plain_res
     _, gs = ws.plan(items)
     pj = np.asarray([r["phi"] for r in plain])
     wj = np.asarray([r["phi"] for r in warm])
@@ -394,8 +401,8 @@ def evaluate(ws: WarmStart, items: list, options: dict | None = None, concurrenc
     n = len(items)
     return {
         "packings": n,
-        "plain_packings_per_hour": n / (t1 - t0) * 3600.0,
-        "warm_packings_per_hour": n / (t2 - t1) * 3600.0,
+        "plain_packings_per_hour": n / plain_s * 3600.0,
+        "warm_packings_per_hour": n / warm_s * 3600.0,
         "plain_mean_steps": float(ps.mean()),
         "warm_mean_steps": float(wsteps.mean()),
         "growth_steps_mean": float(np.mean(gs)),
@@ -413,4 +420,6 @@ def evaluate(ws: WarmStart, items: list, options: dict | None = None, concurrenc
         "max_overlap_plain": float(max(r["max_min_dist"] for r in plain)),
         "plain_pair_precision": str((plain_opts or {}).get("pair_precision", "f64")),
         "warm_pair_precision": str((options or {}).get("pair_precision", "f64")),
+        "margin": float(ws.margin),
+        "plain_runs": (plain, plain_s),  # for further evaluations of the same items
     }
