@@ -136,7 +136,7 @@ struct UnitShape {
     static constexpr int maxw = ndc == 2 ? 256 : 128;    // cells per unit at most
     static constexpr int slice = maxw + 3;               // cell_start entries per row (build)
     static constexpr int windows = 3 * rows;             // main, wrapped x-1, wrapped x+1 per row
-    static constexpr int min_blocks = 5;                 // resident blocks per SM (register budget)
+    static constexpr int min_blocks = 6;                 // resident blocks per SM (register budget)
 };
 
 // Cells per unit for a build with `cells` cells in a grid of nc0 cells per row:
@@ -1400,15 +1400,13 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
                         sb[r] = s_ws[3 * r] + (pb[r] - s_wb[3 * r]);
                     }
                     const std::uint32_t c1 = ns[0], c2 = ns[0] + ns[1], tot = c2 + ns[2];
-                    // kW candidates per round (4 mixed, 2 FP64: the FP64
-                    // probes hold twice the registers): all probed
-                    // (independent work for the lane), then committed in scan order
-                    constexpr int kW = MX ? 4 : 2;
-                    for (std::uint32_t k = 0; k < tot; k += kW) {
-                        std::uint32_t pp[kW];
-                        typename UnitPair<ND, MX>::Probe pr[kW];
+                    // two candidates per round: both probed (independent
+                    // work for the lane), then committed in scan order
+                    for (std::uint32_t k = 0; k < tot; k += 2) {
+                        std::uint32_t pp[2];
+                        typename UnitPair<ND, MX>::Probe pr[2];
                         RCPG_UNROLL
-                        for (int v = 0; v < kW; ++v) {
+                        for (int v = 0; v < 2; ++v) {
                             const std::uint32_t kk = min(k + static_cast<std::uint32_t>(v), tot - 1);
                             const bool r0 = kk < c1, r1 = kk < c2;
                             const std::uint32_t o = r0 ? kk : (r1 ? kk - c1 : kk - c2);
@@ -1423,7 +1421,7 @@ __global__ void __launch_bounds__(UnitShape<ND>::threads, UnitShape<ND>::min_blo
                             up.probe(pr[v], xj, D0j, D0jf, bx, ibx, hbf, t_shell, tf, fuse);
                         }
                         RCPG_UNROLL
-                        for (int v = 0; v < kW; ++v) {
+                        for (int v = 0; v < 2; ++v) {
                             if (k + static_cast<std::uint32_t>(v) < tot && pp[v] != q && pr[v].pass) {
                                 if (n < S) a.nbr[static_cast<std::uint64_t>(n) * N + q] = pp[v];
                                 ++n;
