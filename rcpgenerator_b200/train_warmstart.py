@@ -32,7 +32,7 @@ def main(argv=None) -> dict:
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eps", type=float, default=2e-3)
-    ap.add_argument("--margin", type=float, default=1.5)
+    ap.add_argument("--margin", type=float, default=2.0)
     ap.add_argument("--pair-precision", default="mixed", choices=("f64", "mixed"))
     ap.add_argument("--data", default=None, help="reuse a saved training set (.npz with X, Y)")
     ap.add_argument("--save-data", default=None)

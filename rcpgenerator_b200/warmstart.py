@@ -198,7 +198,7 @@ class WarmStart:
     extrapolating the network in log N."""
 
     def __init__(self, net: Network, x_mean, x_std, y_mean, y_std, eps: float = 2e-3,
-                 margin: float = 1.5, min_steps: int = 1500, meta: dict | None = None,
+                 margin: float = 2.0, min_steps: int = 1500, meta: dict | None = None,
                  x_lo=None, x_hi=None):
         self.net = net
         self.x_mean = np.asarray(x_mean, dtype=np.float64)
