@@ -1602,19 +1602,37 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
                 RCPG_UNROLL
                 for (std::uint32_t u = 0; u < kChunk; ++u)
                     if (k0 + u < n && jj[u] < N) load_pos_g<ND>(a.pos, jj[u], xj[u], D0j[u], 1);
+                // the chunk's displacements and overlap tests first (independent
+                // work), then the overlapping pairs' terms in row order
+                using PT = std::conditional_t<MX, float, double>;
+                PT pdx[kChunk][ND], pd2[kChunk], pr[kChunk];
+                bool pov[kChunk];
                 RCPG_UNROLL
                 for (std::uint32_t u = 0; u < kChunk; ++u) {
-                    if (k0 + u >= n) break;
+                    const bool live = k0 + u < n && jj[u] < N;
+                    if (!live) {  // a defined record for the unused slots
+                        RCPG_UNROLL
+                        for (int d = 0; d < ND; ++d) xj[u][d] = xi[d];
+                        D0j[u] = 0.0;
+                    }
+                    if constexpr (MX) {
+                        pd2[u] = mixed_disp<ND>(xi, xj[u], bx, hbf, pdx[u]);
+                        pr[u] = 0.5f * (Dif + static_cast<float>(D0j[u]) * kapf);
+                        pov[u] = live && pd2[u] < pr[u] * pr[u];
+                    } else {
+                        pr[u] = xmul(0.5, xadd(Di, xmul(D0j[u], kap)));
+                        pd2[u] = pair_disp<ND>(xi, xj[u], bx, ibx, pdx[u]);
+                        pov[u] = live && pd2[u] < xmul(pr[u], pr[u]);
+                    }
+                }
+                RCPG_UNROLL
+                for (std::uint32_t u = 0; u < kChunk; ++u) {
+                    if (!pov[u]) continue;
                     const std::uint32_t j = jj[u];
-                    if (j >= N) continue;
                     if constexpr (MX) {
                         // FP32 terms summed in FP32 (EXACT never takes FP32 terms)
-                        float dxf[ND];
-                        const float d2f = mixed_disp<ND>(xi, xj[u], bx, hbf, dxf);
-                        const float rsum = 0.5f * (Dif + static_cast<float>(D0j[u]) * kapf);
-                        if (!(d2f < rsum * rsum)) continue;
                         PairTermsF pf;
-                        pair_terms_mixed_f<ND>(dxf, d2f, rsum, fif, pf);
+                        pair_terms_mixed_f<ND>(pdx[u], pd2[u], pr[u], fif, pf);
                         if (j > i) {
                             sU += pf.U;
                             sLc += pf.Lc;
@@ -1623,27 +1641,21 @@ __global__ void __launch_bounds__(kForceBlock, EXACT ? 1 : ((MIXED && ND == 2) ?
                             smax = fmaxf(smax, pf.U);
                             ++scount;
                         }
-                        continue;
-                    }
-                    PairTerms pt;
-                    {
-                        const double r_ij = xmul(0.5, xadd(Di, xmul(D0j[u], kap)));
-                        double dx[ND];
-                        const double d2 = pair_disp<ND>(xi, xj[u], bx, ibx, dx);
-                        if (!(d2 < xmul(r_ij, r_ij))) continue;
-                        pair_terms_f64<ND>(dx, d2, r_ij, fi, pt);
-                    }
-                    if (j > i) {
-                        if constexpr (EXACT) {
-                            a.pterm[static_cast<std::uint64_t>(nterm) * N + i] = pt;
-                            ++nterm;
-                        } else {
-                            sU = xadd(sU, pt.U);
-                            sLc = xadd(sLc, pt.Lc);
-                            sdk = xadd(sdk, pt.dk);
-                            sFm = xadd(sFm, pt.Fm);
-                            smax = fmax(smax, pt.U);
-                            ++scount;
+                    } else {
+                        PairTerms pt;
+                        pair_terms_f64<ND>(pdx[u], pd2[u], pr[u], fi, pt);
+                        if (j > i) {
+                            if constexpr (EXACT) {
+                                a.pterm[static_cast<std::uint64_t>(nterm) * N + i] = pt;
+                                ++nterm;
+                            } else {
+                                sU = xadd(sU, pt.U);
+                                sLc = xadd(sLc, pt.Lc);
+                                sdk = xadd(sdk, pt.dk);
+                                sFm = xadd(sFm, pt.Fm);
+                                smax = fmax(smax, pt.U);
+                                ++scount;
+                            }
                         }
                     }
                 }
