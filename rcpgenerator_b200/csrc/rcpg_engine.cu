@@ -745,7 +745,7 @@ void Engine::destroy_graph() {
 
 // Kernels of one neighbour build (launch_rebuild): prepare, bin, the scan
 // (one kernel, or three for more than 4096 tiles of cells), scatter, cell
-// sort, the permutation of cell-order storage, the cell-order search
+// sort, the permutation of cell-order storage, the cell-unit search
 // (ndim <= 3, N >= 20,000; one kernel per pair precision the run may use) or
 // the tiled search, and the warp search.
 std::uint64_t Engine::kernels_per_build() const {

@@ -349,7 +349,7 @@ __device__ __forceinline__ bool use_tiled(const DevArrays& a) {
     return !a.permute && a.sorted_rows && (a.N >= kTiledMinN) && tiled_build_ok<ND>(a.ctl);
 }
 
-// the cell-order search builds the rows (graph mode, ndim 2 and 3, one size
+// the cell-unit search builds the rows (graph mode, ndim 2 and 3, one size
 // class, at least 3 cells per axis)
 template <int ND>
 __device__ __forceinline__ bool use_cells(const DevArrays& a) {
@@ -2388,7 +2388,7 @@ void launch_rebuild_timed(const DevArrays& a, cudaStream_t st, cudaEvent_t e0, c
 }
 
 void launch_forces(const DevArrays& a, int exact_terms, cudaStream_t st) {
-    // k_forces (and the cell-order search) read a 4-double particle record
+    // k_forces (and the cell-unit search) read a 4-double particle record
     // (ndim <= 3) with one 256-bit load
     if (a.P == 4 && (((reinterpret_cast<std::uintptr_t>(a.pos) | reinterpret_cast<std::uintptr_t>(a.pos_alt)) & 31u) != 0))
         throw std::invalid_argument("rcpgenerator_b200: particle records must be 32-byte aligned");

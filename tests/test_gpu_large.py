@@ -10,7 +10,7 @@ tests/golden/make_large_golden.py from the compiled reference):
   half list (get_pairs_kdtree, ENG:2758-3526) exactly, and rcpg_forces on it the
   reference's get_forces_nd_3 forces bit for bit;
 * the graph engine's build (particles in cell order, rows in scan order, the
-  step's forces fused into the cell-order search) holds the same pair set in FP64; its fused FP64 forces equal the
+  step's forces fused into the cell-unit search) holds the same pair set in FP64; its fused FP64 forces equal the
   pair kernel's on the same rows bit for bit and the reference's to 1e-12 (the
   rows are summed in scan order instead of ascending order); in mixed
   precision its rows are a superset of the FP64 shell (every extra pair lies
@@ -35,7 +35,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 CASES = ["bi2d_n30k", "mono3d_n24k", "bi3d_sphere_n20k", "walls2d_n25k", "powerlaw3d_sphere_n25k"]
-# whether the build computes the forces in the same pass: the cell-order search
+# whether the build computes the forces in the same pass: the cell-unit search
 # of the graph engine does (ndim <= 3, one size class); the power law of size
 # ratio 10 has several size classes and takes the warp search, after which the
 # pair kernel computes the forces
