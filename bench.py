@@ -38,9 +38,9 @@ WORKLOAD = dict(phi=0.30, N=1_000_000, Ndim=2, box=[1.0, 1.0], walls=[0, 0],
                 dist={"type": "bidisperse", "d1": 1.0, "d2": 1.4, "p": 0.5}, seed=123)
 PEAKS = REPO / "MEASURED_PEAKS.json"
 # DRAM bytes (read + write) per algorithmic byte of k_forces from one ncu capture
-# (profiles/k_forces_bidisperse2d_n3e5_mixed.md: 24.2 MB for 20.1 MB at N = 300k);
+# (profiles/k_forces_bidisperse2d_n3e5_mixed.md: 23.2 MB for 20.26 MB at N = 300k);
 # the N = 1M launch is too large to capture with the full metric set
-FORCES_TRAFFIC_PER_ALG_BYTE = 24.2 / 20.1
+FORCES_TRAFFIC_PER_ALG_BYTE = 23.2 / 20.26
 # the same for the cell-unit build with fused forces, k_cells<2, mixed>
 # (profiles/k_cells_bidisperse2d_n3e5_mixed.md: 12.3 MB for 22.7 MB at N = 300k; the rows and
 # forces it writes are still in L2 when the launch ends)
