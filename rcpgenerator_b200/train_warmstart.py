@@ -22,6 +22,14 @@ import numpy as np
 from . import warmstart as W
 
 
+def training_rows(seeds, stride: int) -> np.ndarray:
+    """Rows of a saved training set that train the network: every packing
+    whose seed is not a multiple of ``stride`` (those are the batch
+    benchmark's sample, held out); all rows when ``stride`` <= 0."""
+    seeds = np.asarray(seeds, dtype=np.int64)
+    return np.ones(seeds.shape, dtype=bool) if stride <= 0 else (seeds % stride) != 0
+
+
 def main(argv=None) -> dict:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--count", type=int, default=4096)
@@ -71,7 +79,7 @@ def main(argv=None) -> dict:
         z = np.load(a.data)
         X, Y = z["X"], z["Y"]
         if a.exclude_stride > 0 and "seeds" in z.files:
-            keep = (z["seeds"] % a.exclude_stride) != 0
+            keep = training_rows(z["seeds"], a.exclude_stride)
             held = int((~keep).sum())
             X, Y = X[keep], Y[keep]
     else:

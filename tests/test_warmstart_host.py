@@ -65,6 +65,40 @@ def test_growth_rule():
     assert ws.growth_steps_from_prediction(np.concatenate([[0.6], np.ones(16)]), 400, 3) == 1500
 
 
+class _EchoNet:
+    """Stands in for the device network: returns its standardised input."""
+    widths = (3, 4, 3)
+
+    def forward(self, Xn):
+        return np.asarray(Xn, dtype=np.float32)
+
+
+def test_inputs_held_inside_the_training_range():
+    ws = W.WarmStart(_EchoNet(), np.zeros(3), np.ones(3), np.zeros(3), np.ones(3),
+                     x_lo=np.array([0.0, -1.0, 2.0]), x_hi=np.array([1.0, 1.0, 5.0]))
+    P = ws.predict(np.array([[0.5, -3.0, 9.0], [2.0, 0.25, 3.0]]))
+    np.testing.assert_array_equal(P, [[0.5, -1.0, 5.0], [1.0, 0.25, 3.0]])
+    # a model without a recorded range sees the raw inputs
+    ws2 = W.WarmStart(_EchoNet(), np.zeros(3), np.ones(3), np.zeros(3), np.ones(3))
+    np.testing.assert_array_equal(ws2.predict([[9.0, 9.0, 9.0]]), [[9.0, 9.0, 9.0]])
+
+
+def test_shipped_model_records_its_training_range():
+    z = np.load(W.MODEL_PATH)
+    assert "x_lo" in z.files and z["x_lo"].shape == z["x_mean"].shape == z["x_hi"].shape
+    assert np.all(z["x_lo"] <= z["x_mean"]) and np.all(z["x_mean"] <= z["x_hi"])
+    # log N is the last input: trained on N in [64, 16384]
+    assert math.exp(z["x_lo"][-1]) >= 64 - 1e-6 and math.exp(z["x_hi"][-1]) <= 16384 + 1e-6
+    assert float(z["margin"]) == 2.0
+
+
+def test_training_rows_hold_out_the_benchmark_sample():
+    from rcpgenerator_b200.train_warmstart import training_rows
+    keep = training_rows(np.arange(4096), 8)
+    assert keep.sum() == 3584 and not keep[::8].any() and keep[1::8].all()
+    assert training_rows(np.arange(5), 0).all()
+
+
 def test_growth_steps_option_in_the_host_emulation(golden):
     """growth_steps = 1500 ends the rung at step 1501 (mu_flag 1 -> 0), the
     default keeps the reference's deadline; everything before is identical."""
