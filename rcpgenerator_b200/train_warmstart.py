@@ -47,6 +47,7 @@ def main(argv=None) -> dict:
     ap.add_argument("--out", default=str(W.MODEL_PATH))
     ap.add_argument("--eval-count", type=int, default=16)
     ap.add_argument("--eval-n", type=int, default=100_000)
+    ap.add_argument("--eval-seed0", type=int, default=0, help="first seed of the held-out evaluation packings")
     ap.add_argument("--eval-concurrency", type=int, default=8)
     ap.add_argument("--eval-margins", default="", help="extra comma-separated margins to evaluate")
     ap.add_argument("--eval-plain-precision", default=None, choices=("f64", "mixed"),
@@ -60,7 +61,7 @@ def main(argv=None) -> dict:
     plain_opts = {"pair_precision": a.eval_plain_precision or a.pair_precision}
     if a.eval_only:
         ws = W.WarmStart.load(a.out)
-        items = [W.draw_evaluation_packing(s, a.eval_n) for s in range(a.eval_count)]
+        items = [W.draw_evaluation_packing(s, a.eval_n) for s in range(a.eval_seed0, a.eval_seed0 + a.eval_count)]
         ev = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)
         plain_runs = ev.pop("plain_runs")
         out = {"model": str(a.out), "eval": ev}
@@ -100,7 +101,7 @@ def main(argv=None) -> dict:
            "train_phi_mae": float(np.abs(P[:, 0] - Y[:, 0]).mean()),
            "train_phi_std": float(Y[:, 0].std())}
     if a.eval_count > 0:
-        items = [W.draw_evaluation_packing(s, a.eval_n) for s in range(a.eval_count)]
+        items = [W.draw_evaluation_packing(s, a.eval_n) for s in range(a.eval_seed0, a.eval_seed0 + a.eval_count)]
         ev = W.evaluate(ws, items, opts, a.eval_concurrency, plain_opts)
         plain_runs = ev.pop("plain_runs")
         out["eval"] = ev
