@@ -1079,7 +1079,8 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_build_search_tiled(DevArray
 // neighbour row, rows in order (row offset r = (dy+1) + 3 (dz+1)), then the
 // wrapped cell of each row where the particle sits at the row's end (2-D: the
 // three rows' ranges are walked as one sequence, so the lanes of a warp run
-// about as many rounds as their longest candidate list). Each goes through
+// about as many rounds as their longest candidate list, and each round probes
+// two candidates before committing them in order). Each goes through
 // the reference's predicate in FP64, or (MX) the mixed-precision shell test
 // (FP32 on FP64 differences, widened by kShellMarginF so that the rows hold
 // every pair of the FP64 shell); rows hold the partners in that order and the
